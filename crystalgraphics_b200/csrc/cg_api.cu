@@ -1,0 +1,787 @@
+// cg_api.cu — the C ABI of libcg_cuda.so (include/cg_cuda.h).
+//
+// Host side of the View() hot path: the environment (EnvInit/EnvTerm), scene
+// upload (LoadScene), the chunked wavefront frame loop, film readback and the
+// parity ray query.  The batched form is in cg_batch.cu, the served form in
+// cg_server.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cg_cuda.h"
+#include "cg_api_internal.h"
+#include "cg_kernels.h"
+#include "cg_scene.h"
+
+namespace cg {
+
+thread_local std::string tl_error;
+
+int fail(int code, const std::string& msg) {
+  tl_error = msg;
+  return code;
+}
+
+int cudaFail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a non-sticky error so the next call starts clean
+  return fail(e == cudaErrorMemoryAllocation ? CG_E_OOM : CG_E_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int DeviceArena::alloc(size_t bytes) {
+  release();
+  if (bytes == 0) bytes = 256;
+  cudaError_t e = cudaMalloc(&base, bytes);
+  if (e != cudaSuccess) {
+    base = nullptr;
+    cudaGetLastError();
+    return cudaFail(e, "cudaMalloc");
+  }
+  size = bytes;
+  return CG_OK;
+}
+void DeviceArena::release() {
+  if (base) cudaFree(base);
+  base = nullptr;
+  size = 0;
+}
+
+// ---- scenes -------------------------------------------------------------------
+namespace {
+std::atomic<uint64_t> g_tag_counter{0x5eed0000u};
+template <class T>
+size_t bytesOf(const std::vector<T>& v) {
+  return v.size() * sizeof(T);
+}
+}  // namespace
+
+int uploadScene(const HostScene& h, SceneDev& s) {
+  struct Part {
+    const void* src;
+    size_t bytes;
+    size_t off;
+  };
+  std::vector<Part> parts = {
+      {h.tlas.data(), bytesOf(h.tlas), 0},       {h.blas.data(), bytesOf(h.blas), 0},
+      {h.tris.data(), bytesOf(h.tris), 0},       {h.tri_vidx.data(), bytesOf(h.tri_vidx), 0},
+      {h.vnormal.data(), bytesOf(h.vnormal), 0}, {h.inst.data(), bytesOf(h.inst), 0},
+      {h.mat.data(), bytesOf(h.mat), 0},         {h.eprim.data(), bytesOf(h.eprim), 0},
+      {h.alias.data(), bytesOf(h.alias), 0},     {h.light_bvh.data(), bytesOf(h.light_bvh), 0},
+      {h.ltri.data(), bytesOf(h.ltri), 0},       {h.env.data(), bytesOf(h.env), 0}};
+  size_t total = 0;
+  for (auto& p : parts) {
+    p.off = total;
+    total += align256(std::max<size_t>(p.bytes, 16));
+  }
+  int rc = s.arena.alloc(total);
+  if (rc != CG_OK) return rc;
+  char* base = static_cast<char*>(s.arena.base);
+  for (auto& p : parts)
+    if (p.bytes) CG_CUDA(cudaMemcpy(base + p.off, p.src, p.bytes, cudaMemcpyHostToDevice));
+  SceneView& v = s.view;
+  v.tlas = reinterpret_cast<const BvhNode*>(base + parts[0].off);
+  v.blas = reinterpret_cast<const BvhNode*>(base + parts[1].off);
+  v.tris = reinterpret_cast<const float4*>(base + parts[2].off);
+  v.tri_vidx = reinterpret_cast<const uint4*>(base + parts[3].off);
+  v.vnormal = reinterpret_cast<const float4*>(base + parts[4].off);
+  v.inst = reinterpret_cast<const DevInstance*>(base + parts[5].off);
+  v.mat = reinterpret_cast<const DevMaterial*>(base + parts[6].off);
+  v.eprim = reinterpret_cast<const DevEmissivePrim*>(base + parts[7].off);
+  v.alias = reinterpret_cast<const DevAlias*>(base + parts[8].off);
+  v.light_bvh = reinterpret_cast<const BvhNode*>(base + parts[9].off);
+  v.light_tri = reinterpret_cast<const DevLightTri*>(base + parts[10].off);
+  v.env = reinterpret_cast<const float4*>(base + parts[11].off);
+  v.env_w = h.env_w;
+  v.env_h = h.env_h;
+  v.emissive_count = static_cast<uint32_t>(h.eprim.size());
+  v.instance_count = static_cast<uint32_t>(h.inst.size());
+  v.has_tlas = h.inst.empty() ? 0u : 1u;
+  v.has_lights = h.eprim.empty() ? 0u : 1u;
+  s.eprim_off = parts[7].off;
+  s.alias_off = parts[8].off;
+  return CG_OK;
+}
+
+// ---- frame planning ---------------------------------------------------------------
+Caps capsOf(const cg_conf& c) {
+  Caps k;
+  k.trace_depth = std::clamp(c.trace_depth, 1u, 64u);
+  k.transport_cap = c.max_transport_sample_count;
+  k.emission_cap = c.max_emission_sample_count;
+  k.diffuse_cap = c.max_diffuse_sample_count;
+  k.rough_cap = c.max_rough_sample_count;
+  return k;
+}
+
+// The transport and light sample budgets per depth (sample.wesl:215-233 with
+// lod.wesl:16-18), in the kernels' float arithmetic: which depths can hold
+// rays, which can draw light samples, and the most rays a sample can have at
+// one depth (each lobe gets at most one sample, so a hit has at most
+// min(budget, lobes) children).
+LevelPlan planLevels(const Caps& caps, uint32_t max_lobes) {
+  LevelPlan p;
+  const int32_t D = static_cast<int32_t>(caps.trace_depth);
+  const uint32_t cut = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
+  uint64_t prod = 1, maxprod = 1;
+  for (int32_t d = 0; d < D; ++d) {
+    p.levels = static_cast<uint32_t>(d) + 1u;
+    const float heur = static_cast<float>(D - d) / static_cast<float>(D);
+    const float tf = heur * static_cast<float>(std::min(caps.transport_cap, 4u));
+    const float ef = heur * static_cast<float>(std::min(caps.emission_cap, 1u));
+    const uint32_t ta = tf > 0.0f ? static_cast<uint32_t>(tf) : 0u;
+    const uint32_t ea = ef > 0.0f ? static_cast<uint32_t>(ef) : 0u;
+    const bool shades = static_cast<uint32_t>(d) < cut;
+    p.shadow[d] = shades && ea > 0u;
+    const uint32_t fan = shades ? std::min(ta, max_lobes) : 0u;
+    if (fan == 0) break;
+    prod *= fan;
+    maxprod = std::max(maxprod, prod);
+  }
+  p.max_product = maxprod;
+  return p;
+}
+
+void layoutViews(std::vector<ViewDev>& views) {
+  uint64_t px_off = 0, smp_off = 0;
+  for (auto& v : views) {
+    v.pixel_offset = px_off;
+    v.sample_offset = smp_off;
+    px_off += v.pixel_count;
+    smp_off += uint64_t(v.pixel_count) * v.spp;
+  }
+}
+
+void cameraBasis(const cg_camera& cam, ViewDev& v) {
+  // cameraRay's basis (compute.wesl:68-74) in plain float, as the host
+  // restatement computes it: dx = normalize(cross(dir, +z)) * viewport.x,
+  // dy = normalize(cross(dir, dx)) * viewport.y.
+  const float* d = cam.direction;
+  const float cx[3] = {d[1] * 1.0f - 0.0f * d[2], d[2] * 0.0f - 1.0f * d[0],
+                       d[0] * 0.0f - 0.0f * d[1]};
+  const float l = std::sqrt(cx[0] * cx[0] + cx[1] * cx[1] + cx[2] * cx[2]);
+  const float dx[3] = {cx[0] / l * cam.viewport[0], cx[1] / l * cam.viewport[0],
+                       cx[2] / l * cam.viewport[0]};
+  const float cy[3] = {d[1] * dx[2] - dx[1] * d[2], d[2] * dx[0] - dx[2] * d[0],
+                       d[0] * dx[1] - dx[0] * d[1]};
+  const float m = std::sqrt(cy[0] * cy[0] + cy[1] * cy[1] + cy[2] * cy[2]);
+  for (int a = 0; a < 3; ++a) {
+    v.pos[a] = cam.position[a];
+    v.dir[a] = d[a];
+    v.dx[a] = dx[a];
+    v.dy[a] = cy[a] / m * cam.viewport[1];
+  }
+}
+
+// ---- Renderer ------------------------------------------------------------------------
+int Renderer::init(int dev) {
+  device = dev;
+  CG_CUDA(cudaSetDevice(dev));
+  CG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CG_CUDA(cudaEventCreate(&ev0));
+  CG_CUDA(cudaEventCreate(&ev1));
+  CG_CUDA(cudaMalloc(&wl_tree, 65535 * sizeof(float)));
+  CG_CUDA(cudaMalloc(&wl_const, 4 * sizeof(float)));
+  launchWavelengthTree(wl_tree, wl_const, stream);
+  CG_CUDA(cudaGetLastError());
+  CG_CUDA(cudaStreamSynchronize(stream));
+  return CG_OK;
+}
+
+Renderer::~Renderer() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
+  wave_arena.release();
+  if (wl_tree) cudaFree(wl_tree);
+  if (wl_const) cudaFree(wl_const);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+int Renderer::ensureWave(uint32_t capacity) {
+  if (wave_arena.base && wave.capacity == capacity) return CG_OK;
+  if (stream) CG_CUDA(cudaStreamSynchronize(stream));
+  const size_t Q = capacity;
+  const size_t parts[] = {Q * 16, Q * 16, Q * 16, Q * 16, Q * 4, Q * 4,  // ray queues
+                          Q * 16, Q * 4,                                 // hits
+                          Q * 16, Q * 16, Q * 4,                         // shadow queue
+                          Q * 4,  Q * 4,  Q * 4,                         // sample slots
+                          256,    256,    256};                          // counts, stats, status
+  size_t total = 0;
+  for (size_t b : parts) total += align256(b);
+  wave = WaveBuffers{};
+  int rc = wave_arena.alloc(total);
+  if (rc != CG_OK) return rc;
+  char* p = static_cast<char*>(wave_arena.base);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    char* r = p + off;
+    off += align256(b);
+    return r;
+  };
+  wave.ray_o[0] = reinterpret_cast<float4*>(take(Q * 16));
+  wave.ray_o[1] = reinterpret_cast<float4*>(take(Q * 16));
+  wave.ray_d[0] = reinterpret_cast<float4*>(take(Q * 16));
+  wave.ray_d[1] = reinterpret_cast<float4*>(take(Q * 16));
+  wave.ray_slot[0] = reinterpret_cast<uint32_t*>(take(Q * 4));
+  wave.ray_slot[1] = reinterpret_cast<uint32_t*>(take(Q * 4));
+  wave.hit = reinterpret_cast<float4*>(take(Q * 16));
+  wave.hit_inst = reinterpret_cast<int32_t*>(take(Q * 4));
+  wave.sh_o = reinterpret_cast<float4*>(take(Q * 16));
+  wave.sh_d = reinterpret_cast<float4*>(take(Q * 16));
+  wave.sh_slot = reinterpret_cast<uint32_t*>(take(Q * 4));
+  wave.s_L = reinterpret_cast<float*>(take(Q * 4));
+  wave.s_lambda = reinterpret_cast<float*>(take(Q * 4));
+  wave.s_prob = reinterpret_cast<float*>(take(Q * 4));
+  wave.counts = reinterpret_cast<uint32_t*>(take(256));
+  wave.stats = reinterpret_cast<unsigned long long*>(take(256));
+  wave.status = reinterpret_cast<uint32_t*>(take(256));
+  wave.capacity = capacity;
+  wave.sample_capacity = capacity;
+  CG_CUDA(cudaMemset(wave.counts, 0, 256));
+  CG_CUDA(cudaMemset(wave.stats, 0, 256));
+  CG_CUDA(cudaMemset(wave.status, 0, 256));
+  return CG_OK;
+}
+
+uint32_t Renderer::chunkSamples(const SceneDev& scene, const Caps& caps) const {
+  const LevelPlan plan = planLevels(caps, std::max(1u, scene.max_lobes));
+  return static_cast<uint32_t>(std::min<uint64_t>(
+      wave.sample_capacity, wave.capacity / std::max<uint64_t>(1, plan.max_product)));
+}
+
+void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const ViewDev* table,
+                            const ChunkDesc& ch, const Caps& caps, cudaStream_t s,
+                            RenderRecord& rec) {
+  const LevelPlan plan = planLevels(caps, std::max(1u, scene.max_lobes));
+  FrameConst fc;
+  fc.views = table;
+  fc.view_count = view_count;
+  fc.caps = caps;
+  fc.wl_tree = wl_tree;
+  fc.wl_const = wl_const;
+  LaunchShape ls;
+  ls.extend_block = tuning.extend_block;
+  ls.shade_block = tuning.shade_block;
+  profBegin(CG_K_GEN, s);
+  launchGen(fc, wave, ch, s);
+  profEnd(s);
+  ++rec.launches;
+  for (uint32_t d = 0; d < plan.levels; ++d) {
+    const int parity = static_cast<int>(d & 1u);
+    profBegin(CG_K_EXTEND, s);
+    launchExtend(scene.view, wave, parity, counting, ls, s);
+    profEnd(s);
+    profBegin(CG_K_SHADE, s);
+    launchShade(scene.view, fc, wave, static_cast<int>(d), parity, ls, s);
+    profEnd(s);
+    rec.launches += 2;
+    if (plan.shadow[d]) {
+      profBegin(CG_K_SHADOW, s);
+      launchShadow(scene.view, wave, counting, ls, s);
+      profEnd(s);
+      ++rec.launches;
+    }
+  }
+  profBegin(CG_K_RESOLVE, s);
+  launchResolve(fc, wave, ch, s);
+  profEnd(s);
+  ++rec.launches;
+  ++rec.chunks;
+  rec.samples += ch.sample_count;
+}
+
+int Renderer::enqueueViews(const SceneDev& scene, const std::vector<ViewDev>& views,
+                           const ViewDev* table, const Caps& caps, cudaStream_t s,
+                           RenderRecord& rec) {
+  if (views.empty()) return CG_OK;
+  int rc = ensureWave(tuning.queue_capacity);
+  if (rc != CG_OK) return rc;
+  const uint32_t sample_cap = chunkSamples(scene, caps);
+  for (const auto& v : views)
+    if (v.spp > sample_cap)
+      return fail(CG_E_INVALID, "spp " + std::to_string(v.spp) + " exceeds the wavefront chunk of " +
+                                    std::to_string(sample_cap) + " samples");
+  // chunks of whole pixels, each filled up to sample_cap samples
+  size_t vi = 0;
+  uint64_t pix_in_view = 0, gpix = 0, gsmp = 0;
+  while (vi < views.size()) {
+    ChunkDesc ch;
+    ch.sample_begin = gsmp;
+    ch.pixel_begin = gpix;
+    ch.sample_count = 0;
+    ch.pixel_count = 0;
+    while (vi < views.size()) {
+      const ViewDev& v = views[vi];
+      if (pix_in_view >= v.pixel_count) {
+        ++vi;
+        pix_in_view = 0;
+        continue;
+      }
+      const uint64_t room = (sample_cap - ch.sample_count) / v.spp;
+      if (room == 0) break;
+      const uint64_t take = std::min<uint64_t>(room, v.pixel_count - pix_in_view);
+      ch.sample_count += static_cast<uint32_t>(take * v.spp);
+      ch.pixel_count += static_cast<uint32_t>(take);
+      pix_in_view += take;
+    }
+    if (ch.pixel_count == 0) break;
+    gpix += ch.pixel_count;
+    gsmp += ch.sample_count;
+    enqueueChunk(scene, static_cast<uint32_t>(views.size()), table, ch, caps, s, rec);
+  }
+  return CG_OK;
+}
+
+void Renderer::profBegin(int kind, cudaStream_t s) {
+  if (!profiling) return;
+  if (prof_used + 2 > prof_events.size()) {
+    for (int k = 0; k < 64; ++k) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return;
+      prof_events.push_back(e);
+    }
+  }
+  prof_kind.resize(prof_events.size() / 2 + 1);
+  prof_kind[prof_used / 2] = kind;
+  cudaEventRecord(prof_events[prof_used], s);
+}
+
+void Renderer::profEnd(cudaStream_t s) {
+  if (!profiling || prof_used + 2 > prof_events.size()) return;
+  cudaEventRecord(prof_events[prof_used + 1], s);
+  prof_used += 2;
+}
+
+void Renderer::profCollect() {
+  for (size_t i = 0; i + 1 < prof_used; i += 2) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, prof_events[i], prof_events[i + 1]) == cudaSuccess) {
+      const int k = prof_kind[i / 2];
+      prof.ms[k] += ms;
+      ++prof.launches[k];
+    }
+  }
+  prof_used = 0;
+}
+
+int Renderer::beginStats(cudaStream_t s) {
+  CG_CUDA(cudaMemsetAsync(wave.stats, 0, 256, s));
+  CG_CUDA(cudaMemsetAsync(wave.status, 0, 256, s));
+  return CG_OK;
+}
+
+int Renderer::readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_stats& out) {
+  unsigned long long st[8] = {0};
+  uint32_t status = 0;
+  CG_CUDA(cudaMemcpyAsync(st, wave.stats, sizeof(st), cudaMemcpyDeviceToHost, s));
+  CG_CUDA(cudaMemcpyAsync(&status, wave.status, sizeof(status), cudaMemcpyDeviceToHost, s));
+  CG_CUDA(cudaStreamSynchronize(s));
+  profCollect();
+  out.samples = rec.samples;
+  out.extend_rays = st[0];
+  out.shadow_rays = st[1];
+  out.node_visits = st[2];
+  out.tri_tests = st[3];
+  out.inst_visits = st[4];
+  out.chunks = rec.chunks;
+  out.kernel_launches = rec.launches;
+  out.device_ms = ms;
+  if (status & 1u) return fail(CG_E_DEVICE, "traversal stack overflow in a kernel");
+  if (status & 2u) return fail(CG_E_DEVICE, "ray queue overflow in a kernel");
+  return CG_OK;
+}
+
+// ---- the environment ---------------------------------------------------------------
+Env* g_env = nullptr;
+std::mutex g_env_mu;
+
+int Env::uploadViews(const std::vector<ViewDev>& views, cudaStream_t s) {
+  if (views.size() > view_cap) {
+    if (views_dev) cudaFree(views_dev);
+    views_dev = nullptr;
+    view_cap = 0;
+    CG_CUDA(cudaMalloc(&views_dev, views.size() * sizeof(ViewDev)));
+    view_cap = views.size();
+  }
+  CG_CUDA(cudaMemcpyAsync(views_dev, views.data(), views.size() * sizeof(ViewDev),
+                          cudaMemcpyHostToDevice, s));
+  return CG_OK;
+}
+
+Env::~Env() {
+  if (stream) cudaStreamSynchronize(stream);
+  graphs.clear();
+  if (views_dev) cudaFree(views_dev);
+  if (film) cudaFree(film);
+  if (rgba) cudaFree(rgba);
+}
+
+static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& out) {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CG_E_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= ndev) return fail(CG_E_INVALID, "device index out of range");
+  if (conf_in.render_width == 0 || conf_in.render_height == 0)
+    return fail(CG_E_INVALID, "render size must be nonzero");
+  if (conf_in.sample_count == 0) return fail(CG_E_INVALID, "sample_count must be nonzero");
+  auto env = std::make_unique<Env>();
+  env->conf = conf_in;
+  env->conf.trace_depth = std::clamp(conf_in.trace_depth, 1u, 64u);
+  int rc = env->init(device);
+  if (rc != CG_OK) return rc;
+  const size_t npx = size_t(env->conf.render_width) * env->conf.render_height;
+  CG_CUDA(cudaMalloc(&env->film, npx * sizeof(float4)));
+  CG_CUDA(cudaMalloc(&env->rgba, npx * sizeof(uchar4)));
+  CG_CUDA(cudaMemset(env->film, 0, npx * sizeof(float4)));
+  CG_CUDA(cudaMemset(env->rgba, 0, npx * sizeof(uchar4)));
+  out = std::move(env);
+  return CG_OK;
+}
+
+}  // namespace cg
+
+using namespace cg;
+
+extern "C" {
+
+CG_API const char* cg_version(void) { return "crystalgraphics-b200 0.1 (sm_100a)"; }
+
+CG_API const char* cg_last_error(void) { return tl_error.c_str(); }
+
+CG_API int cg_init(const cg_conf* conf, int device) {
+  if (!conf) return fail(CG_E_INVALID, "conf is null");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  delete g_env;
+  g_env = nullptr;
+  std::unique_ptr<Env> env;
+  int rc = createEnv(*conf, device, env);
+  if (rc != CG_OK) return rc;
+  g_env = env.release();
+  return CG_OK;
+}
+
+CG_API int cg_term(void) {
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  delete g_env;
+  g_env = nullptr;
+  return CG_OK;
+}
+
+CG_API int cg_status(void) {
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  return g_env ? 1 : 0;
+}
+
+CG_API int cg_get_conf(cg_conf* out) {
+  if (!out) return fail(CG_E_INVALID, "out is null");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  *out = g_env->conf;
+  return CG_OK;
+}
+
+CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
+  if (!out) return fail(CG_E_INVALID, "out is null");
+  *out = nullptr;
+  auto sd = std::make_unique<SceneDev>();
+  std::string err;
+  int rc = packScene(desc, sd->host, err);
+  if (rc != CG_OK) return fail(rc, err);
+  if (sd->host.blas_depth + sd->host.tlas_depth + 2 > 64)
+    return fail(CG_E_INVALID, "BVH too deep for the 64-entry traversal stack");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CG_E_CUDA, "no CUDA device");
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (g_env) cudaSetDevice(g_env->device);
+  }
+  rc = uploadScene(sd->host, *sd);
+  if (rc != CG_OK) return rc;
+  sd->max_lobes = sd->host.max_lobes;
+  sd->tag = ++g_tag_counter;
+  cg_scene_info& in = sd->info;
+  in.instance_count = static_cast<uint32_t>(sd->host.inst.size());
+  in.mesh_count = sd->host.mesh_count;
+  in.triangle_count = sd->host.triangle_count;
+  in.material_count = static_cast<uint32_t>(sd->host.mat.size());
+  in.emissive_count = static_cast<uint32_t>(sd->host.eprim.size());
+  in.blas_node_count = static_cast<uint32_t>(sd->host.blas.size());
+  in.tlas_node_count = static_cast<uint32_t>(sd->host.tlas.size());
+  in.light_node_count = static_cast<uint32_t>(sd->host.light_bvh.size());
+  in.device_bytes = sd->arena.size;
+  in.tag = sd->tag;
+  // the device holds the geometry now
+  HostScene& h = sd->host;
+  std::vector<BvhNode>().swap(h.blas);
+  std::vector<float>().swap(h.tris);
+  std::vector<uint32_t>().swap(h.tri_vidx);
+  std::vector<float>().swap(h.vnormal);
+  *out = reinterpret_cast<cg_scene_t>(sd.release());
+  return CG_OK;
+}
+
+CG_API int cg_scene_destroy(cg_scene_t scene) {
+  if (!scene) return CG_OK;
+  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+  {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (g_env) {
+      cudaStreamSynchronize(g_env->stream);
+      g_env->dropGraphsFor(s->tag);
+    }
+  }
+  delete s;
+  return CG_OK;
+}
+
+CG_API int cg_scene_get_info(cg_scene_t scene, cg_scene_info* out) {
+  if (!scene || !out) return fail(CG_E_INVALID, "null argument");
+  *out = reinterpret_cast<SceneDev*>(scene)->info;
+  return CG_OK;
+}
+
+CG_API int cg_scene_read_emissive(cg_scene_t scene, cg_emissive_prim* prims, cg_alias_entry* alias,
+                                  uint32_t capacity, uint32_t* count) {
+  if (!scene) return fail(CG_E_INVALID, "scene is null");
+  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+  const uint32_t n = s->info.emissive_count;
+  if (count) *count = n;
+  if (n == 0 || (!prims && !alias)) return CG_OK;  // count query
+  if (capacity < n) return fail(CG_E_INVALID, "capacity below the emissive count");
+  const char* base = static_cast<const char*>(s->arena.base);
+  if (prims)
+    CG_CUDA(cudaMemcpy(prims, base + s->eprim_off, n * sizeof(cg_emissive_prim),
+                       cudaMemcpyDeviceToHost));
+  if (alias)
+    CG_CUDA(cudaMemcpy(alias, base + s->alias_off, n * sizeof(cg_alias_entry),
+                       cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
+
+CG_API int cg_alias_build(const double* weights, uint32_t count, cg_alias_entry* out) {
+  if (count && (!weights || !out)) return fail(CG_E_INVALID, "null argument");
+  buildAliasTable(weights, count, out);
+  return CG_OK;
+}
+
+CG_API int cg_view(cg_scene_t scene, const cg_camera* camera) {
+  if (!scene || !camera) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  Env& env = *g_env;
+  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+  CG_CUDA(cudaSetDevice(env.device));
+  // FrameHistory::NextIteration (src/wgpu/frame_history.h:12-23)
+  const bool same = env.has_prev && env.prev_tag == s->tag &&
+                    camera->position[0] == env.prev_cam.position[0] &&
+                    camera->position[1] == env.prev_cam.position[1] &&
+                    camera->position[2] == env.prev_cam.position[2] &&
+                    camera->direction[0] == env.prev_cam.direction[0] &&
+                    camera->direction[1] == env.prev_cam.direction[1] &&
+                    camera->direction[2] == env.prev_cam.direction[2] &&
+                    camera->viewport[0] == env.prev_cam.viewport[0] &&
+                    camera->viewport[1] == env.prev_cam.viewport[1];
+  uint32_t iter;
+  if (!same) {
+    env.has_prev = true;
+    env.prev_tag = s->tag;
+    env.prev_cam = *camera;
+    env.frame_count = 1;
+    iter = 0;
+  } else {
+    iter = env.frame_count++;
+  }
+  std::vector<ViewDev> views(1);
+  ViewDev& v = views[0];
+  std::memset(&v, 0, sizeof(v));
+  cameraBasis(*camera, v);
+  v.width = env.conf.render_width;
+  v.height = env.conf.render_height;
+  v.spp = env.conf.sample_count;
+  v.seed = env.seed;
+  v.frame = iter;
+  v.sample_weight = 1.0f / static_cast<float>(iter + 1u);
+  v.pixel_base = 0;
+  v.pixel_count = v.width * v.height;
+  v.film = static_cast<float4*>(env.film);
+  v.rgba = static_cast<uchar4*>(env.rgba);
+  layoutViews(views);
+  const Caps caps = capsOf(env.conf);
+  int rc = env.ensureWave(env.tuning.queue_capacity);
+  if (rc != CG_OK) return rc;
+  rc = env.beginStats(env.stream);
+  if (rc != CG_OK) return rc;
+  rc = env.uploadViews(views, env.stream);
+  if (rc != CG_OK) return rc;
+  RenderRecord rec;
+  CG_CUDA(cudaEventRecord(env.ev0, env.stream));
+  rc = env.enqueueViews(*s, views, static_cast<const ViewDev*>(env.views_dev), caps, env.stream, rec);
+  if (rc != CG_OK) return rc;
+  CG_CUDA(cudaEventRecord(env.ev1, env.stream));
+  CG_CUDA(cudaGetLastError());
+  CG_CUDA(cudaEventSynchronize(env.ev1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, env.ev0, env.ev1);
+  return env.endStats(env.stream, rec, ms);
+}
+
+CG_API int cg_film_read(void* host, size_t bytes, int format) {
+  if (!host) return fail(CG_E_INVALID, "host is null");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  Env& env = *g_env;
+  const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
+  CG_CUDA(cudaSetDevice(env.device));
+  if (format == CG_FILM_RGBA8) {
+    if (bytes < npx * 4) return fail(CG_E_INVALID, "buffer too small for RGBA8");
+    CG_CUDA(cudaMemcpyAsync(host, env.rgba, npx * 4, cudaMemcpyDeviceToHost, env.stream));
+    CG_CUDA(cudaStreamSynchronize(env.stream));
+    return CG_OK;
+  }
+  if (format != CG_FILM_XYZ32F && format != CG_FILM_RGB32F)
+    return fail(CG_E_INVALID, "unknown film format");
+  if (bytes < npx * 12) return fail(CG_E_INVALID, "buffer too small for 3 floats per pixel");
+  // strided copy: 12 of every 16 bytes per pixel
+  CG_CUDA(cudaMemcpy2DAsync(host, 12, env.film, 16, 12, npx, cudaMemcpyDeviceToHost, env.stream));
+  CG_CUDA(cudaStreamSynchronize(env.stream));
+  if (format == CG_FILM_RGB32F) {
+    float* o = static_cast<float*>(host);
+    for (size_t i = 0; i < npx; ++i) {  // xyz_to_srgb of physics/srgb.wesl:6-10
+      const float X = o[3 * i], Y = o[3 * i + 1], Z = o[3 * i + 2];
+      o[3 * i] = (2.36461385f * X + -0.89654057f * Y) + -0.46807328f * Z;
+      o[3 * i + 1] = (-0.51516621f * X + 1.4264081f * Y) + 0.0887581f * Z;
+      o[3 * i + 2] = (0.0052037f * X + -0.01440816f * Y) + 1.00920446f * Z;
+    }
+  }
+  return CG_OK;
+}
+
+CG_API int cg_film_frames(uint32_t* frames) {
+  if (!frames) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  *frames = g_env->has_prev ? g_env->frame_count : 0u;
+  return CG_OK;
+}
+
+CG_API int cg_last_stats(cg_stats* out) {
+  if (!out) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  *out = g_env->last;
+  return CG_OK;
+}
+
+CG_API int cg_set_counting(int enable) {
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  g_env->counting = enable != 0;
+  g_env->dropAllGraphs();
+  return CG_OK;
+}
+
+CG_API int cg_set_profiling(int enable) {
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  g_env->profiling = enable != 0;
+  g_env->prof = cg_profile{};
+  return CG_OK;
+}
+
+CG_API int cg_profile_read(cg_profile* out) {
+  if (!out) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  *out = g_env->prof;
+  g_env->prof = cg_profile{};
+  return CG_OK;
+}
+
+CG_API int cg_set_seed(uint32_t seed) {
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  g_env->seed = seed;
+  return CG_OK;
+}
+
+CG_API int cg_set_tuning(const cg_tuning* t) {
+  if (!t) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  auto okBlock = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 1024 && b % 32 == 0); };
+  if (!okBlock(t->extend_block) || !okBlock(t->shade_block))
+    return fail(CG_E_INVALID, "block sizes must be multiples of 32 in [32, 1024]");
+  if (t->queue_capacity && (t->queue_capacity < 4096 || t->queue_capacity > (1u << 28)))
+    return fail(CG_E_INVALID, "queue capacity must be in [4096, 2^28]");
+  if (t->queue_capacity) g_env->tuning.queue_capacity = t->queue_capacity;
+  if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
+  if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
+  g_env->tuning.use_graph = t->use_graph;
+  g_env->dropAllGraphs();
+  return CG_OK;
+}
+
+CG_API int cg_get_tuning(cg_tuning* out) {
+  if (!out) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  *out = g_env->tuning;
+  return CG_OK;
+}
+
+CG_API int cg_trace_closest(cg_scene_t scene, const float* rays, uint32_t n, cg_hit* hits) {
+  if (!scene || (n && (!rays || !hits))) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  if (n == 0) return CG_OK;
+  Env& env = *g_env;
+  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+  CG_CUDA(cudaSetDevice(env.device));
+  DeviceArena a;
+  const size_t rb = size_t(n) * 32, ob = size_t(n) * 16;
+  int rc = a.alloc(align256(rb) + 2 * align256(ob) + 256);
+  if (rc != CG_OK) return rc;
+  char* p = static_cast<char*>(a.base);
+  float4* d_rays = reinterpret_cast<float4*>(p);
+  float4* d_tuv = reinterpret_cast<float4*>(p + align256(rb));
+  int4* d_ids = reinterpret_cast<int4*>(p + align256(rb) + align256(ob));
+  uint32_t* d_status = reinterpret_cast<uint32_t*>(p + align256(rb) + 2 * align256(ob));
+  CG_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, env.stream));
+  CG_CUDA(cudaMemsetAsync(d_status, 0, 4, env.stream));
+  launchTraceClosest(s->view, d_rays, n, d_tuv, d_ids, d_status, env.stream);
+  CG_CUDA(cudaGetLastError());
+  std::vector<float4> tuv(n);
+  std::vector<int4> ids(n);
+  uint32_t status = 0;
+  CG_CUDA(cudaMemcpyAsync(tuv.data(), d_tuv, ob, cudaMemcpyDeviceToHost, env.stream));
+  CG_CUDA(cudaMemcpyAsync(ids.data(), d_ids, ob, cudaMemcpyDeviceToHost, env.stream));
+  CG_CUDA(cudaMemcpyAsync(&status, d_status, 4, cudaMemcpyDeviceToHost, env.stream));
+  CG_CUDA(cudaStreamSynchronize(env.stream));
+  if (status) return fail(CG_E_DEVICE, "traversal stack overflow in k_trace_closest");
+  for (uint32_t i = 0; i < n; ++i) {
+    cg_hit h{};
+    h.t = tuv[i].x;
+    h.u = tuv[i].y;
+    h.v = tuv[i].z;
+    h.instance = ids[i].x;
+    h.triangle = ids[i].y;
+    hits[i] = h;
+  }
+  return CG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+// cg_api_internal.h — host-side state shared by the C ABI implementation
+// files (cg_api.cu, cg_batch.cu, cg_server.cu).
+#ifndef CG_API_INTERNAL_H_
+#define CG_API_INTERNAL_H_
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cg_cuda.h"
+#include "cg_kernels.h"
+#include "cg_scene.h"
+
+namespace cg {
+
+extern thread_local std::string tl_error;
+int fail(int code, const std::string& msg);
+int cudaFail(cudaError_t e, const char* what);
+
+#define CG_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cudaFail(e_, #call); \
+  } while (0)
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct DeviceArena {
+  void* base = nullptr;
+  size_t size = 0;
+  int alloc(size_t bytes);
+  void release();
+  DeviceArena() = default;
+  DeviceArena(const DeviceArena&) = delete;
+  DeviceArena& operator=(const DeviceArena&) = delete;
+  ~DeviceArena() { release(); }
+};
+
+// An uploaded scene (cg_scene_t).  Immutable after cg_scene_create.
+struct SceneDev {
+  HostScene host;     // packing result; big arrays are dropped after upload
+  DeviceArena arena;
+  SceneView view;
+  size_t eprim_off = 0, alias_off = 0;
+  uint32_t max_lobes = 1;
+  uint64_t tag = 0;
+  cg_scene_info info{};
+};
+
+int uploadScene(const HostScene& h, SceneDev& s);
+
+struct LevelPlan {
+  uint32_t levels = 0;      // depths that can hold rays
+  bool shadow[64] = {};     // depths that can draw a light sample
+  uint64_t max_product = 1; // most rays one sample can have at one depth
+};
+LevelPlan planLevels(const Caps& caps, uint32_t max_lobes);
+Caps capsOf(const cg_conf& c);
+void cameraBasis(const cg_camera& cam, ViewDev& v);
+// Fills the views' global pixel / sample offsets from pixel_count and spp.
+void layoutViews(std::vector<ViewDev>& views);
+
+struct RenderRecord {
+  uint64_t samples = 0;
+  uint32_t chunks = 0;
+  uint32_t launches = 0;
+};
+
+// Device resources of one launch stream: wavelength tables, ray queues and
+// the launch shape.  The View() environment and each server own one.
+struct Renderer {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float* wl_tree = nullptr;
+  float* wl_const = nullptr;
+  bool counting = false;
+  cg_tuning tuning{16u << 20, 128u, 128u, 1u};
+  DeviceArena wave_arena;
+  WaveBuffers wave{};
+
+  int init(int dev);
+  int ensureWave(uint32_t capacity);
+  // Samples one chunk may hold for this scene and caps (whole trees fit the
+  // queues).
+  uint32_t chunkSamples(const SceneDev& scene, const Caps& caps) const;
+  // Enqueues the chunked wavefront over `views` (laid out by layoutViews; the
+  // same table already on the device at `table`).  No host<->device copies
+  // and no synchronisation: the sequence can be captured into a CUDA graph.
+  int enqueueViews(const SceneDev& scene, const std::vector<ViewDev>& views, const ViewDev* table,
+                   const Caps& caps, cudaStream_t s, RenderRecord& rec);
+  // Enqueues one chunk covering all of `views` (their samples must fit).
+  void enqueueChunk(const SceneDev& scene, uint32_t view_count, const ViewDev* table,
+                    const ChunkDesc& ch, const Caps& caps, cudaStream_t s, RenderRecord& rec);
+  int beginStats(cudaStream_t s);
+  int readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_stats& out);
+
+  // Per-kernel CUDA-event timing (off by default; never inside a capture).
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;  // pairs
+  std::vector<int> prof_kind;
+  size_t prof_used = 0;
+  cg_profile prof{};
+  void profBegin(int kind, cudaStream_t s);
+  void profEnd(cudaStream_t s);
+  void profCollect();  // after the stream is synchronised
+  ~Renderer();
+};
+
+// A captured batch: the graph replays the whole chunk sequence of one
+// (scene, views) pair into the films it was captured with.
+struct BatchGraph {
+  uint64_t scene_tag = 0;
+  std::vector<cg_view_desc> views;
+  cudaGraphExec_t exec = nullptr;
+  DeviceArena films;        // float4 films, rgba8 films, then the view table
+  std::vector<size_t> film_off, rgba_off;
+  size_t table_off = 0;
+  RenderRecord rec;
+  ~BatchGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+// The process-global environment (the reference's global::env,
+// src/global.h:14): the View() film and its frame history.
+struct Env : Renderer {
+  cg_conf conf{};
+  void* film = nullptr;   // float4 per pixel
+  void* rgba = nullptr;   // uchar4 per pixel
+  // FrameHistory (src/wgpu/frame_history.h)
+  bool has_prev = false;
+  uint64_t prev_tag = 0;
+  cg_camera prev_cam{};
+  uint32_t frame_count = 0;
+  uint32_t seed = 0;
+  void* views_dev = nullptr;
+  size_t view_cap = 0;
+  cg_stats last{};
+  std::vector<std::unique_ptr<BatchGraph>> graphs;
+
+  int uploadViews(const std::vector<ViewDev>& views, cudaStream_t s);
+  int endStats(cudaStream_t s, const RenderRecord& rec, float ms) {
+    return readStats(s, rec, ms, last);
+  }
+  void dropGraphsFor(uint64_t tag);
+  void dropAllGraphs();
+  ~Env();
+};
+
+extern Env* g_env;
+extern std::mutex g_env_mu;
+
+}  // namespace cg
+
+#endif

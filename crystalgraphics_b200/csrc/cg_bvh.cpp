@@ -1,0 +1,268 @@
+// cg_bvh.cpp — binned-SAH BVH builder for the device BvhNode layout.
+#include "cg_bvh.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+namespace cg {
+namespace {
+
+constexpr float kInf = std::numeric_limits<float>::infinity();
+
+inline void boxReset(Box& b) {
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = kInf;
+    b.hi[a] = -kInf;
+  }
+}
+inline void boxGrow(Box& b, const Box& o) {
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = std::min(b.lo[a], o.lo[a]);
+    b.hi[a] = std::max(b.hi[a], o.hi[a]);
+  }
+}
+inline void boxGrowPt(Box& b, const float* p) {
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = std::min(b.lo[a], p[a]);
+    b.hi[a] = std::max(b.hi[a], p[a]);
+  }
+}
+inline float boxArea(const Box& b) {
+  float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+  if (dx < 0 || dy < 0 || dz < 0) return 0.0f;
+  return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+struct TmpNode {
+  Box box;
+  int32_t left = -1, right = -1;  // TmpNode indices (inner)
+  uint32_t first = 0, count = 0;  // leaf range in order[]
+};
+
+struct Builder {
+  const std::vector<Box>& boxes;
+  const BvhBuildOptions& opt;
+  std::vector<float> centers;  // 3 per primitive
+  std::vector<uint32_t>& order;
+  uint32_t order_base;
+  std::vector<TmpNode> tmp;
+  uint32_t max_depth = 0;
+
+  Builder(const std::vector<Box>& b, const BvhBuildOptions& o, std::vector<uint32_t>& ord)
+      : boxes(b), opt(o), order(ord), order_base(static_cast<uint32_t>(ord.size())) {}
+
+  // Splits order[begin, end) in place; returns the split position or `end`
+  // to make a leaf.
+  uint32_t split(uint32_t begin, uint32_t end, const Box& bounds) {
+    const uint32_t n = end - begin;
+    if (n <= 1) return end;
+    Box cb;
+    boxReset(cb);
+    for (uint32_t i = begin; i < end; ++i) boxGrowPt(cb, &centers[3 * order[i]]);
+    const uint32_t B = opt.bins;
+    float best_cost = kInf;
+    int best_axis = -1;
+    uint32_t best_bin = 0;
+    std::vector<Box> bin_box(B);
+    std::vector<uint32_t> bin_cnt(B);
+    std::vector<float> right_area(B);
+    std::vector<uint32_t> right_cnt(B);
+    for (int a = 0; a < 3; ++a) {
+      float ext = cb.hi[a] - cb.lo[a];
+      if (!(ext > 0.0f)) continue;
+      float scale = static_cast<float>(B) / ext;
+      for (uint32_t k = 0; k < B; ++k) {
+        boxReset(bin_box[k]);
+        bin_cnt[k] = 0;
+      }
+      for (uint32_t i = begin; i < end; ++i) {
+        uint32_t p = order[i];
+        uint32_t k = static_cast<uint32_t>((centers[3 * p + a] - cb.lo[a]) * scale);
+        if (k >= B) k = B - 1;
+        boxGrow(bin_box[k], boxes[p]);
+        ++bin_cnt[k];
+      }
+      Box acc;
+      boxReset(acc);
+      uint32_t cnt = 0;
+      for (uint32_t k = B - 1; k > 0; --k) {
+        boxGrow(acc, bin_box[k]);
+        cnt += bin_cnt[k];
+        right_area[k] = boxArea(acc);
+        right_cnt[k] = cnt;
+      }
+      boxReset(acc);
+      cnt = 0;
+      for (uint32_t k = 0; k + 1 < B; ++k) {
+        boxGrow(acc, bin_box[k]);
+        cnt += bin_cnt[k];
+        if (cnt == 0 || right_cnt[k + 1] == 0) continue;
+        float c = boxArea(acc) * static_cast<float>(cnt) +
+                  right_area[k + 1] * static_cast<float>(right_cnt[k + 1]);
+        if (c < best_cost) {
+          best_cost = c;
+          best_axis = a;
+          best_bin = k;
+        }
+      }
+    }
+    float parent_area = boxArea(bounds);
+    float leaf_cost = static_cast<float>(n) * opt.intersect_cost;
+    float split_cost = parent_area > 0.0f
+                           ? opt.traversal_cost + opt.intersect_cost * best_cost / parent_area
+                           : kInf;
+    if (best_axis < 0) {
+      // all centroids coincide: median split by index if the node is too big
+      if (n <= opt.max_leaf) return end;
+      return begin + n / 2;
+    }
+    if (n <= opt.max_leaf && leaf_cost <= split_cost) return end;
+    const int a = best_axis;
+    const float scale = static_cast<float>(B) / (cb.hi[a] - cb.lo[a]);
+    auto mid = std::partition(order.begin() + begin, order.begin() + end, [&](uint32_t p) {
+      uint32_t k = static_cast<uint32_t>((centers[3 * p + a] - cb.lo[a]) * scale);
+      if (k >= B) k = B - 1;
+      return k <= best_bin;
+    });
+    uint32_t m = static_cast<uint32_t>(mid - order.begin());
+    if (m == begin || m == end) m = begin + n / 2;
+    return m;
+  }
+
+  void run() {
+    const uint32_t N = static_cast<uint32_t>(boxes.size());
+    centers.resize(3 * size_t(N));
+    for (uint32_t i = 0; i < N; ++i)
+      for (int a = 0; a < 3; ++a) centers[3 * i + a] = 0.5f * (boxes[i].lo[a] + boxes[i].hi[a]);
+    for (uint32_t i = 0; i < N; ++i) order.push_back(i);
+    tmp.reserve(2 * size_t(N) + 1);
+    struct Work {
+      int32_t node;
+      uint32_t begin, end, depth;
+    };
+    std::vector<Work> stack;
+    tmp.emplace_back();
+    stack.push_back({0, order_base, order_base + N, 1});
+    while (!stack.empty()) {
+      Work w = stack.back();
+      stack.pop_back();
+      max_depth = std::max(max_depth, w.depth);
+      Box bounds;
+      boxReset(bounds);
+      for (uint32_t i = w.begin; i < w.end; ++i) boxGrow(bounds, boxes[order[i]]);
+      tmp[w.node].box = bounds;
+      // split works on local order indices; order[] holds local primitive ids
+      uint32_t m = (w.end - w.begin <= 1) ? w.end : split(w.begin, w.end, bounds);
+      if (m == w.end) {
+        tmp[w.node].first = w.begin;
+        tmp[w.node].count = w.end - w.begin;
+        continue;
+      }
+      int32_t l = static_cast<int32_t>(tmp.size());
+      tmp.emplace_back();
+      tmp.emplace_back();
+      tmp[w.node].left = l;
+      tmp[w.node].right = l + 1;
+      stack.push_back({l + 1, m, w.end, w.depth + 1});
+      stack.push_back({l, w.begin, m, w.depth + 1});
+    }
+  }
+};
+
+void setChild(BvhNode& n, int which, const Box& b, int32_t link, uint32_t cnt) {
+  if (which == 0) {
+    n.c0lx = b.lo[0]; n.c0hx = b.hi[0]; n.c0ly = b.lo[1]; n.c0hy = b.hi[1];
+    n.c0lz = b.lo[2]; n.c0hz = b.hi[2];
+    n.child0 = link;
+    n.cnt0 = cnt;
+  } else {
+    n.c1lx = b.lo[0]; n.c1hx = b.hi[0]; n.c1ly = b.lo[1]; n.c1hy = b.hi[1];
+    n.c1lz = b.lo[2]; n.c1hz = b.hi[2];
+    n.child1 = link;
+    n.cnt1 = cnt;
+  }
+}
+
+}  // namespace
+
+void padBox(Box& b) {
+  for (int a = 0; a < 3; ++a) {
+    float m = std::max(std::fabs(b.lo[a]), std::fabs(b.hi[a]));
+    float pad = m * 1.0e-5f + 1.0e-5f;
+    b.lo[a] -= pad;
+    b.hi[a] += pad;
+  }
+}
+
+uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt, uint32_t prim_base,
+                  std::vector<BvhNode>& nodes, std::vector<uint32_t>& order,
+                  uint32_t* depth_out) {
+  const uint32_t base = static_cast<uint32_t>(nodes.size());
+  const size_t order_base = order.size();
+  Builder b(boxes, opt, order);
+  if (!boxes.empty()) b.run();
+  if (depth_out) *depth_out = b.max_depth;
+  // Emit: every inner TmpNode becomes one BvhNode; DFS order keeps siblings'
+  // subtrees contiguous.  A root that is a leaf gets a node with one child.
+  // An absent child gets a point box at 1e30: slab tests reorder bounds, so an
+  // inverted box would still be entered; a box that far is entered only
+  // beyond any t the traversal accepts (hits are below 1e6).
+  Box empty;
+  for (int a = 0; a < 3; ++a) {
+    empty.lo[a] = 1e30f;
+    empty.hi[a] = 1e30f;
+  }
+  auto leafLink = [&](const TmpNode& t) {
+    // order[] entries from order_base are local ids; leaves index order[]
+    return leafLinkOf(prim_base + (t.first - static_cast<uint32_t>(order_base)), t.count);
+  };
+  if (boxes.empty()) {
+    BvhNode n{};
+    setChild(n, 0, empty, leafLinkOf(prim_base, 0), 0);
+    setChild(n, 1, empty, leafLinkOf(prim_base, 0), 0);
+    nodes.push_back(n);
+    return base;
+  }
+  std::vector<int32_t> out_index(b.tmp.size(), -1);
+  // assign output indices in DFS preorder over inner nodes
+  std::vector<int32_t> st{0};
+  uint32_t next = base;
+  std::vector<int32_t> inner_order;
+  while (!st.empty()) {
+    int32_t t = st.back();
+    st.pop_back();
+    if (b.tmp[t].left < 0) continue;
+    out_index[t] = static_cast<int32_t>(next++);
+    inner_order.push_back(t);
+    st.push_back(b.tmp[t].right);
+    st.push_back(b.tmp[t].left);
+  }
+  if (inner_order.empty()) {  // root is a leaf
+    BvhNode n{};
+    Box bx = b.tmp[0].box;
+    padBox(bx);
+    setChild(n, 0, bx, leafLink(b.tmp[0]), b.tmp[0].count);
+    setChild(n, 1, empty, leafLink(b.tmp[0]), 0);
+    nodes.push_back(n);
+    return base;
+  }
+  nodes.resize(next);
+  for (int32_t t : inner_order) {
+    BvhNode n{};
+    for (int c = 0; c < 2; ++c) {
+      const TmpNode& ch = b.tmp[c == 0 ? b.tmp[t].left : b.tmp[t].right];
+      int32_t ci = c == 0 ? b.tmp[t].left : b.tmp[t].right;
+      Box bx = ch.box;
+      padBox(bx);
+      if (ch.left >= 0)
+        setChild(n, c, bx, out_index[ci], 0);
+      else
+        setChild(n, c, bx, leafLink(ch), ch.count);
+    }
+    nodes[out_index[t]] = n;
+  }
+  return base;
+}
+
+}  // namespace cg

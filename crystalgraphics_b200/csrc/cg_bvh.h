@@ -1,0 +1,52 @@
+// cg_bvh.h — host BVH builder (binned SAH) emitting the device BvhNode layout.
+//
+// The reference builds median-split BVH2s with one triangle pair per leaf
+// (src/pathtracing/blas.h:112-194) and a median-split TLAS
+// (src/pathtracing/tlas.h:98-140).  The closest hit does not depend on the
+// tree (only exact ties can resolve differently), so this backend builds
+// surface-area-heuristic trees instead, which visit fewer nodes per ray.
+#ifndef CG_BVH_H_
+#define CG_BVH_H_
+
+#include <cstdint>
+#include <vector>
+
+#include "cg_types.h"
+
+namespace cg {
+
+struct Box {
+  float lo[3], hi[3];
+};
+
+struct BvhBuildOptions {
+  uint32_t max_leaf = 4;      // primitives per leaf at most
+  uint32_t bins = 16;         // SAH bins per axis
+  float traversal_cost = 1.0f;
+  float intersect_cost = 1.0f;
+};
+
+// Builds a BVH over `boxes`.  Appends nodes to `nodes` (child indices are
+// absolute, offset by nodes.size() at entry) and returns the root index.
+// `order` receives the primitive permutation: leaf ranges index `order`,
+// offset by `prim_base` (the caller's global primitive offset).
+uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt,
+                  uint32_t prim_base, std::vector<BvhNode>& nodes,
+                  std::vector<uint32_t>& order, uint32_t* depth_out = nullptr);
+
+// Leaf links: ~((first << 3) | count), count <= 7 (so the values INT_MIN and
+// INT_MIN + 1, i.e. count 7 and 6 with first = 2^28 - 1, never occur and
+// serve as traversal markers).  first < 2^28.
+inline int32_t leafLinkOf(uint32_t first, uint32_t count) {
+  return static_cast<int32_t>(~((first << 3) | count));
+}
+inline uint32_t leafFirst(int32_t link) { return static_cast<uint32_t>(~link) >> 3; }
+inline uint32_t leafCount(int32_t link) { return static_cast<uint32_t>(~link) & 7u; }
+
+// Enlarges a box by a small margin so slab tests computed with rounding
+// never reject a primitive that lies on the box boundary.
+void padBox(Box& b);
+
+}  // namespace cg
+
+#endif

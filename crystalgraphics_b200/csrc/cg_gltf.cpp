@@ -1,0 +1,566 @@
+// cg_gltf.cpp — glTF 2.0 loader for LoadScene(path).
+//
+// The reference loads glTF through cgltf (src/scene.cpp:829-1003); cgltf is
+// not available here, so this is a self-contained reader of the subset the
+// path tracer consumes, with the reference's conventions:
+//   - material 0 is the default material, glTF material i becomes i + 1, a
+//     primitive without a material uses 0 (scene.cpp:869-872, 952-956);
+//   - the default material is glTF's defaults (scene.cpp:659-690);
+//   - POSITION / NORMAL / TEXCOORD_0 / TEXCOORD_1 and indices per primitive,
+//     indices made absolute (scene.cpp:876-967); a primitive without indices
+//     contributes no triangles;
+//   - one instance per (node, mesh primitive) in depth-first node order,
+//     node matrix or TRS (scene.cpp:972-995);
+//   - the y-up glTF world is rotated by +90 degrees about x to z-up
+//     (scene.cpp:1000).
+// Supported: .gltf with external .bin or base64 data URIs, and .glb.
+// Material extensions read: KHR_materials_emissive_strength, _ior,
+// _transmission, _volume (thickness), _dispersion.  Textured materials are
+// rejected by the scene packer.
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/cg_cuda.h"
+#include "cg_api_internal.h"
+
+namespace cg {
+namespace {
+
+// ---- minimal JSON -----------------------------------------------------------
+struct Json {
+  enum Kind { Null, Bool, Num, Str, Arr, Obj } kind = Null;
+  bool b = false;
+  double n = 0.0;
+  std::string s;
+  std::vector<Json> a;
+  std::map<std::string, Json> o;
+
+  const Json* get(const std::string& k) const {
+    if (kind != Obj) return nullptr;
+    auto it = o.find(k);
+    return it == o.end() ? nullptr : &it->second;
+  }
+  double num(const std::string& k, double def) const {
+    const Json* j = get(k);
+    return (j && j->kind == Num) ? j->n : def;
+  }
+  int64_t integer(const std::string& k, int64_t def) const {
+    const Json* j = get(k);
+    return (j && j->kind == Num) ? static_cast<int64_t>(j->n) : def;
+  }
+};
+
+struct Parser {
+  const char* p;
+  const char* end;
+  std::string err;
+
+  void ws() {
+    while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
+  }
+  bool parse(Json& out) {
+    ws();
+    if (p >= end) return fail("unexpected end");
+    char c = *p;
+    if (c == '{') return object(out);
+    if (c == '[') return array(out);
+    if (c == '"') {
+      out.kind = Json::Str;
+      return string(out.s);
+    }
+    if (c == 't' || c == 'f' || c == 'n') return literal(out);
+    return number(out);
+  }
+  bool fail(const std::string& m) {
+    if (err.empty()) err = m;
+    return false;
+  }
+  bool literal(Json& out) {
+    auto match = [&](const char* w) {
+      size_t n = std::strlen(w);
+      if (size_t(end - p) >= n && std::strncmp(p, w, n) == 0) {
+        p += n;
+        return true;
+      }
+      return false;
+    };
+    if (match("true")) {
+      out.kind = Json::Bool;
+      out.b = true;
+      return true;
+    }
+    if (match("false")) {
+      out.kind = Json::Bool;
+      out.b = false;
+      return true;
+    }
+    if (match("null")) {
+      out.kind = Json::Null;
+      return true;
+    }
+    return fail("bad literal");
+  }
+  bool number(Json& out) {
+    char* e = nullptr;
+    out.n = std::strtod(p, &e);
+    if (e == p) return fail("bad number");
+    p = e;
+    out.kind = Json::Num;
+    return true;
+  }
+  bool string(std::string& s) {
+    ++p;  // opening quote
+    while (p < end && *p != '"') {
+      if (*p == '\\') {
+        ++p;
+        if (p >= end) return fail("bad escape");
+        char c = *p++;
+        switch (c) {
+          case 'n': s += '\n'; break;
+          case 't': s += '\t'; break;
+          case 'r': s += '\r'; break;
+          case 'b': s += '\b'; break;
+          case 'f': s += '\f'; break;
+          case 'u': {
+            if (end - p < 4) return fail("bad unicode escape");
+            unsigned v = static_cast<unsigned>(std::stoul(std::string(p, 4), nullptr, 16));
+            p += 4;
+            if (v < 0x80) {
+              s += static_cast<char>(v);
+            } else if (v < 0x800) {
+              s += static_cast<char>(0xC0 | (v >> 6));
+              s += static_cast<char>(0x80 | (v & 0x3F));
+            } else {
+              s += static_cast<char>(0xE0 | (v >> 12));
+              s += static_cast<char>(0x80 | ((v >> 6) & 0x3F));
+              s += static_cast<char>(0x80 | (v & 0x3F));
+            }
+            break;
+          }
+          default: s += c;
+        }
+      } else {
+        s += *p++;
+      }
+    }
+    if (p >= end) return fail("unterminated string");
+    ++p;
+    return true;
+  }
+  bool array(Json& out) {
+    out.kind = Json::Arr;
+    ++p;
+    ws();
+    if (p < end && *p == ']') {
+      ++p;
+      return true;
+    }
+    while (true) {
+      out.a.emplace_back();
+      if (!parse(out.a.back())) return false;
+      ws();
+      if (p < end && *p == ',') {
+        ++p;
+        continue;
+      }
+      if (p < end && *p == ']') {
+        ++p;
+        return true;
+      }
+      return fail("expected , or ]");
+    }
+  }
+  bool object(Json& out) {
+    out.kind = Json::Obj;
+    ++p;
+    ws();
+    if (p < end && *p == '}') {
+      ++p;
+      return true;
+    }
+    while (true) {
+      ws();
+      if (p >= end || *p != '"') return fail("expected key");
+      std::string key;
+      if (!string(key)) return false;
+      ws();
+      if (p >= end || *p != ':') return fail("expected :");
+      ++p;
+      if (!parse(out.o[key])) return false;
+      ws();
+      if (p < end && *p == ',') {
+        ++p;
+        continue;
+      }
+      if (p < end && *p == '}') {
+        ++p;
+        return true;
+      }
+      return fail("expected , or }");
+    }
+  }
+};
+
+std::vector<uint8_t> base64(const std::string& in) {
+  auto val = [](char c) -> int {
+    if (c >= 'A' && c <= 'Z') return c - 'A';
+    if (c >= 'a' && c <= 'z') return c - 'a' + 26;
+    if (c >= '0' && c <= '9') return c - '0' + 52;
+    if (c == '+') return 62;
+    if (c == '/') return 63;
+    return -1;
+  };
+  std::vector<uint8_t> out;
+  uint32_t acc = 0;
+  int bits = 0;
+  for (char c : in) {
+    int v = val(c);
+    if (v < 0) continue;
+    acc = (acc << 6) | static_cast<uint32_t>(v);
+    bits += 6;
+    if (bits >= 8) {
+      bits -= 8;
+      out.push_back(static_cast<uint8_t>((acc >> bits) & 0xFF));
+    }
+  }
+  return out;
+}
+
+// column-major 4x4 helpers (glTF convention)
+struct M4 {
+  double m[16];  // column-major
+};
+M4 identity() {
+  M4 r{};
+  for (int i = 0; i < 4; ++i) r.m[i * 5] = 1.0;
+  return r;
+}
+M4 mul(const M4& a, const M4& b) {
+  M4 r{};
+  for (int c = 0; c < 4; ++c)
+    for (int rr = 0; rr < 4; ++rr) {
+      double s = 0;
+      for (int k = 0; k < 4; ++k) s += a.m[k * 4 + rr] * b.m[c * 4 + k];
+      r.m[c * 4 + rr] = s;
+    }
+  return r;
+}
+
+struct Loader {
+  Json doc;
+  std::vector<std::vector<uint8_t>> buffers;
+  std::string dir;
+  std::string err;
+
+  std::vector<cg_vertex> vertices;
+  std::vector<uint32_t> indices;
+  std::vector<cg_mesh> meshes;              // one per glTF mesh primitive
+  std::vector<uint32_t> prim_material;      // per cg_mesh
+  std::vector<std::vector<uint32_t>> mesh_prims;  // glTF mesh -> cg_mesh ids
+  std::vector<cg_instance> instances;
+  std::vector<cg_material> materials;
+
+  bool fail(const std::string& m) {
+    if (err.empty()) err = m;
+    return false;
+  }
+
+  bool loadBuffers(const std::vector<uint8_t>* glb_bin) {
+    const Json* bs = doc.get("buffers");
+    if (!bs) return true;
+    for (size_t i = 0; i < bs->a.size(); ++i) {
+      const Json& b = bs->a[i];
+      const Json* uri = b.get("uri");
+      if (!uri) {
+        if (!glb_bin) return fail("buffer without uri outside a .glb");
+        buffers.push_back(*glb_bin);
+        continue;
+      }
+      const std::string& u = uri->s;
+      if (u.rfind("data:", 0) == 0) {
+        size_t comma = u.find(',');
+        if (comma == std::string::npos) return fail("bad data uri");
+        buffers.push_back(base64(u.substr(comma + 1)));
+        continue;
+      }
+      std::ifstream f(dir + "/" + u, std::ios::binary);
+      if (!f) return fail("cannot open buffer " + u);
+      buffers.emplace_back((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    }
+    return true;
+  }
+
+  // Reads accessor `idx` as `comps` floats per element (or as indices).
+  bool readAccessor(int64_t idx, int comps, std::vector<double>& out, size_t& count) {
+    const Json* acc = doc.get("accessors");
+    if (!acc || idx < 0 || size_t(idx) >= acc->a.size()) return fail("bad accessor index");
+    const Json& a = acc->a[idx];
+    if (a.get("sparse")) return fail("sparse accessors are not supported");
+    count = static_cast<size_t>(a.integer("count", 0));
+    const int64_t ctype = a.integer("componentType", 5126);
+    const bool normalized = a.get("normalized") && a.get("normalized")->b;
+    const std::string type = a.get("type") ? a.get("type")->s : "SCALAR";
+    int ncomp = type == "SCALAR" ? 1 : type == "VEC2" ? 2 : type == "VEC3" ? 3 : type == "VEC4" ? 4 : 0;
+    if (ncomp == 0) return fail("unsupported accessor type " + type);
+    int csize = (ctype == 5120 || ctype == 5121) ? 1 : (ctype == 5122 || ctype == 5123) ? 2 : 4;
+    out.assign(count * comps, 0.0);
+    if (!a.get("bufferView")) return true;  // all zeros
+    const Json* bvs = doc.get("bufferViews");
+    const int64_t bvi = a.integer("bufferView", -1);
+    if (!bvs || bvi < 0 || size_t(bvi) >= bvs->a.size()) return fail("bad bufferView");
+    const Json& bv = bvs->a[bvi];
+    const int64_t bi = bv.integer("buffer", -1);
+    if (bi < 0 || size_t(bi) >= buffers.size()) return fail("bad buffer index");
+    const std::vector<uint8_t>& buf = buffers[bi];
+    const size_t base = size_t(bv.integer("byteOffset", 0)) + size_t(a.integer("byteOffset", 0));
+    const size_t stride = bv.integer("byteStride", 0) ? size_t(bv.integer("byteStride", 0))
+                                                      : size_t(ncomp * csize);
+    if (count && base + (count - 1) * stride + size_t(ncomp * csize) > buf.size())
+      return fail("accessor exceeds its buffer");
+    for (size_t e = 0; e < count; ++e) {
+      const uint8_t* src = buf.data() + base + e * stride;
+      for (int c = 0; c < std::min(ncomp, comps); ++c) {
+        const uint8_t* q = src + c * csize;
+        double v = 0;
+        switch (ctype) {
+          case 5126: { float f; std::memcpy(&f, q, 4); v = f; break; }
+          case 5125: { uint32_t u; std::memcpy(&u, q, 4); v = u; break; }
+          case 5123: { uint16_t u; std::memcpy(&u, q, 2); v = normalized ? u / 65535.0 : u; break; }
+          case 5121: { uint8_t u = *q; v = normalized ? u / 255.0 : u; break; }
+          case 5122: { int16_t s; std::memcpy(&s, q, 2); v = normalized ? std::max(s / 32767.0, -1.0) : s; break; }
+          case 5120: { int8_t s = static_cast<int8_t>(*q); v = normalized ? std::max(s / 127.0, -1.0) : s; break; }
+          default: return fail("unsupported component type");
+        }
+        out[e * comps + c] = v;
+      }
+    }
+    return true;
+  }
+
+  int32_t textureIndex(const Json* info) {
+    if (!info) return -1;
+    return static_cast<int32_t>(info->integer("index", -1));
+  }
+
+  void loadMaterials() {
+    auto def = [] {
+      cg_material m{};
+      for (int k = 0; k < 4; ++k) m.base_color_factor[k] = 1.0f;
+      m.emissive_strength = 1.0f;
+      m.metallic_factor = 1.0f;
+      m.roughness_factor = 1.0f;
+      m.ior = 1.5f;
+      m.base_color_texture = m.metallic_roughness_texture = m.emissive_texture =
+          m.transmission_texture = -1;
+      return m;
+    };
+    materials.push_back(def());
+    const Json* ms = doc.get("materials");
+    if (!ms) return;
+    for (const Json& mj : ms->a) {
+      cg_material m = def();
+      if (const Json* pbr = mj.get("pbrMetallicRoughness")) {
+        if (const Json* bc = pbr->get("baseColorFactor"))
+          for (size_t k = 0; k < 4 && k < bc->a.size(); ++k)
+            m.base_color_factor[k] = static_cast<float>(bc->a[k].n);
+        m.metallic_factor = static_cast<float>(pbr->num("metallicFactor", 1.0));
+        m.roughness_factor = static_cast<float>(pbr->num("roughnessFactor", 1.0));
+        m.base_color_texture = textureIndex(pbr->get("baseColorTexture"));
+        m.metallic_roughness_texture = textureIndex(pbr->get("metallicRoughnessTexture"));
+      }
+      if (const Json* ef = mj.get("emissiveFactor"))
+        for (size_t k = 0; k < 3 && k < ef->a.size(); ++k)
+          m.emissive_factor[k] = static_cast<float>(ef->a[k].n);
+      m.emissive_texture = textureIndex(mj.get("emissiveTexture"));
+      if (const Json* ext = mj.get("extensions")) {
+        if (const Json* e = ext->get("KHR_materials_emissive_strength"))
+          m.emissive_strength = static_cast<float>(e->num("emissiveStrength", 1.0));
+        if (const Json* e = ext->get("KHR_materials_ior"))
+          m.ior = static_cast<float>(e->num("ior", 1.5));
+        if (const Json* e = ext->get("KHR_materials_dispersion"))
+          m.dispersion = static_cast<float>(e->num("dispersion", 0.0));
+        if (const Json* e = ext->get("KHR_materials_transmission")) {
+          m.transmission_factor = static_cast<float>(e->num("transmissionFactor", 0.0));
+          m.transmission_texture = textureIndex(e->get("transmissionTexture"));
+        }
+        if (const Json* e = ext->get("KHR_materials_volume"))
+          m.thickness_factor = static_cast<float>(e->num("thicknessFactor", 0.0));
+      }
+      materials.push_back(m);
+    }
+  }
+
+  bool loadMeshes() {
+    const Json* ms = doc.get("meshes");
+    if (!ms) return true;
+    for (const Json& mesh : ms->a) {
+      mesh_prims.emplace_back();
+      const Json* prims = mesh.get("primitives");
+      if (!prims) continue;
+      for (const Json& pr : prims->a) {
+        if (pr.integer("mode", 4) != 4) return fail("only triangle primitives are supported");
+        const Json* attrs = pr.get("attributes");
+        if (!attrs || !attrs->get("POSITION")) return fail("primitive without POSITION");
+        std::vector<double> pos, nrm, uv0, uv1, idx;
+        size_t nv = 0, n2 = 0;
+        if (!readAccessor(attrs->integer("POSITION", -1), 3, pos, nv)) return false;
+        const uint32_t voff = static_cast<uint32_t>(vertices.size());
+        vertices.resize(vertices.size() + nv);
+        auto fill = [&](const char* name, int comps, int which) -> bool {
+          if (!attrs->get(name)) return true;
+          std::vector<double> d;
+          if (!readAccessor(attrs->integer(name, -1), comps, d, n2)) return false;
+          for (size_t v = 0; v < std::min(nv, n2); ++v) {
+            cg_vertex& vx = vertices[voff + v];
+            float* dst = which == 0 ? vx.normal : which == 1 ? vx.tex_coord0 : vx.tex_coord1;
+            for (int c = 0; c < comps; ++c) dst[c] = static_cast<float>(d[v * comps + c]);
+          }
+          return true;
+        };
+        for (size_t v = 0; v < nv; ++v)
+          for (int c = 0; c < 3; ++c) vertices[voff + v].position[c] = static_cast<float>(pos[v * 3 + c]);
+        if (!fill("NORMAL", 3, 0) || !fill("TEXCOORD_0", 2, 1) || !fill("TEXCOORD_1", 2, 2))
+          return false;
+        const uint32_t ioff = static_cast<uint32_t>(indices.size());
+        size_t ni = 0;
+        if (pr.get("indices")) {
+          if (!readAccessor(pr.integer("indices", -1), 1, idx, ni)) return false;
+          for (size_t k = 0; k < ni; ++k) {
+            const double iv = idx[k];
+            if (iv < 0 || iv >= double(nv)) return fail("index out of range in a primitive");
+            indices.push_back(static_cast<uint32_t>(iv) + voff);
+          }
+        }
+        cg_mesh m{voff, static_cast<uint32_t>(nv), ioff, static_cast<uint32_t>(ni)};
+        const int64_t mat = pr.integer("material", -1);
+        mesh_prims.back().push_back(static_cast<uint32_t>(meshes.size()));
+        meshes.push_back(m);
+        prim_material.push_back(mat >= 0 ? static_cast<uint32_t>(mat + 1) : 0u);
+      }
+    }
+    return true;
+  }
+
+  M4 nodeTransform(const Json& n) {
+    if (const Json* mj = n.get("matrix")) {
+      M4 r = identity();
+      for (size_t k = 0; k < 16 && k < mj->a.size(); ++k) r.m[k] = mj->a[k].n;
+      return r;
+    }
+    double t[3] = {0, 0, 0}, q[4] = {0, 0, 0, 1}, s[3] = {1, 1, 1};
+    if (const Json* tj = n.get("translation"))
+      for (size_t k = 0; k < 3 && k < tj->a.size(); ++k) t[k] = tj->a[k].n;
+    if (const Json* rj = n.get("rotation"))
+      for (size_t k = 0; k < 4 && k < rj->a.size(); ++k) q[k] = rj->a[k].n;
+    if (const Json* sj = n.get("scale"))
+      for (size_t k = 0; k < 3 && k < sj->a.size(); ++k) s[k] = sj->a[k].n;
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)},
+                            {2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)},
+                            {2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)}};
+    M4 r = identity();
+    for (int c = 0; c < 3; ++c)
+      for (int rr = 0; rr < 3; ++rr) r.m[c * 4 + rr] = R[rr][c] * s[c];
+    for (int rr = 0; rr < 3; ++rr) r.m[12 + rr] = t[rr];
+    return r;
+  }
+
+  bool walk(int64_t node, const M4& parent, int depth) {
+    const Json* ns = doc.get("nodes");
+    if (!ns || node < 0 || size_t(node) >= ns->a.size()) return fail("bad node index");
+    if (depth > 256) return fail("node hierarchy too deep (cycle?)");
+    const Json& n = ns->a[node];
+    const M4 world = mul(parent, nodeTransform(n));
+    const int64_t mesh = n.integer("mesh", -1);
+    if (mesh >= 0) {
+      if (size_t(mesh) >= mesh_prims.size()) return fail("bad mesh index");
+      for (uint32_t pm : mesh_prims[mesh]) {
+        cg_instance in{};
+        for (int rr = 0; rr < 3; ++rr)
+          for (int c = 0; c < 4; ++c) in.world_from_local[rr * 4 + c] = static_cast<float>(world.m[c * 4 + rr]);
+        in.mesh = pm;
+        in.material = prim_material[pm] < materials.size() ? prim_material[pm] : 0u;
+        instances.push_back(in);
+      }
+    }
+    if (const Json* ch = n.get("children"))
+      for (const Json& c : ch->a)
+        if (!walk(static_cast<int64_t>(c.n), world, depth + 1)) return false;
+    return true;
+  }
+
+  bool load(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return fail("cannot open " + path);
+    std::vector<uint8_t> bytes((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    size_t slash = path.find_last_of('/');
+    dir = slash == std::string::npos ? "." : path.substr(0, slash);
+    std::string json;
+    std::vector<uint8_t> bin;
+    bool glb = bytes.size() >= 12 && std::memcmp(bytes.data(), "glTF", 4) == 0;
+    if (glb) {
+      size_t off = 12;
+      while (off + 8 <= bytes.size()) {
+        uint32_t len, type;
+        std::memcpy(&len, &bytes[off], 4);
+        std::memcpy(&type, &bytes[off + 4], 4);
+        if (off + 8 + len > bytes.size()) return fail("truncated .glb chunk");
+        if (type == 0x4E4F534Au) json.assign(reinterpret_cast<char*>(&bytes[off + 8]), len);
+        if (type == 0x004E4942u) bin.assign(bytes.begin() + off + 8, bytes.begin() + off + 8 + len);
+        off += 8 + len;
+      }
+    } else {
+      json.assign(bytes.begin(), bytes.end());
+    }
+    Parser p{json.data(), json.data() + json.size(), {}};
+    if (!p.parse(doc)) return fail("invalid JSON: " + p.err);
+    if (!loadBuffers(glb ? &bin : nullptr)) return false;
+    loadMaterials();
+    if (!loadMeshes()) return false;
+    // root: Rx(+90 deg), glTF y-up -> z-up (scene.cpp:1000)
+    M4 root = identity();
+    root.m[5] = 0.0;   // column 1: (0, 0, 1)
+    root.m[6] = 1.0;
+    root.m[9] = -1.0;  // column 2: (0, -1, 0)
+    root.m[10] = 0.0;
+    const Json* scenes = doc.get("scenes");
+    int64_t sc = doc.integer("scene", 0);
+    if (scenes && !scenes->a.empty()) {
+      if (sc < 0 || size_t(sc) >= scenes->a.size()) sc = 0;
+      if (const Json* nodes = scenes->a[sc].get("nodes"))
+        for (const Json& n : nodes->a)
+          if (!walk(static_cast<int64_t>(n.n), root, 0)) return false;
+    }
+    return true;
+  }
+};
+
+}  // namespace
+}  // namespace cg
+
+using namespace cg;
+
+extern "C" CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out) {
+  if (!path || !out) return fail(CG_E_INVALID, "null argument");
+  *out = nullptr;
+  Loader L;
+  if (!L.load(path)) return fail(CG_E_INVALID, std::string(path) + ": " + L.err);
+  cg_scene_desc d{};
+  d.vertices = L.vertices.data();
+  d.vertex_count = static_cast<uint32_t>(L.vertices.size());
+  d.indices = L.indices.data();
+  d.index_count = static_cast<uint32_t>(L.indices.size());
+  d.meshes = L.meshes.data();
+  d.mesh_count = static_cast<uint32_t>(L.meshes.size());
+  d.instances = L.instances.data();
+  d.instance_count = static_cast<uint32_t>(L.instances.size());
+  d.materials = L.materials.data();
+  d.material_count = static_cast<uint32_t>(L.materials.size());
+  return cg_scene_create(&d, out);
+}

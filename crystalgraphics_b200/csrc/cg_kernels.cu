@@ -1,0 +1,625 @@
+// cg_kernels.cu — the wavefront path tracer (sm_100a).
+//
+// The reference evaluates every camera sample as a depth-first tree inside
+// one thread with a 64-frame private stack (trace.wesl:22-89).  Its result is
+// linear in the children's radiance (backwardPass, shading.wesl:48-53), so
+// here each tree node is a queued ray carrying the product of the transport
+// coefficients above it; emission, environment and light-sample terms are
+// added straight into the sample's radiance slot.  Trees are processed level
+// by level: every level is one extend (closest hit), one shade and one shadow
+// launch over all rays of that depth in the chunk.
+#include "cg_kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <climits>
+
+#include "cg_device.cuh"
+#include "cg_traverse.cuh"
+
+namespace cg {
+namespace {
+
+using namespace dev;
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ V3 ld3(const float* p) { return V3{p[0], p[1], p[2]}; }
+
+// transpose(inv_trans) * vec4(n, 0) (bvh.wesl:110-111)
+__device__ __forceinline__ V3 normalToWorld(const float* m, V3 n) {
+  return {(m[0] * n.x + m[4] * n.y) + m[8] * n.z, (m[1] * n.x + m[5] * n.y) + m[9] * n.z,
+          (m[2] * n.x + m[6] * n.y) + m[10] * n.z};
+}
+
+// ---- view lookup ------------------------------------------------------------
+__device__ __forceinline__ uint32_t findViewBySample(const FrameConst& fc, uint64_t g) {
+  uint32_t lo = 0, hi = fc.view_count;  // last view with sample_offset <= g
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (fc.views[mid].sample_offset <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ uint32_t findViewByPixel(const FrameConst& fc, uint64_t g) {
+  uint32_t lo = 0, hi = fc.view_count;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (fc.views[mid].pixel_offset <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// ---- wavelength tree (physics/wavelength.wesl:24-45) ---------------------------
+__global__ void k_wavelength_tree(float* tree, float* consts) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const float total = xyzMatchSumIntegral(380.0f, 720.0f);
+  if (k == 0) {
+    consts[0] = total;
+    consts[1] = xyzMatchSumIntegral(380.0f, 720.0f) / 3.0f;
+  }
+  if (k >= 65535u) return;
+  // replay the bisection path from the root to node k
+  uint32_t path[16];
+  int depth = 0;
+  for (uint32_t x = k; x > 0; x = (x - 1u) >> 1) path[depth++] = x;
+  float low = 380.0f, high = 720.0f;
+  for (int i = depth - 1; i >= 0; --i) {
+    const uint32_t x = path[i];
+    const uint32_t parent = (x - 1u) >> 1;
+    const float mid = 0.5f * (low + high);
+    if (x == 2u * parent + 1u)
+      high = mid;  // cdf >= target
+    else
+      low = mid;
+  }
+  const float mid = 0.5f * (low + high);
+  tree[k] = xyzMatchSumIntegral(380.0f, mid) / total;
+}
+
+// ---- generate: one primary ray per sample (compute.wesl:32-62, render.wesl) ----
+__global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    wb.counts[0] = ch.sample_count;
+    wb.counts[2] = 0u;
+  }
+  if (i >= ch.sample_count) return;
+  const uint64_t g = ch.sample_begin + i;
+  const ViewDev& v = fc.views[findViewBySample(fc, g)];
+  const uint64_t local = g - v.sample_offset;
+  const uint32_t lp = static_cast<uint32_t>(local / v.spp);
+  const uint32_t k = static_cast<uint32_t>(local - uint64_t(lp) * v.spp);
+  const uint32_t pixel = v.pixel_base + lp;
+  const uint32_t px = pixel % v.width, py = pixel / v.width;
+  const uint32_t key = sampleKey(v.seed, v.frame, pixel, k);
+  Rng wr;
+  seedRng(wr, wavelengthKey(key));
+  const float lambda = sampleWavelengthTree(fc.wl_tree, randFloat(wr));
+  const V3 xyz = xyzMatch(lambda);
+  const float prob = fmaxf((xyz.x + xyz.y + xyz.z) / fc.wl_const[0], 1e-6f);
+  wb.s_L[i] = 0.0f;
+  wb.s_lambda[i] = lambda;
+  wb.s_prob[i] = prob;
+  // cameraRay, rounded per operation like the host restatement
+  const float cx = XS(XM(__fdiv_rn(static_cast<float>(px), static_cast<float>(v.width)), 2.0f), 1.0f);
+  const float cy = XS(XM(__fdiv_rn(static_cast<float>(py), static_cast<float>(v.height)), 2.0f), 1.0f);
+  float d[3];
+  for (int a = 0; a < 3; ++a) d[a] = XA(XA(v.dir[a], XM(cx, v.dx[a])), XM(cy, v.dy[a]));
+  const float len = __fsqrt_rn(XA(XA(XM(d[0], d[0]), XM(d[1], d[1])), XM(d[2], d[2])));
+  wb.ray_o[0][i] = make_float4(v.pos[0], v.pos[1], v.pos[2], 1.0f);
+  wb.ray_d[0][i] = make_float4(__fdiv_rn(d[0], len), __fdiv_rn(d[1], len), __fdiv_rn(d[2], len),
+                               __uint_as_float(key));
+  wb.ray_slot[0][i] = i;
+}
+
+// ---- extend: closest hit --------------------------------------------------------
+template <bool kCount>
+__global__ void k_extend(SceneView sc, WaveBuffers wb, int parity) {
+  // counts can exceed the capacity after an overflow (the appends are then
+  // dropped and the status word set); never read past the queue
+  const uint32_t n = min(wb.counts[parity], wb.capacity);
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) {
+    wb.counts[parity ^ 1] = 0u;
+    wb.counts[2] = 0u;
+    atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
+  }
+  TravCounters cnt{0u, 0u, 0u};
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = tid; i < n; i += stride) {
+    const float4 o = wb.ray_o[parity][i];
+    const float4 d = wb.ray_d[parity][i];
+    HitRec h = traceRay<false, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, MAXD, cnt, wb.status);
+    wb.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+    wb.hit_inst[i] = h.inst;
+  }
+  if (kCount) {
+    unsigned long long a = cnt.nodes, b = cnt.tris, c = cnt.insts;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(kFull, a, o);
+      b += __shfl_down_sync(kFull, b, o);
+      c += __shfl_down_sync(kFull, c, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&wb.stats[2], a);
+      atomicAdd(&wb.stats[3], b);
+      atomicAdd(&wb.stats[4], c);
+    }
+  }
+}
+
+// ---- shadow: t-bounded any hit (solveEmission, trace.wesl:91-113) ----------------
+template <bool kCount>
+__global__ void k_shadow(SceneView sc, WaveBuffers wb) {
+  const uint32_t n = min(wb.counts[2], wb.capacity);
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) atomicAdd(&wb.stats[1], static_cast<unsigned long long>(n));
+  TravCounters cnt{0u, 0u, 0u};
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = tid; i < n; i += stride) {
+    const float4 o = wb.sh_o[i];
+    const float4 d = wb.sh_d[i];
+    // occluded iff the closest hit (< 1e6) is nearer than expected - 1e-3
+    const float tmax = fminf(d.w, MAXD);
+    HitRec h = traceRay<true, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, wb.status);
+    if (h.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[i]], o.w);
+  }
+  if (kCount) {
+    unsigned long long a = cnt.nodes, b = cnt.tris, c = cnt.insts;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(kFull, a, o);
+      b += __shfl_down_sync(kFull, b, o);
+      c += __shfl_down_sync(kFull, c, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&wb.stats[2], a);
+      atomicAdd(&wb.stats[3], b);
+      atomicAdd(&wb.stats[4], c);
+    }
+  }
+}
+
+// ---- light pdf: sum over every emissive triangle the ray meets -------------------
+// (pdf/emission.wesl:120-179).  A BVH over the emissive triangles finds them;
+// the terms are added in traversal order rather than buffer order.
+__device__ __forceinline__ float triangleHitDist(V3 rp, V3 rd, const DevLightTri& L) {
+  V3 e1 = ld3(L.e1), e2 = ld3(L.e2);
+  V3 pv = cross(rd, e2);
+  float det = dot(e1, pv);
+  if (fabsf(det) <= 1e-3f) return -1.0f;
+  float inv_det = 1.0f / det;
+  V3 tv = rp - ld3(L.v0);
+  float bu = dot(tv, pv) * inv_det;
+  if (bu < 0.0f || bu > 1.0f) return -1.0f;
+  V3 qv = cross(tv, e1);
+  float bv = dot(rd, qv) * inv_det;
+  if (bv < 0.0f || bu + bv > 1.0f) return -1.0f;
+  float hd = dot(e2, qv) * inv_det;
+  return hd > 1e-3f ? hd : -1.0f;
+}
+
+__device__ float lightPdf(const SceneView& sc, V3 pos, V3 next, uint32_t* status) {
+  if (!sc.has_lights) return 0.0f;
+  const V3 rd = normalize(next);
+  const float idx = safeInv(rd.x), idy = safeInv(rd.y), idz = safeInv(rd.z);
+  const float oix = pos.x * idx, oiy = pos.y * idy, oiz = pos.z * idz;
+  int32_t stack[32];
+  int sp = 0;
+  int32_t node = 0;
+  float pdf = 0.0f;
+  while (true) {
+    while (node >= 0) {
+      const float4* np = reinterpret_cast<const float4*>(sc.light_bvh + node);
+      const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+      const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+      const float a0 = fmaf(n0.x, idx, -oix), a1 = fmaf(n0.y, idx, -oix);
+      const float b0 = fmaf(n0.z, idy, -oiy), b1 = fmaf(n0.w, idy, -oiy);
+      const float c0 = fmaf(n2.x, idz, -oiz), c1 = fmaf(n2.y, idz, -oiz);
+      const float t0min = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
+      const float t0max = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fmaxf(c0, c1));
+      const float d0 = fmaf(n1.x, idx, -oix), d1 = fmaf(n1.y, idx, -oix);
+      const float e0 = fmaf(n1.z, idy, -oiy), e1 = fmaf(n1.w, idy, -oiy);
+      const float f0 = fmaf(n2.z, idz, -oiz), f1 = fmaf(n2.w, idz, -oiz);
+      const float t1min = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), 0.0f));
+      const float t1max = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fmaxf(f0, f1));
+      // a child exists if it is an inner node or a leaf with triangles
+      const bool h0 = t0min <= t0max && (n3.x >= 0 || n3.z != 0);
+      const bool h1 = t1min <= t1max && (n3.y >= 0 || n3.w != 0);
+      if (h0 && h1) {
+        if (sp >= 32) {
+          atomicOr(status, 1u);
+          return pdf;
+        }
+        stack[sp++] = n3.y;
+        node = n3.x;
+      } else if (h0) {
+        node = n3.x;
+      } else if (h1) {
+        node = n3.y;
+      } else {
+        node = sp > 0 ? stack[--sp] : kDone;
+      }
+    }
+    if (node == kDone) break;
+    const uint32_t first = static_cast<uint32_t>(~node) >> 3;
+    const uint32_t count = static_cast<uint32_t>(~node) & 7u;
+    for (uint32_t k = 0; k < count; ++k) {
+      const DevLightTri L = sc.light_tri[first + k];
+      const float hd = triangleHitDist(pos, rd, L);
+      if (hd <= 0.0f) continue;
+      const float lp = fabsf(dot(ld3(L.n), -rd));
+      pdf += L.area_pdf * hd * hd / fmaxf(lp, 1e-3f);
+    }
+    node = sp > 0 ? stack[--sp] : kDone;
+  }
+  return pdf;
+}
+
+// ---- environment (environment.wesl:7-25) -----------------------------------------
+__device__ __forceinline__ float envRadiance(const SceneView& sc, V3 dir, const SmitsPos& sp) {
+  V3 d = normalize(dir);
+  float u = atan2f(d.y, d.x) / (2.0f * PI) + 0.5f;
+  float v = acosf(wclamp(d.z, -1.0f, 1.0f)) / PI;
+  float wu = u - floorf(u);
+  float cv = wclamp(1.0f - v, 0.0f, 0.999999f);
+  uint32_t x = min(sc.env_w - 1u, u32f(wu * static_cast<float>(sc.env_w)));
+  uint32_t y = min(sc.env_h - 1u, u32f(cv * static_cast<float>(sc.env_h)));
+  float4 t = __ldg(sc.env + size_t(y) * sc.env_w + x);
+  return rgbToRadiance(V3{t.x, t.y, t.z}, sp);
+}
+
+enum { M_NONE = 0, M_DIFFUSE = 1, M_SREFL = 2, M_RREFL = 3, M_STRANS = 4, M_RTRANS = 5 };
+
+// balancePdfDenominator (sample.wesl:505-554).  A lobe (or the light) with a
+// zero sample count contributes 0 * pdf = 0; its pdf is not evaluated.
+__device__ __forceinline__ float balanceDenom(const SceneView& sc, V3 curr, V3 next, const Surf& s,
+                                              const Mat& m, const Counts& c, int model,
+                                              float model_pdf, float light_pdf_in,
+                                              uint32_t* status) {
+  float pd = 0.0f, psr = 0.0f, prr = 0.0f, pst = 0.0f, prt = 0.0f, pl = 0.0f;
+  if (c.diffuse) pd = model == M_DIFFUSE ? model_pdf : diffusePdf(curr, next, s);
+  if (c.specular_reflect) psr = model == M_SREFL ? model_pdf : specularReflectPdf(curr, next, s);
+  if (c.rough_reflect) prr = model == M_RREFL ? model_pdf : roughReflectPdf(curr, next, s, m);
+  if (c.specular_transmit)
+    pst = model == M_STRANS ? model_pdf : specularTransmitPdf(curr, next, s, m);
+  if (c.rough_transmit) prt = model == M_RTRANS ? model_pdf : roughTransmitPdf(curr, next, s, m);
+  if (c.light) pl = light_pdf_in >= 0.0f ? light_pdf_in : lightPdf(sc, s.pos, next, status);
+  return fmaxf(static_cast<float>(c.diffuse) * pd + static_cast<float>(c.specular_reflect) * psr +
+                   static_cast<float>(c.rough_reflect) * prr +
+                   static_cast<float>(c.specular_transmit) * pst +
+                   static_cast<float>(c.rough_transmit) * prt +
+                   static_cast<float>(c.light) * pl,
+               1e-6f);
+}
+
+// spawnSurfaceRay (spawn_surface_ray.wesl:4-15)
+__device__ __forceinline__ V3 spawnOrigin(const Surf& s, V3 next) {
+  V3 on = dot(next, s.gn) > 0.0f ? s.gn : -s.gn;
+  return s.pos + on * 1e-3f;
+}
+
+struct Child {
+  V3 o, d;
+  float w;
+  uint32_t key;
+};
+
+// ---- shade: one tree node per ray ------------------------------------------------
+__global__ void k_shade(SceneView sc, FrameConst fc, WaveBuffers wb, int depth, int parity) {
+  const uint32_t n = min(wb.counts[parity], wb.capacity);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int out = parity ^ 1;
+  const uint32_t cut_depth = max(1u, min(fc.caps.trace_depth, 64u)) - 1u;
+  const SampleCaps caps{fc.caps.trace_depth, fc.caps.transport_cap, fc.caps.emission_cap,
+                        fc.caps.diffuse_cap, fc.caps.rough_cap};
+  for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
+    const uint32_t i = base + lane;
+    Child ch[4];
+    uint32_t nch = 0;
+    bool shadow = false;
+    float4 sh_o = make_float4(0, 0, 0, 0), sh_d = make_float4(0, 0, 0, 0);
+    uint32_t slot = 0;
+    if (i < n) {
+      const float4 o4 = wb.ray_o[parity][i];
+      const float4 d4 = wb.ray_d[parity][i];
+      slot = wb.ray_slot[parity][i];
+      const V3 ro{o4.x, o4.y, o4.z}, rd{d4.x, d4.y, d4.z};
+      const float W = o4.w;
+      const uint32_t key = __float_as_uint(d4.w);
+      const float4 h4 = wb.hit[i];
+      const int32_t hinst = wb.hit_inst[i];
+      const float lambda = wb.s_lambda[slot];
+      const SmitsPos spos = smitsPos(lambda);
+      float addL = 0.0f;
+      if (hinst < 0) {
+        addL = W * envRadiance(sc, rd, spos);
+      } else if (static_cast<uint32_t>(depth) < cut_depth) {
+        // surface frame of the closest hit (bvh.wesl:102-129, 167-179)
+        const uint32_t tri = __float_as_uint(h4.w);
+        const float t = h4.x, u = h4.y, v = h4.z;
+        const DevInstance* ip = sc.inst + hinst;
+        const float4* ipf = reinterpret_cast<const float4*>(ip);
+        const float4 r0 = __ldg(ipf), r1 = __ldg(ipf + 1), r2 = __ldg(ipf + 2);
+        const uint4 meta = __ldg(reinterpret_cast<const uint4*>(ipf + 3));
+        const float inv[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+        const uint4 vi = __ldg(sc.tri_vidx + tri);
+        const float4 N0 = __ldg(sc.vnormal + vi.x), N1 = __ldg(sc.vnormal + vi.y),
+                     N2 = __ldg(sc.vnormal + vi.z);
+        const float4 E1 = __ldg(sc.tris + 3u * tri + 1u), E2 = __ldg(sc.tris + 3u * tri + 2u);
+        const float w0 = 1.0f - u - v;
+        const V3 ln = normalize(w0 * V3{N0.x, N0.y, N0.z} + u * V3{N1.x, N1.y, N1.z} +
+                                v * V3{N2.x, N2.y, N2.z});
+        const V3 lgn = normalize(cross(V3{E1.x, E1.y, E1.z}, V3{E2.x, E2.y, E2.z}));
+        const V3 wgn = normalize(normalToWorld(inv, lgn));
+        const V3 wsn = normalize(normalToWorld(inv, ln));
+        Surf s;
+        s.pos = ro + t * rd;
+        s.gn = wgn;
+        s.sn = dot(wsn, wgn) >= 0.0f ? wsn : -wsn;
+        const Mat m = decode(sc.mat[meta.y], lambda, spos);
+        const Counts c = counts(m, sc.has_lights != 0u, depth, caps);
+        Rng rng;
+        seedRng(rng, key);
+        addL = W * m.emission;
+        const V3 curr = rd;
+        uint32_t ti = 0;  // transport sample index (child key)
+        auto push = [&](V3 next, int model, float prob, float dist) {
+          const float coeff = dist / balanceDenom(sc, curr, next, s, m, c, model, prob, -1.0f, wb.status);
+          const float cw = W * coeff;
+          if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
+          ++ti;
+        };
+        // sampleModels (sample.wesl:301-425) in its lobe order
+        if (c.diffuse) {  // pdf/diffuse.wesl:7-36
+          const V3 macro = orientedNormal(curr, s.sn);
+          const float r = sqrtf(randFloat(rng));
+          const float angle = 2.0f * PI * randFloat(rng);
+          float sa, ca;
+          sincosf(angle, &sa, &ca);
+          const V3 local{r * ca, r * sa, sqrtf(fmaxf(0.0f, 1.0f - r * r))};
+          const V3 next = mul(makeTangentSpace(macro), local);
+          push(next, M_DIFFUSE, diffusePdf(curr, next, s), diffuseDist(curr, next, s, m));
+        }
+        if (c.specular_reflect) {  // pdf/specular_reflection.wesl:7-15
+          const V3 next = specularDir(curr, s);
+          push(next, M_SREFL, specularReflectPdf(curr, next, s), specularReflectDist(curr, next, s, m));
+        }
+        if (c.rough_reflect) {  // pdf/rough_reflection.wesl:9-27
+          const V3 micro = orientedNormal(curr, sampleNorm(curr, s, m.microfacet_roughness, rng));
+          const V3 next = reflect(curr, micro);
+          const V3 macro = orientedNormal(curr, s.sn);
+          const float prob = dot(next, macro) <= 0.0f
+                                 ? 0.0f
+                                 : reflectPdf(curr, micro, macro, m.microfacet_roughness);
+          push(next, M_RREFL, prob, roughReflectDist(curr, next, s, m));
+        }
+        if (c.specular_transmit) {  // pdf/specular_transmission.wesl:9-27
+          const V3 next = m.volume ? refract(curr, orientedNormal(curr, s.sn), relIor(s.sn, curr, m).re)
+                                   : curr;
+          push(next, M_STRANS, specularTransmitPdf(curr, next, s, m),
+               specularTransmitDist(curr, next, s, m));
+        }
+        if (c.rough_transmit) {  // pdf/rough_transmission.wesl:9-32
+          const V3 macro = orientedNormal(curr, s.sn);
+          const V3 micro = orientedNormal(curr, sampleNorm(curr, s, m.microfacet_roughness, rng));
+          const V3 next = refract(curr, micro, relIorT(relIor(micro, curr, m)));
+          float prob;
+          if (dot(next, next) <= VNDF_EPS)
+            prob = 0.0f;
+          else if (dot(next, macro) >= 0.0f)
+            prob = 0.0f;
+          else
+            prob = roughTransmitPdf(curr, next, s, m);
+          push(next, M_RTRANS, prob, roughTransmitDist(curr, next, s, m));
+        }
+        if (c.light) {  // sample.wesl:407-422 with pdf/emission.wesl:32-82
+          const uint32_t ne = sc.emissive_count;
+          uint32_t bin = static_cast<uint32_t>(randFloat(rng) * static_cast<float>(ne));
+          if (bin >= ne) bin = ne - 1u;  // randFloat() can return 1.0
+          const float rf = randFloat(rng);
+          const DevAlias al = sc.alias[bin];
+          const DevEmissivePrim& P = sc.eprim[rf < al.prob ? bin : al.alias];
+          const float tsx = randFloat(rng);
+          const float tsy = randFloat(rng);
+          const float tss = sqrtf(tsx);
+          const float bx = 1.0f - tss, by = tss * (1.0f - tsy), bz = tss * tsy;
+          const V3 v0 = ld3(P.v0), v1 = ld3(P.v1), v2 = ld3(P.v2);
+          const V3 spos3 = bx * v0 + by * v1 + bz * v2;
+          const V3 lo = spos3 - s.pos;
+          const float dsq = fmaxf(dot(lo, lo), 1e-3f);
+          const V3 next = lo / sqrtf(dsq);
+          const V3 lnrm = normalize(cross(v1 - v0, v2 - v0));
+          const float lp = fabsf(dot(lnrm, -next));
+          const float area_pdf = fmaxf(P.weight / P.area, 1e-3f);
+          const float sapdf = area_pdf * dsq / fmaxf(lp, 1e-3f);
+          if (!(sapdf <= 1e-6f)) {  // addEmissionSample's MIN_SAMPLE_WEIGHT check
+            const float radiance = rgbToRadiance(ld3(P.emission), spos);
+            const float sproj = fabsf(dot(s.sn, next));
+            float ec = diffuseDist(curr, next, s, m) + roughReflectDist(curr, next, s, m);
+            if (m.transmission != 0.0f) ec = ec + roughTransmitDist(curr, next, s, m);
+            const float rad = radiance * ec * sproj /
+                              balanceDenom(sc, curr, next, s, m, c, M_NONE, -1.0f, sapdf, wb.status);
+            const float contrib = W * rad;
+            if (contrib != 0.0f) {
+              const float expected_dist = sqrtf(dsq);
+              const V3 light_pos = s.pos + next * expected_dist;
+              const V3 so = spawnOrigin(s, next);
+              const float tmax = distance3(so, light_pos) - 1e-3f;
+              shadow = true;
+              sh_o = make_float4(so.x, so.y, so.z, contrib);
+              sh_d = make_float4(next.x, next.y, next.z, tmax);
+            }
+          }
+        }
+      }
+      if (addL != 0.0f) atomicAdd(&wb.s_L[slot], addL);
+    }
+    // ---- warp-aggregated queue appends ----
+    uint32_t incl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= static_cast<uint32_t>(o)) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    uint32_t qbase = 0;
+    if (lane == 31 && total) qbase = atomicAdd(&wb.counts[out], total);
+    qbase = __shfl_sync(kFull, qbase, 31);
+    if (total) {
+      if (qbase + total > wb.capacity) {
+        if (lane == 0) atomicOr(wb.status, 2u);
+      } else {
+        uint32_t pos = qbase + incl - nch;
+        for (uint32_t k = 0; k < nch; ++k, ++pos) {
+          wb.ray_o[out][pos] = make_float4(ch[k].o.x, ch[k].o.y, ch[k].o.z, ch[k].w);
+          wb.ray_d[out][pos] = make_float4(ch[k].d.x, ch[k].d.y, ch[k].d.z, __uint_as_float(ch[k].key));
+          wb.ray_slot[out][pos] = slot;
+        }
+      }
+    }
+    const unsigned ballot = __ballot_sync(kFull, shadow);
+    if (ballot) {
+      uint32_t sbase = 0;
+      if (lane == 0) sbase = atomicAdd(&wb.counts[2], static_cast<uint32_t>(__popc(ballot)));
+      sbase = __shfl_sync(kFull, sbase, 0);
+      if (sbase + __popc(ballot) > wb.capacity) {
+        if (lane == 0) atomicOr(wb.status, 2u);
+      } else if (shadow) {
+        const uint32_t pos = sbase + __popc(ballot & ((1u << lane) - 1u));
+        wb.sh_o[pos] = sh_o;
+        wb.sh_d[pos] = sh_d;
+        wb.sh_slot[pos] = slot;
+      }
+    }
+  }
+}
+
+// ---- resolve: spp loop sum + running mean + sRGB (compute.wesl:41-61) -----------
+__global__ void k_resolve(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ch.pixel_count) return;
+  const uint64_t gp = ch.pixel_begin + j;
+  const ViewDev& v = fc.views[findViewByPixel(fc, gp)];
+  const uint32_t lp = static_cast<uint32_t>(gp - v.pixel_offset);
+  const uint32_t pixel = v.pixel_base + lp;
+  const uint64_t first = v.sample_offset + uint64_t(lp) * v.spp - ch.sample_begin;
+  const float avg = fc.wl_const[1];
+  const float spp = static_cast<float>(v.spp);
+  V3 acc{0.0f, 0.0f, 0.0f};
+  for (uint32_t k = 0; k < v.spp; ++k) {
+    const float L = wb.s_L[first + k];
+    const float lambda = wb.s_lambda[first + k];
+    const float prob = wb.s_prob[first + k];
+    const V3 il = xyzMatch(lambda) * L / avg;
+    acc = acc + il / prob / spp;
+  }
+  V3 lum{0.0f, 0.0f, 0.0f};
+  if (v.frame > 0u) {
+    const float4 f = v.film[pixel];
+    lum = V3{f.x, f.y, f.z} * (1.0f - v.sample_weight);
+  }
+  lum = lum + acc * v.sample_weight;
+  v.film[pixel] = make_float4(lum.x, lum.y, lum.z, 0.0f);
+  if (v.rgba) {
+    const V3 lin = xyzToLinearSrgb(lum);
+    v.rgba[pixel] = make_uchar4(static_cast<unsigned char>(__float2uint_rn(encodeChannel(lin.x) * 255.0f)),
+                                static_cast<unsigned char>(__float2uint_rn(encodeChannel(lin.y) * 255.0f)),
+                                static_cast<unsigned char>(__float2uint_rn(encodeChannel(lin.z) * 255.0f)),
+                                255);
+  }
+}
+
+// ---- closest-hit query for parity tests -------------------------------------------
+__global__ void k_trace_closest(SceneView sc, const float4* rays, uint32_t n, float4* out_tuv,
+                                int4* out_ids, uint32_t* status) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 o = rays[2 * i], d = rays[2 * i + 1];
+  TravCounters cnt{0u, 0u, 0u};
+  HitRec h = traceRay<false, false>(sc, o.x, o.y, o.z, d.x, d.y, d.z, MAXD, cnt, status);
+  if (h.inst >= 0) {
+    const uint32_t orig = __float_as_uint(__ldg(sc.tris + 3u * h.tri).w);
+    out_tuv[i] = make_float4(h.t, h.u, h.v, 0.0f);
+    out_ids[i] = make_int4(h.inst, static_cast<int>(orig), static_cast<int>(h.tri), 0);
+  } else {
+    out_tuv[i] = make_float4(MAXD, 0.0f, 0.0f, 0.0f);
+    out_ids[i] = make_int4(-1, -1, -1, 0);
+  }
+}
+
+int gSmCount = 0;
+
+uint32_t gridFor(uint32_t blocks_per_sm) {
+  return static_cast<uint32_t>(smCount()) * (blocks_per_sm > 0 ? blocks_per_sm : 1u);
+}
+
+}  // namespace
+
+int smCount() {
+  if (gSmCount == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&gSmCount, cudaDevAttrMultiProcessorCount, dev);
+    if (gSmCount <= 0) gSmCount = 148;
+  }
+  return gSmCount;
+}
+
+void launchWavelengthTree(float* tree, float* consts, cudaStream_t s) {
+  k_wavelength_tree<<<(65535 + 255) / 256, 256, 0, s>>>(tree, consts);
+}
+
+void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch, cudaStream_t s) {
+  const uint32_t n = ch.sample_count > 0 ? ch.sample_count : 1u;
+  k_gen<<<(n + 255) / 256, 256, 0, s>>>(fc, wb, ch);
+}
+
+void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
+                  const LaunchShape& ls, cudaStream_t s) {
+  const uint32_t block = ls.extend_block;
+  const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
+  if (counting)
+    k_extend<true><<<grid, block, 0, s>>>(sc, wb, parity);
+  else
+    k_extend<false><<<grid, block, 0, s>>>(sc, wb, parity);
+}
+
+void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
+                 int parity, const LaunchShape& ls, cudaStream_t s) {
+  const uint32_t block = ls.shade_block;
+  const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
+  k_shade<<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+}
+
+void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
+                  const LaunchShape& ls, cudaStream_t s) {
+  const uint32_t block = ls.extend_block;
+  const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
+  if (counting)
+    k_shadow<true><<<grid, block, 0, s>>>(sc, wb);
+  else
+    k_shadow<false><<<grid, block, 0, s>>>(sc, wb);
+}
+
+void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
+                   cudaStream_t s) {
+  const uint32_t n = ch.pixel_count > 0 ? ch.pixel_count : 1u;
+  k_resolve<<<(n + 127) / 128, 128, 0, s>>>(fc, wb, ch);
+}
+
+void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
+                        int4* out_ids, uint32_t* status, cudaStream_t s) {
+  if (n == 0) return;
+  k_trace_closest<<<(n + 127) / 128, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
+}
+
+}  // namespace cg

@@ -1,0 +1,100 @@
+// cg_kernels.h — launch interface of the wavefront kernels (cg_kernels.cu).
+//
+// One View() frame is a sequence of chunks.  A chunk is a run of whole pixels
+// (all their samples) from one or more views; per chunk the launches are
+//   gen -> D x (extend -> shade -> shadow) -> resolve
+// over ping-pong ray queues in HBM.  Every launch reads its work count from
+// device memory, so the sequence needs no host synchronisation and can be
+// captured as a CUDA graph.
+#ifndef CG_KERNELS_H_
+#define CG_KERNELS_H_
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cg_types.h"
+
+namespace cg {
+
+// Per-view constants (device).  An entry covers image pixels
+// [pixel_base, pixel_base + pixel_count) of a view, so a chunk can hold slices
+// of several views.
+struct ViewDev {
+  float pos[3], dir[3], dx[3], dy[3];  // camera basis of cameraRay (compute.wesl:64-79)
+  uint32_t width, height, spp, seed;
+  uint32_t frame;              // iter_count: 0 starts a fresh running mean
+  float sample_weight;         // 1 / (frame + 1)
+  uint32_t pixel_base;         // first image pixel this entry covers
+  uint32_t pixel_count;        // image pixels this entry covers
+  uint64_t pixel_offset;       // first global pixel index of this entry
+  uint64_t sample_offset;      // first global sample index of this entry
+  float4* film;                // running-mean XYZ (w unused)
+  uchar4* rgba;                // sRGB rgba8 (may be null)
+};
+
+// Sample caps of a frame (PathTraceConf, after clamping).
+struct Caps {
+  uint32_t trace_depth, transport_cap, emission_cap, diffuse_cap, rough_cap;
+};
+
+// Wavefront buffers (device).
+struct WaveBuffers {
+  float4* ray_o[2];      // origin.xyz, path weight
+  float4* ray_d[2];      // dir.xyz, node key bits
+  uint32_t* ray_slot[2];
+  float4* hit;           // t, u, v, triangle slot bits
+  int32_t* hit_inst;     // -1 = miss
+  float4* sh_o;          // shadow origin.xyz, contribution
+  float4* sh_d;          // shadow dir.xyz, tmax
+  uint32_t* sh_slot;
+  float* s_L;            // per sample slot: accumulated radiance
+  float* s_lambda;
+  float* s_prob;
+  uint32_t* counts;      // [0], [1] ray queues, [2] shadow queue
+  unsigned long long* stats;  // [0] extend rays [1] shadow rays [2] nodes [3] tris [4] insts
+  uint32_t* status;      // bit 0: traversal stack overflow, bit 1: queue overflow
+  uint32_t capacity;     // rays per queue (and shadow rays)
+  uint32_t sample_capacity;
+};
+
+struct FrameConst {
+  const ViewDev* views;
+  uint32_t view_count;
+  Caps caps;
+  const float* wl_tree;  // 65535 cdf values (sampleWavelengthCdf bisection)
+  const float* wl_const; // [0] total integral, [1] total / 3
+};
+
+struct ChunkDesc {
+  uint64_t sample_begin;
+  uint64_t pixel_begin;
+  uint32_t sample_count;
+  uint32_t pixel_count;
+};
+
+struct LaunchShape {
+  uint32_t extend_block = 128;
+  uint32_t shade_block = 128;
+  uint32_t grid_extend = 0;  // 0: derived from the SM count
+  uint32_t grid_shade = 0;
+};
+
+void launchWavelengthTree(float* tree, float* consts, cudaStream_t s);
+void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch, cudaStream_t s);
+void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
+                  const LaunchShape& ls, cudaStream_t s);
+void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
+                 int parity, const LaunchShape& ls, cudaStream_t s);
+void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
+                  const LaunchShape& ls, cudaStream_t s);
+void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
+                   cudaStream_t s);
+void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
+                        int4* out_ids, uint32_t* status, cudaStream_t s);
+
+int smCount();
+
+}  // namespace cg
+
+#endif

@@ -1,0 +1,390 @@
+// cg_scene.cpp — host scene packing for the CUDA backend.
+//
+// Compiled with -ffp-contract=off: the emissive buffer, its weights and the
+// inverse instance transforms must round exactly as the host code they
+// restate (src/pathtracing/emissive_buffer.h:44-100, tlas.h:56-73).
+#include "cg_scene.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "cg_bvh.h"
+
+namespace cg {
+namespace {
+
+struct F3 {
+  float x, y, z;
+};
+inline F3 sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline F3 cross3(F3 a, F3 b) {
+  return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+inline F3 vpos(const cg_vertex& v) { return {v.position[0], v.position[1], v.position[2]}; }
+
+// glm mat4 * vec4(p, 1): (m0 x + m1 y) + (m2 z + m3 w)  (emissive_buffer.h:134-137)
+F3 transformPoint(const float* m, F3 p) {
+  float r[3];
+  const float q[3] = {p.x, p.y, p.z};
+  for (int i = 0; i < 3; ++i) {
+    float add0 = m[i * 4 + 0] * q[0] + m[i * 4 + 1] * q[1];
+    float add1 = m[i * 4 + 2] * q[2] + m[i * 4 + 3] * 1.0f;
+    r[i] = add0 + add1;
+  }
+  return {r[0], r[1], r[2]};
+}
+
+float luminance(F3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
+
+}  // namespace
+
+void invertAffine(const float* m, float* out) {
+  double a[3][3], t[3];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) a[i][j] = m[i * 4 + j];
+    t[i] = m[i * 4 + 3];
+  }
+  double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+  double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+  double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+  double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+  double inv[3][3];
+  inv[0][0] = c00 / det;
+  inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+  inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+  inv[1][0] = c01 / det;
+  inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+  inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+  inv[2][0] = c02 / det;
+  inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+  inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+  for (int i = 0; i < 3; ++i) {
+    double ti = -(inv[i][0] * t[0] + inv[i][1] * t[1] + inv[i][2] * t[2]);
+    for (int j = 0; j < 3; ++j) out[i * 4 + j] = static_cast<float>(inv[i][j]);
+    out[i * 4 + 3] = static_cast<float>(ti);
+  }
+}
+
+void buildAliasTable(const double* weights, uint32_t count, cg_alias_entry* entries) {
+  for (uint32_t i = 0; i < count; ++i) entries[i] = cg_alias_entry{0u, 0.0f};
+  if (count == 0) return;
+  std::vector<double> p(count);
+  double total = 0.0;
+  for (uint32_t i = 0; i < count; ++i) p[i] = std::max(0.0, weights[i]);
+  for (uint32_t i = 0; i < count; ++i) total += p[i];
+  if (total <= 0.0) return;
+  std::vector<uint32_t> small, large;
+  small.reserve(count);
+  large.reserve(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    p[i] = p[i] / total * count;
+    (p[i] >= 1.0 ? large : small).push_back(i);
+  }
+  while (!large.empty() && !small.empty()) {
+    const uint32_t s = small.back(), l = large.back();
+    small.pop_back();
+    large.pop_back();
+    entries[s].prob = static_cast<float>(p[s]);
+    entries[s].alias = l;
+    p[l] -= 1.0 - static_cast<double>(entries[s].prob);
+    (p[l] < 1.0 ? small : large).push_back(l);
+  }
+  for (auto* list : {&large, &small}) {
+    while (!list->empty()) {
+      const uint32_t i = list->back();
+      list->pop_back();
+      entries[i].prob = 1.0f;
+      entries[i].alias = i;
+    }
+  }
+}
+
+int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
+  if (!d) {
+    err = "scene description is null";
+    return CG_E_INVALID;
+  }
+  if ((d->vertex_count && !d->vertices) || (d->index_count && !d->indices) ||
+      (d->mesh_count && !d->meshes) || (d->instance_count && !d->instances) ||
+      (d->material_count && !d->materials)) {
+    err = "scene description has a null array with a nonzero count";
+    return CG_E_INVALID;
+  }
+  // ---- validation -------------------------------------------------------
+  for (uint32_t m = 0; m < d->mesh_count; ++m) {
+    const cg_mesh& mesh = d->meshes[m];
+    if (uint64_t(mesh.index_offset) + mesh.index_count > d->index_count) {
+      err = "mesh " + std::to_string(m) + " index range exceeds the index buffer";
+      return CG_E_INVALID;
+    }
+    if (uint64_t(mesh.vertex_offset) + mesh.vertex_count > d->vertex_count) {
+      err = "mesh " + std::to_string(m) + " vertex range exceeds the vertex buffer";
+      return CG_E_INVALID;
+    }
+    for (uint32_t i = 0; i < mesh.index_count; ++i) {
+      if (d->indices[mesh.index_offset + i] >= d->vertex_count) {
+        err = "mesh " + std::to_string(m) + " has an index beyond the vertex buffer";
+        return CG_E_INVALID;
+      }
+    }
+  }
+  for (uint32_t i = 0; i < d->instance_count; ++i) {
+    const cg_instance& in = d->instances[i];
+    if (in.mesh >= d->mesh_count || in.material >= d->material_count) {
+      err = "instance " + std::to_string(i) + " names a missing mesh or material";
+      return CG_E_INVALID;
+    }
+    for (float f : in.world_from_local)
+      if (!std::isfinite(f)) {
+        err = "instance " + std::to_string(i) + " has a non-finite transform";
+        return CG_E_INVALID;
+      }
+  }
+  for (uint32_t i = 0; i < d->material_count; ++i) {
+    const cg_material& m = d->materials[i];
+    if (m.base_color_texture >= 0 || m.metallic_roughness_texture >= 0 ||
+        m.emissive_texture >= 0 || m.transmission_texture >= 0) {
+      err = "material " + std::to_string(i) + " uses a texture; textured materials are not supported";
+      return CG_E_INVALID;
+    }
+  }
+  if (d->env_rgba32f && (d->env_width == 0 || d->env_height == 0)) {
+    err = "environment texture has a zero dimension";
+    return CG_E_INVALID;
+  }
+
+  // ---- vertices ---------------------------------------------------------
+  s.vnormal.resize(size_t(d->vertex_count) * 4);
+  for (uint32_t v = 0; v < d->vertex_count; ++v) {
+    for (int k = 0; k < 3; ++k) s.vnormal[size_t(v) * 4 + k] = d->vertices[v].normal[k];
+    s.vnormal[size_t(v) * 4 + 3] = 0.0f;
+  }
+
+  // ---- one BLAS per mesh ------------------------------------------------------
+  s.mesh_count = d->mesh_count;
+  std::vector<uint32_t> mesh_root(d->mesh_count), mesh_tri_base(d->mesh_count);
+  std::vector<Box> mesh_bounds(d->mesh_count);
+  BvhBuildOptions blas_opt;
+  blas_opt.max_leaf = 4;
+  std::vector<uint32_t> order;
+  for (uint32_t m = 0; m < d->mesh_count; ++m) {
+    const cg_mesh& mesh = d->meshes[m];
+    const uint32_t nt = mesh.index_count / 3;
+    std::vector<Box> boxes(nt);
+    Box mb;
+    for (int a = 0; a < 3; ++a) {
+      mb.lo[a] = std::numeric_limits<float>::infinity();
+      mb.hi[a] = -std::numeric_limits<float>::infinity();
+    }
+    for (uint32_t t = 0; t < nt; ++t) {
+      const uint32_t* ix = d->indices + mesh.index_offset + 3 * t;
+      Box& b = boxes[t];
+      for (int a = 0; a < 3; ++a) {
+        b.lo[a] = std::numeric_limits<float>::infinity();
+        b.hi[a] = -std::numeric_limits<float>::infinity();
+      }
+      for (int k = 0; k < 3; ++k) {
+        const float* p = d->vertices[ix[k]].position;
+        for (int a = 0; a < 3; ++a) {
+          b.lo[a] = std::min(b.lo[a], p[a]);
+          b.hi[a] = std::max(b.hi[a], p[a]);
+          mb.lo[a] = std::min(mb.lo[a], p[a]);
+          mb.hi[a] = std::max(mb.hi[a], p[a]);
+        }
+      }
+    }
+    mesh_bounds[m] = mb;
+    const uint32_t tri_base = static_cast<uint32_t>(s.tri_vidx.size() / 4);
+    mesh_tri_base[m] = tri_base;
+    order.clear();
+    uint32_t depth = 0;
+    mesh_root[m] = buildBvh(boxes, blas_opt, tri_base, s.blas, order, &depth);
+    s.blas_depth = std::max(s.blas_depth, depth);
+    for (uint32_t k = 0; k < nt; ++k) {
+      const uint32_t t = order[k];
+      const uint32_t* ix = d->indices + mesh.index_offset + 3 * t;
+      F3 v0 = vpos(d->vertices[ix[0]]), v1 = vpos(d->vertices[ix[1]]), v2 = vpos(d->vertices[ix[2]]);
+      F3 e1 = sub(v1, v0), e2 = sub(v2, v0);  // the subtractions of bvh.wesl:189-190
+      float idbits;
+      std::memcpy(&idbits, &t, 4);
+      const float rec[12] = {v0.x, v0.y, v0.z, idbits, e1.x, e1.y, e1.z, 0.0f,
+                             e2.x, e2.y, e2.z, 0.0f};
+      s.tris.insert(s.tris.end(), rec, rec + 12);
+      const uint32_t vi[4] = {ix[0], ix[1], ix[2], t};
+      s.tri_vidx.insert(s.tri_vidx.end(), vi, vi + 4);
+    }
+  }
+  s.triangle_count = static_cast<uint32_t>(s.tri_vidx.size() / 4);
+
+  // ---- materials ------------------------------------------------------------------
+  auto clamp01 = [](float x) { return std::fmin(std::fmax(x, 0.0f), 1.0f); };
+  s.max_lobes = 0;
+  for (uint32_t i = 0; i < d->material_count; ++i) {
+    const cg_material& m = d->materials[i];
+    DevMaterial dm{};
+    for (int k = 0; k < 3; ++k) {
+      dm.base[k] = m.base_color_factor[k];
+      dm.emission[k] = std::fmax(m.emissive_factor[k] * m.emissive_strength, 0.0f);
+    }
+    dm.metallic = clamp01(m.metallic_factor);
+    dm.roughness = clamp01(m.roughness_factor);
+    dm.ior = m.ior;
+    dm.dispersion = m.dispersion;
+    dm.transmission = clamp01(m.transmission_factor);
+    dm.volume = m.thickness_factor > 0.0f ? 1u : 0u;
+    s.mat.push_back(dm);
+    uint32_t lobes = 1;  // a reflection lobe
+    if ((1.0f - dm.metallic) * (1.0f - dm.transmission) > 0.0f) ++lobes;
+    if (dm.transmission > 1e-6f) ++lobes;
+    s.max_lobes = std::max(s.max_lobes, lobes);
+  }
+
+  // ---- instances and the TLAS ---------------------------------------------------------
+  std::vector<Box> inst_boxes(d->instance_count);
+  for (uint32_t i = 0; i < d->instance_count; ++i) {
+    const cg_instance& ci = d->instances[i];
+    DevInstance di{};
+    invertAffine(ci.world_from_local, di.inv);
+    di.blas_root = mesh_root[ci.mesh];
+    di.material = ci.material;
+    di.tri_base = mesh_tri_base[ci.mesh];
+    di.mesh = ci.mesh;
+    s.inst.push_back(di);
+    // world box of the mesh box's 8 corners (double, then widened)
+    const Box& mb = mesh_bounds[ci.mesh];
+    Box wb;
+    for (int a = 0; a < 3; ++a) {
+      wb.lo[a] = std::numeric_limits<float>::infinity();
+      wb.hi[a] = -std::numeric_limits<float>::infinity();
+    }
+    if (mb.lo[0] <= mb.hi[0]) {
+      for (int c = 0; c < 8; ++c) {
+        double p[3] = {(c & 1) ? mb.hi[0] : mb.lo[0], (c & 2) ? mb.hi[1] : mb.lo[1],
+                       (c & 4) ? mb.hi[2] : mb.lo[2]};
+        for (int a = 0; a < 3; ++a) {
+          const float* r = ci.world_from_local + 4 * a;
+          double w = double(r[0]) * p[0] + double(r[1]) * p[1] + double(r[2]) * p[2] + double(r[3]);
+          wb.lo[a] = std::min(wb.lo[a], std::nextafter(static_cast<float>(w), -INFINITY));
+          wb.hi[a] = std::max(wb.hi[a], std::nextafter(static_cast<float>(w), INFINITY));
+        }
+      }
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        wb.lo[a] = 1.0f;
+        wb.hi[a] = -1.0f;
+      }
+    }
+    inst_boxes[i] = wb;
+  }
+  {
+    BvhBuildOptions opt;
+    opt.max_leaf = 1;
+    std::vector<uint32_t> tlas_order;
+    uint32_t depth = 0;
+    buildBvh(inst_boxes, opt, 0, s.tlas, tlas_order, &depth);
+    s.tlas_depth = depth;
+    // TLAS leaves index tlas_order -> instance; store instance ids directly
+    for (BvhNode& n : s.tlas) {
+      if (n.child0 < 0 && n.cnt0) n.child0 = leafLinkOf(tlas_order[leafFirst(n.child0)], 1);
+      if (n.child1 < 0 && n.cnt1) n.child1 = leafLinkOf(tlas_order[leafFirst(n.child1)], 1);
+    }
+  }
+
+  // ---- emissive buffer (emissive_buffer.h:44-100) --------------------------------------
+  for (uint32_t p = 0; p < d->instance_count; ++p) {
+    const cg_instance& inst = d->instances[p];
+    const DevMaterial& m = s.mat[inst.material];
+    F3 base{m.emission[0], m.emission[1], m.emission[2]};
+    if (luminance(base) <= 0.0f) continue;
+    const cg_mesh& mesh = d->meshes[inst.mesh];
+    for (uint32_t i = 0; i + 2 < mesh.index_count; i += 3) {
+      const uint32_t* ix = d->indices + mesh.index_offset + i;
+      F3 p0 = transformPoint(inst.world_from_local, vpos(d->vertices[ix[0]]));
+      F3 p1 = transformPoint(inst.world_from_local, vpos(d->vertices[ix[1]]));
+      F3 p2 = transformPoint(inst.world_from_local, vpos(d->vertices[ix[2]]));
+      F3 c = cross3(sub(p1, p0), sub(p2, p0));
+      float area = std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z) * 0.5f;
+      if (area <= 0.0f) continue;
+      float w = luminance(base);
+      if (w <= 0.0f) continue;
+      DevEmissivePrim e{};
+      e.v0[0] = p0.x; e.v0[1] = p0.y; e.v0[2] = p0.z;
+      e.v1[0] = p1.x; e.v1[1] = p1.y; e.v1[2] = p1.z;
+      e.v2[0] = p2.x; e.v2[1] = p2.y; e.v2[2] = p2.z;
+      e.emission[0] = base.x; e.emission[1] = base.y; e.emission[2] = base.z;
+      e.area = area;
+      e.weight = area * w;
+      s.eprim.push_back(e);
+      s.total_weight += e.weight;
+    }
+  }
+  if (s.total_weight > 0.0f)
+    for (auto& e : s.eprim) e.weight /= s.total_weight;
+  {
+    std::vector<double> w(s.eprim.size());
+    for (size_t i = 0; i < w.size(); ++i) w[i] = static_cast<double>(s.eprim[i].weight);
+    std::vector<cg_alias_entry> a(w.size());
+    buildAliasTable(w.data(), static_cast<uint32_t>(w.size()), a.data());
+    s.alias.resize(a.size());
+    for (size_t i = 0; i < a.size(); ++i) s.alias[i] = DevAlias{a[i].alias, a[i].prob};
+  }
+
+  // ---- light BVH for the light-pdf sum (pdf/emission.wesl:120-149) ------------------------
+  {
+    std::vector<Box> boxes(s.eprim.size());
+    for (size_t i = 0; i < s.eprim.size(); ++i) {
+      const DevEmissivePrim& e = s.eprim[i];
+      Box& b = boxes[i];
+      for (int a = 0; a < 3; ++a) {
+        b.lo[a] = std::min(std::min(e.v0[a], e.v1[a]), e.v2[a]);
+        b.hi[a] = std::max(std::max(e.v0[a], e.v1[a]), e.v2[a]);
+      }
+    }
+    BvhBuildOptions opt;
+    opt.max_leaf = 4;
+    std::vector<uint32_t> lorder;
+    buildBvh(boxes, opt, 0, s.light_bvh, lorder);
+    for (uint32_t k = 0; k < lorder.size(); ++k) {
+      const DevEmissivePrim& e = s.eprim[lorder[k]];
+      DevLightTri lt{};
+      F3 v0{e.v0[0], e.v0[1], e.v0[2]}, v1{e.v1[0], e.v1[1], e.v1[2]}, v2{e.v2[0], e.v2[1], e.v2[2]};
+      F3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+      F3 n = cross3(e1, e2);
+      float len = std::sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+      lt.v0[0] = v0.x; lt.v0[1] = v0.y; lt.v0[2] = v0.z;
+      lt.e1[0] = e1.x; lt.e1[1] = e1.y; lt.e1[2] = e1.z;
+      lt.e2[0] = e2.x; lt.e2[1] = e2.y; lt.e2[2] = e2.z;
+      lt.n[0] = n.x / len; lt.n[1] = n.y / len; lt.n[2] = n.z / len;
+      lt.area_pdf = std::fmax(e.weight / e.area, 1e-3f);
+      s.ltri.push_back(lt);
+    }
+  }
+
+  // ---- environment (scene_data.h:57-98) ---------------------------------------------------
+  if (d->env_rgba32f) {
+    s.env_w = d->env_width;
+    s.env_h = d->env_height;
+    s.env.assign(d->env_rgba32f, d->env_rgba32f + size_t(s.env_w) * s.env_h * 4);
+  } else {
+    s.env_w = 512;
+    s.env_h = 256;
+    s.env.resize(size_t(512) * 256 * 4);
+    for (uint32_t y = 0; y < 256; ++y) {
+      float t = static_cast<float>(y) / static_cast<float>(255);
+      float c[3] = {0.7f * (1.0f - t) + 0.05f * t, 0.8f * (1.0f - t) + 0.05f * t,
+                    1.0f * (1.0f - t) + 0.06f * t};
+      for (uint32_t x = 0; x < 512; ++x) {
+        float* p = &s.env[(size_t(y) * 512 + x) * 4];
+        p[0] = c[0];
+        p[1] = c[1];
+        p[2] = c[2];
+        p[3] = 1.0f;
+      }
+    }
+  }
+  return CG_OK;
+}
+
+}  // namespace cg

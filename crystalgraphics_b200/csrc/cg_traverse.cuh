@@ -1,0 +1,198 @@
+// cg_traverse.cuh — two-level BVH traversal on sm_100a.
+//
+// Closest hit (rayTraverseTlas / rayTraverseBlas, structural/bvh.wesl:52-186)
+// and t-bounded any hit (the shadow test of trace.wesl:91-113) over the
+// BvhNode layout of cg_types.h.  Unlike the reference, which walks every
+// overlapping node, boxes beyond the current closest hit are skipped and the
+// nearer child is visited first; the closest hit is the same except for
+// exact ties.  The ray->instance transform and Möller–Trumbore
+// (bvh.wesl:84-88, 188-221) use explicitly rounded intrinsics in the
+// reference's operation order, so t, u, v are bit-identical to it.
+#ifndef CG_TRAVERSE_CUH_
+#define CG_TRAVERSE_CUH_
+
+#include <climits>
+#include <cstdint>
+
+#include "cg_types.h"
+
+namespace cg {
+namespace dev {
+
+#define XM(a, b) __fmul_rn((a), (b))
+#define XA(a, b) __fadd_rn((a), (b))
+#define XS(a, b) __fsub_rn((a), (b))
+
+constexpr int kStackSize = 64;
+constexpr int32_t kToTlas = INT_MIN;      // marker: return to the TLAS
+constexpr int32_t kDone = INT_MIN + 1;    // empty stack
+
+struct TravCounters {
+  uint32_t nodes, tris, insts;
+};
+
+struct HitRec {
+  float t, u, v;
+  int32_t inst;   // -1: miss
+  uint32_t tri;   // global triangle slot
+};
+
+__device__ __forceinline__ float safeInv(float d) {
+  return 1.0f / (fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d));
+}
+
+// Möller–Trumbore on precomputed v0 / e1 = v1 - v0 / e2 = v2 - v0.
+__device__ __forceinline__ bool intersectTri(float ox, float oy, float oz, float dx, float dy,
+                                             float dz, float4 a, float4 b, float4 c, float& t,
+                                             float& u, float& v) {
+  // h = cross(dir, e2)
+  const float hx = XS(XM(dy, c.z), XM(c.y, dz));
+  const float hy = XS(XM(dz, c.x), XM(c.z, dx));
+  const float hz = XS(XM(dx, c.y), XM(c.x, dy));
+  const float det = XA(XA(XM(b.x, hx), XM(b.y, hy)), XM(b.z, hz));
+  if (det > -1e-6f && det < 1e-6f) return false;
+  const float f = __fdiv_rn(1.0f, det);
+  const float sx = XS(ox, a.x), sy = XS(oy, a.y), sz = XS(oz, a.z);
+  u = XM(f, XA(XA(XM(sx, hx), XM(sy, hy)), XM(sz, hz)));
+  if (u < 0.0f || u > 1.0f) return false;
+  // q = cross(s, e1)
+  const float qx = XS(XM(sy, b.z), XM(b.y, sz));
+  const float qy = XS(XM(sz, b.x), XM(b.z, sx));
+  const float qz = XS(XM(sx, b.y), XM(b.x, sy));
+  v = XM(f, XA(XA(XM(dx, qx), XM(dy, qy)), XM(dz, qz)));
+  if (v < 0.0f || XA(u, v) > 1.0f) return false;
+  t = XM(f, XA(XA(XM(c.x, qx), XM(c.y, qy)), XM(c.z, qz)));
+  return t > 1e-6f;
+}
+
+// Ray -> instance space, ((m0 x + m1 y) + m2 z) + m3 w, rounded per op.
+__device__ __forceinline__ void toLocal(const float* m, float ox, float oy, float oz, float dx,
+                                        float dy, float dz, float& lox, float& loy, float& loz,
+                                        float& ldx, float& ldy, float& ldz) {
+  lox = XA(XA(XA(XM(m[0], ox), XM(m[1], oy)), XM(m[2], oz)), m[3]);
+  loy = XA(XA(XA(XM(m[4], ox), XM(m[5], oy)), XM(m[6], oz)), m[7]);
+  loz = XA(XA(XA(XM(m[8], ox), XM(m[9], oy)), XM(m[10], oz)), m[11]);
+  ldx = XA(XA(XM(m[0], dx), XM(m[1], dy)), XM(m[2], dz));
+  ldy = XA(XA(XM(m[4], dx), XM(m[5], dy)), XM(m[6], dz));
+  ldz = XA(XA(XM(m[8], dx), XM(m[9], dy)), XM(m[10], dz));
+}
+
+// kAny: stop at the first hit with t < tmax (returns inst >= 0 if one).
+// kCount: accumulate node / triangle / instance counters.
+template <bool kAny, bool kCount>
+__device__ __forceinline__ HitRec traceRay(const SceneView& sc, float wox, float woy, float woz,
+                                           float wdx, float wdy, float wdz, float tmax,
+                                           TravCounters& cnt, uint32_t* status) {
+  HitRec best{tmax, 0.0f, 0.0f, -1, 0u};
+  if (!sc.has_tlas) return best;
+  int32_t stack[kStackSize];
+  int sp = 0;
+  const BvhNode* nodes = sc.tlas;
+  bool in_blas = false;
+  int32_t cur_inst = -1;
+  float ox = wox, oy = woy, oz = woz, dx = wdx, dy = wdy, dz = wdz;
+  float idx = safeInv(dx), idy = safeInv(dy), idz = safeInv(dz);
+  float oix = ox * idx, oiy = oy * idy, oiz = oz * idz;
+  int32_t node = 0;
+  while (true) {
+    while (node >= 0) {
+      const float4* np = reinterpret_cast<const float4*>(nodes + node);
+      const float4 n0 = __ldg(np);
+      const float4 n1 = __ldg(np + 1);
+      const float4 n2 = __ldg(np + 2);
+      const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+      if (kCount) ++cnt.nodes;
+      const float a0 = fmaf(n0.x, idx, -oix), a1 = fmaf(n0.y, idx, -oix);
+      const float b0 = fmaf(n0.z, idy, -oiy), b1 = fmaf(n0.w, idy, -oiy);
+      const float c0 = fmaf(n2.x, idz, -oiz), c1 = fmaf(n2.y, idz, -oiz);
+      const float t0min = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
+      const float t0max = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), best.t));
+      const float d0 = fmaf(n1.x, idx, -oix), d1 = fmaf(n1.y, idx, -oix);
+      const float e0 = fmaf(n1.z, idy, -oiy), e1 = fmaf(n1.w, idy, -oiy);
+      const float f0 = fmaf(n2.z, idz, -oiz), f1 = fmaf(n2.w, idz, -oiz);
+      const float t1min = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), 0.0f));
+      const float t1max = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), best.t));
+      const bool h0 = t0min <= t0max;
+      const bool h1 = t1min <= t1max;
+      if (h0 && h1) {
+        int32_t near = n3.x, far = n3.y;
+        if (t1min < t0min) {
+          near = n3.y;
+          far = n3.x;
+        }
+        if (sp >= kStackSize) {
+          atomicOr(status, 1u);
+          return HitRec{tmax, 0.0f, 0.0f, -1, 0u};
+        }
+        stack[sp++] = far;
+        node = near;
+      } else if (h0) {
+        node = n3.x;
+      } else if (h1) {
+        node = n3.y;
+      } else {
+        node = sp > 0 ? stack[--sp] : kDone;
+      }
+    }
+    if (node == kDone) break;
+    if (node == kToTlas) {
+      nodes = sc.tlas;
+      in_blas = false;
+      ox = wox; oy = woy; oz = woz;
+      dx = wdx; dy = wdy; dz = wdz;
+      idx = safeInv(dx); idy = safeInv(dy); idz = safeInv(dz);
+      oix = ox * idx; oiy = oy * idy; oiz = oz * idz;
+      node = sp > 0 ? stack[--sp] : kDone;
+      continue;
+    }
+    const uint32_t first = static_cast<uint32_t>(~node) >> 3;
+    const uint32_t count = static_cast<uint32_t>(~node) & 7u;
+    if (!in_blas) {
+      if (count == 0u) {
+        node = sp > 0 ? stack[--sp] : kDone;
+        continue;
+      }
+      // instance leaf: enter its BLAS in local space
+      const DevInstance* ip = sc.inst + first;
+      const float4* ipf = reinterpret_cast<const float4*>(ip);
+      const float4 r0 = __ldg(ipf), r1 = __ldg(ipf + 1), r2 = __ldg(ipf + 2);
+      const uint4 meta = __ldg(reinterpret_cast<const uint4*>(ipf + 3));
+      const float m[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+      if (kCount) ++cnt.insts;
+      toLocal(m, wox, woy, woz, wdx, wdy, wdz, ox, oy, oz, dx, dy, dz);
+      idx = safeInv(dx); idy = safeInv(dy); idz = safeInv(dz);
+      oix = ox * idx; oiy = oy * idy; oiz = oz * idz;
+      if (sp >= kStackSize) {
+        atomicOr(status, 1u);
+        return HitRec{tmax, 0.0f, 0.0f, -1, 0u};
+      }
+      stack[sp++] = kToTlas;
+      nodes = sc.blas;
+      in_blas = true;
+      cur_inst = static_cast<int32_t>(first);
+      node = static_cast<int32_t>(meta.x);  // blas_root
+      continue;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+      const float4* tp = sc.tris + 3u * (first + k);
+      const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
+      if (kCount) ++cnt.tris;
+      float t, u, v;
+      if (intersectTri(ox, oy, oz, dx, dy, dz, ta, tb, tc, t, u, v) && t < best.t) {
+        best.t = t;
+        best.u = u;
+        best.v = v;
+        best.inst = cur_inst;
+        best.tri = first + k;
+        if (kAny) return best;
+      }
+    }
+    node = sp > 0 ? stack[--sp] : kDone;
+  }
+  return best;
+}
+
+}  // namespace dev
+}  // namespace cg
+
+#endif

@@ -1,0 +1,116 @@
+// cg_types.h — device data layout of the B200 path-tracing backend, shared by
+// host packing (cg_scene.cpp) and the kernels (cg_kernels.cu).
+//
+// Everything the traversal reads is 16-byte aligned and fetched with 128-bit
+// loads:
+//   BvhNode      64 B  two child boxes + child links (binary BVH, both
+//                      children tested per visit)
+//   triangle     48 B  v0 | e1 | e2 (Möller–Trumbore operands, precomputed
+//                      on the host with the same float subtraction the
+//                      reference does per test, so t/u/v are bit-identical)
+//   DevInstance  64 B  world->local rows + BLAS root + material
+// Shading-only data (vertex normals, materials) is touched once per hit.
+#ifndef CG_TYPES_H_
+#define CG_TYPES_H_
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define CG_HD __host__ __device__
+#else
+#define CG_HD
+#endif
+
+namespace cg {
+
+// One binary BVH node; children are described in the node itself.
+// child >= 0: inner node index; child < 0: leaf, ~child = first primitive,
+// count in cnt.  An absent child has a point box at 1e30 and count 0.
+struct alignas(16) BvhNode {
+  float c0lx, c0hx, c0ly, c0hy;  // child 0: x and y slabs
+  float c1lx, c1hx, c1ly, c1hy;  // child 1: x and y slabs
+  float c0lz, c0hz, c1lz, c1hz;  // z slabs of both children
+  int32_t child0, child1;
+  uint32_t cnt0, cnt1;
+};
+static_assert(sizeof(BvhNode) == 64, "BvhNode is 64 bytes");
+
+struct alignas(16) DevInstance {
+  float inv[12];        // row-major world -> local (3x4)
+  uint32_t blas_root;   // node index of the mesh BLAS root
+  uint32_t material;
+  uint32_t tri_base;    // first triangle of the mesh in the global arrays
+  uint32_t mesh;
+};
+static_assert(sizeof(DevInstance) == 64, "DevInstance is 64 bytes");
+
+// Pre-decoded material (the fields shading/material.wesl:19-53 reads, with
+// the clamps and max(emissive * strength, 0) that do not depend on the
+// wavelength already applied).
+struct alignas(16) DevMaterial {
+  float base[3];
+  float metallic;         // clamp(metallic, 0, 1)
+  float emission[3];      // max(emissive_factor * emissive_strength, 0)
+  float roughness;        // clamp(roughness, 0, 1)
+  float ior;
+  float dispersion;
+  float transmission;     // clamp(transmission, 0, 1)
+  uint32_t volume;        // thickness_factor > 0
+};
+static_assert(sizeof(DevMaterial) == 48, "DevMaterial is 48 bytes");
+
+// Emissive triangle for the light-pdf sum (pdf/emission.wesl:120-179):
+// v0, e1, e2, the normalised light normal and max(weight / area, 1e-3).
+struct alignas(16) DevLightTri {
+  float v0[3];
+  float area_pdf;
+  float e1[3];
+  float _p1;
+  float e2[3];
+  float _p2;
+  float n[3];
+  float _p3;
+};
+static_assert(sizeof(DevLightTri) == 64, "DevLightTri is 64 bytes");
+
+// Mirror of cg_emissive_prim / EmissivePrim (80 B).
+struct alignas(16) DevEmissivePrim {
+  float v0[3], _p0;
+  float v1[3], _p1;
+  float v2[3], _p2;
+  float emission[3];
+  float area;
+  float weight;
+  float _pad[3];
+};
+static_assert(sizeof(DevEmissivePrim) == 80, "DevEmissivePrim is 80 bytes");
+
+struct DevAlias {
+  uint32_t alias;
+  float prob;
+};
+
+// Device pointers of an uploaded scene (passed to kernels by value).
+struct SceneView {
+  const BvhNode* tlas;         // TLAS nodes (root 0); leaves hold instances
+  const BvhNode* blas;         // all BLAS nodes
+  const float4* tris;          // 3 float4 per triangle: (v0, orig id bits) (e1) (e2)
+  const uint4* tri_vidx;       // vertex indices per triangle (i0, i1, i2, _)
+  const float4* vnormal;       // vertex normals
+  const DevInstance* inst;
+  const DevMaterial* mat;
+  const DevEmissivePrim* eprim;
+  const DevAlias* alias;
+  const BvhNode* light_bvh;    // over DevLightTri
+  const DevLightTri* light_tri;
+  const float4* env;           // env_w * env_h texels
+  uint32_t env_w, env_h;
+  uint32_t emissive_count;
+  uint32_t instance_count;
+  uint32_t has_tlas;
+  uint32_t has_lights;
+};
+
+}  // namespace cg
+
+#endif

@@ -1,0 +1,353 @@
+/*
+ * cg_cuda.h — C ABI of the B200 spectral path-tracing backend (libcg_cuda.so).
+ *
+ * This is the drop-in boundary for the View() hot path of
+ * ray847/CrystalGraphics.  The reference renders through WebGPU:
+ *   View(scene, camera)                    src/view.cpp:12-16
+ *   └ Env::View → SceneData (host packing) src/environment.cpp:69-74
+ *     └ wgpu::Env::View (upload, dispatch) src/wgpu/view.cpp:16-88
+ *       └ compute.wesl main (per pixel)    src/wgpu/shader/compute.wesl:32-62
+ * Here the same work is a set of plain C entry points over plain pointers and
+ * sizes.  The C++23 layer (include/CrystalGraphics/) keeps the reference's
+ * public signatures and calls these; Python reaches them through ctypes.
+ *
+ * Conventions
+ *   - Every function returns an int status: CG_OK (0) or a negative CG_E_*
+ *     code.  cg_last_error() returns a thread-local message for the last
+ *     failure on the calling thread.  No C++ exception crosses this ABI.
+ *   - Host pointers are plain host memory.  The library owns every device
+ *     allocation it makes; handles are opaque.
+ *   - There is no CPU fallback: with no CUDA device every call that needs
+ *     one fails with CG_E_CUDA.
+ */
+#ifndef CG_CUDA_H_
+#define CG_CUDA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CG_API __attribute__((visibility("default")))
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  CG_OK = 0,
+  CG_E_INVALID = -1,     /* bad argument, size or handle                     */
+  CG_E_NOT_INIT = -2,    /* cg_init() not called ("Environment not initialized.") */
+  CG_E_CUDA = -3,        /* a CUDA runtime call failed                       */
+  CG_E_OOM = -4,         /* device allocation failed or over the HBM budget  */
+  CG_E_TIMEOUT = -5,     /* a bounded device or host wait ran out            */
+  CG_E_DEVICE = -6,      /* a kernel reported an error in its status word    */
+  CG_E_CANCELLED = -7,   /* a served request was cancelled                   */
+  CG_E_BUSY = -8         /* a queue is full; retry later                     */
+};
+
+/* ---- configuration ------------------------------------------------------
+ * Mirrors PathTraceConf (include/CrystalGraphics/environment.h:11-18).
+ * window_* are accepted and ignored: the backend is headless.  trace_depth is
+ * clamped to [1, 64] as wgpu::CreateEnv does (src/wgpu/environment.cpp:20).
+ * The max_*_sample_count fields become the override constants @id(5..8) of
+ * shading/sample.wesl:102-105 and are further capped by its constants
+ * (sample.wesl:98-101). */
+typedef struct cg_conf {
+  uint32_t window_width, window_height;
+  uint32_t render_width, render_height;
+  uint32_t sample_count;
+  uint32_t trace_depth;
+  uint32_t max_transport_sample_count, max_diffuse_sample_count,
+      max_rough_sample_count, max_emission_sample_count;
+} cg_conf;
+
+/* ---- camera --------------------------------------------------------------
+ * Same 48-byte layout as crystal::graphics::Camera (camera.h:9-13):
+ * alignas(16) vec3 position, alignas(16) vec3 direction, alignas(8) vec2 viewport. */
+typedef struct cg_camera {
+  float position[3];
+  float _pad0;
+  float direction[3];
+  float _pad1;
+  float viewport[2];
+  float _pad2[2];
+} cg_camera;
+
+/* ---- scene description (the input of LoadScene) ---------------------------
+ * cg_vertex has the layout of the reference Vertex (src/vertex.h:12-24). */
+typedef struct cg_vertex {
+  float position[3];
+  float _pad0;
+  float normal[3];
+  float _pad1;
+  float tex_coord0[2];
+  float tex_coord1[2];
+} cg_vertex;
+
+/* A mesh is one glTF mesh primitive's geometry: a range of the global index
+ * buffer whose entries are absolute vertex indices (Primitive,
+ * src/scene_impl.h:24-30, without its material). */
+typedef struct cg_mesh {
+  uint32_t vertex_offset, vertex_count;
+  uint32_t index_offset, index_count;
+} cg_mesh;
+
+/* An instance is one placed primitive: the reference builds one BLAS and one
+ * Instance per (node, mesh primitive) (src/pathtracing/tlas.h:56-73,
+ * src/pathtracing/instance.h:9-17).  Here instances that name the same mesh
+ * share one BLAS on the device; the geometry and every hit are identical.
+ * world_from_local is a row-major 3x4 affine matrix. */
+typedef struct cg_instance {
+  float world_from_local[12];
+  uint32_t mesh;
+  uint32_t material;
+  uint32_t _pad[2];
+} cg_instance;
+
+/* The material fields the path tracer reads out of the reference's
+ * PackedMaterial (src/material.h:30-87, shading/material.wesl:19-53).
+ * Texture references are glTF texture indices (-1 = none); this backend
+ * renders untextured scenes and rejects materials that name a texture. */
+typedef struct cg_material {
+  float base_color_factor[4];
+  float emissive_factor[3];
+  float emissive_strength;
+  float metallic_factor;
+  float roughness_factor;
+  float ior;
+  float dispersion;
+  float transmission_factor;
+  float thickness_factor;
+  int32_t base_color_texture;
+  int32_t metallic_roughness_texture;
+  int32_t emissive_texture;
+  int32_t transmission_texture;
+  uint32_t _pad[2];
+} cg_material;
+
+/* env_rgba32f == NULL selects the reference's fallback sky: a 512x256
+ * vertical gradient (src/pathtracing/scene_data.h:73-98). */
+typedef struct cg_scene_desc {
+  const cg_vertex* vertices;
+  uint32_t vertex_count;
+  const uint32_t* indices;
+  uint32_t index_count;
+  const cg_mesh* meshes;
+  uint32_t mesh_count;
+  const cg_instance* instances;
+  uint32_t instance_count;
+  const cg_material* materials;
+  uint32_t material_count;
+  const float* env_rgba32f;
+  uint32_t env_width, env_height;
+} cg_scene_desc;
+
+typedef struct cg_scene_s* cg_scene_t;
+
+/* ---- environment (EnvInit / EnvTerm / EnvStatus) -------------------------
+ * cg_init replaces EnvInit (environment.h:20, src/environment.cpp:12-17):
+ * it selects the CUDA device, creates the stream, the wavelength tables and
+ * the film of render_width x render_height.  Calling it again re-creates the
+ * environment. */
+CG_API int cg_init(const cg_conf* conf, int device);
+/* EnvTerm (src/environment.cpp:18-23).  Safe to call when not initialised. */
+CG_API int cg_term(void);
+/* EnvStatus (src/environment.cpp:34-37): 1 when initialised. */
+CG_API int cg_status(void);
+/* Thread-local message of the last failure on this thread ("" if none). */
+CG_API const char* cg_last_error(void);
+/* Effective configuration after clamping. */
+CG_API int cg_get_conf(cg_conf* out);
+
+/* ---- scenes (LoadScene, ~Scene) ------------------------------------------
+ * Builds the BVHs, the emissive buffer and its alias table on the host and
+ * uploads them with the geometry, materials and environment into device
+ * buffers, once.  The reference rebuilds these on every View()
+ * (src/environment.cpp:70); the uploaded scene is immutable. */
+CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out);
+CG_API int cg_scene_destroy(cg_scene_t scene);
+/* LoadScene(path) (src/scene.cpp:829-1003): reads a glTF 2.0 file (.gltf with
+ * .bin or data-URI buffers, or .glb) with the reference's conventions —
+ * material 0 is the default material and glTF material i becomes i + 1, one
+ * instance per (node, mesh primitive), y-up rotated to z-up — and uploads it
+ * as cg_scene_create does. */
+CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out);
+
+typedef struct cg_scene_info {
+  uint32_t instance_count, mesh_count, triangle_count, material_count;
+  uint32_t emissive_count;      /* emissive triangles (EmissivePrim entries) */
+  uint32_t blas_node_count, tlas_node_count, light_node_count;
+  uint64_t device_bytes;        /* device memory held by the scene           */
+  uint64_t tag;                 /* unique per cg_scene_create (Scene::Impl::tag_) */
+} cg_scene_info;
+CG_API int cg_scene_get_info(cg_scene_t scene, cg_scene_info* out);
+
+/* EmissivePrim (src/pathtracing/emissive_buffer.h:27-40), 80 bytes. */
+typedef struct cg_emissive_prim {
+  float v0[3]; float _p0;
+  float v1[3]; float _p1;
+  float v2[3]; float _p2;
+  float emission[3];
+  float area;
+  float weight;
+  float _pad[3];
+} cg_emissive_prim;
+/* AliasTableEntry (src/pathtracing/alias_table.h:14-17), 8 bytes. */
+typedef struct cg_alias_entry {
+  uint32_t alias;
+  float prob;
+} cg_alias_entry;
+
+/* Copies the scene's emissive buffer and alias table, read back from the
+ * device buffers the kernels sample, into host arrays of `capacity`
+ * entries.  *count receives the entry count; with both arrays NULL the call
+ * only reports the count. */
+CG_API int cg_scene_read_emissive(cg_scene_t scene, cg_emissive_prim* prims,
+                                  cg_alias_entry* alias, uint32_t capacity,
+                                  uint32_t* count);
+
+/* Builds an alias table on the host from `count` weights, the way
+ * AliasTable's constructor does (src/pathtracing/alias_table.h:24-70). */
+CG_API int cg_alias_build(const double* weights, uint32_t count,
+                          cg_alias_entry* out);
+
+/* ---- View (the hot path) ---------------------------------------------------
+ * One progressive frame of `scene` from `camera` into the environment's film:
+ * conf.sample_count samples per pixel, the running mean of CIE XYZ kept while
+ * the scene and the camera stay the same (src/wgpu/frame_history.h:12-23,
+ * compute.wesl:41-56), then the sRGB resolve (physics/srgb.wesl:5-27).
+ * Synchronous up to the film on the device; read it with cg_film_read. */
+CG_API int cg_view(cg_scene_t scene, const cg_camera* camera);
+
+enum {
+  CG_FILM_XYZ32F = 0,   /* running-mean XYZ, 3 floats per pixel (12 B/px)   */
+  CG_FILM_RGBA8 = 1,    /* sRGB rgba8unorm, what the reference blits (4 B/px) */
+  CG_FILM_RGB32F = 2    /* linear sRGB before the transfer curve (12 B/px)   */
+};
+/* Copies the film into `host` (row-major, row y = pixel.y of cameraRay). */
+CG_API int cg_film_read(void* host, size_t bytes, int format);
+/* Frames accumulated so far in the film (iter_count + 1 after a View). */
+CG_API int cg_film_frames(uint32_t* frames);
+
+/* Per-View statistics of the last cg_view / batch on this environment. */
+typedef struct cg_stats {
+  uint64_t samples;          /* camera-path samples (pixels x spp)            */
+  uint64_t extend_rays;      /* closest-hit rays traced (all depths)          */
+  uint64_t shadow_rays;      /* shadow rays traced                            */
+  uint64_t node_visits;      /* BVH node visits (counting build only, else 0) */
+  uint64_t tri_tests;        /* triangle tests (counting build only, else 0)  */
+  uint64_t inst_visits;      /* instance entries (counting build only, else 0)*/
+  uint32_t chunks;           /* wavefront chunks the work was split into      */
+  uint32_t kernel_launches;  /* kernels this library launched                 */
+  float device_ms;           /* CUDA-event time of the device work            */
+} cg_stats;
+CG_API int cg_last_stats(cg_stats* out);
+/* 1 = count node visits / triangle tests in the traversal kernels (slower;
+ * for the roofline's algorithmic bytes), 0 = off (default). */
+CG_API int cg_set_counting(int enable);
+
+/* Selects the RNG seed of the keyed sample streams (default 0). */
+CG_API int cg_set_seed(uint32_t seed);
+
+/* Per-kernel device time of the environment's View() / batch launches,
+ * recorded with CUDA events on the launching stream while profiling is on
+ * (batches then run without graph capture).  Index: CG_K_* */
+enum { CG_K_GEN = 0, CG_K_EXTEND = 1, CG_K_SHADE = 2, CG_K_SHADOW = 3, CG_K_RESOLVE = 4,
+       CG_K_COUNT = 5 };
+typedef struct cg_profile {
+  double ms[CG_K_COUNT];
+  uint64_t launches[CG_K_COUNT];
+} cg_profile;
+CG_API int cg_set_profiling(int enable);
+/* Reads and clears the accumulated per-kernel times. */
+CG_API int cg_profile_read(cg_profile* out);
+
+/* ---- ray queries (parity) --------------------------------------------------
+ * Closest hit of `n` world-space rays, each 8 floats (ox, oy, oz, _, dx, dy,
+ * dz, _), against the scene, as rayTraverseTlas/rayTraverseBlas compute it
+ * (structural/bvh.wesl:52-186): t is the smallest Möller–Trumbore distance
+ * below 1e6.  instance = -1 marks a miss. */
+typedef struct cg_hit {
+  float t, u, v;
+  int32_t instance;
+  int32_t triangle;  /* triangle index within the instance's mesh (original order) */
+  int32_t _pad[3];
+} cg_hit;
+CG_API int cg_trace_closest(cg_scene_t scene, const float* rays, uint32_t n,
+                            cg_hit* hits);
+
+/* ---- batched form ------------------------------------------------------------
+ * Renders many views of one scene, of uneven resolution and spp, in one
+ * wavefront over shared ray queues.  Each view writes a fresh film (one frame,
+ * no history).  `films_xyz` receives, per view, width*height*3 floats
+ * (running-mean XYZ) concatenated in view order; `films_rgba8` (may be NULL)
+ * receives width*height*4 bytes per view.  The launch sequence is captured as
+ * a CUDA graph per (scene, batch) and replayed. */
+typedef struct cg_view_desc {
+  cg_camera camera;
+  uint32_t width, height;
+  uint32_t spp;
+  uint32_t seed;        /* stream seed of this view's samples               */
+} cg_view_desc;
+CG_API int cg_batch_render(cg_scene_t scene, const cg_view_desc* views,
+                           uint32_t view_count, float* films_xyz,
+                           uint8_t* films_rgba8);
+
+/* Wavefront tuning: rays per level queue (capacity), threads per block of the
+ * traversal and shading kernels.  0 = keep.  cg_autotune searches these for a
+ * scene and a representative view and keeps the best. */
+typedef struct cg_tuning {
+  uint32_t queue_capacity;
+  uint32_t extend_block;
+  uint32_t shade_block;
+  uint32_t use_graph;   /* 1 = capture the chunk pipeline as a CUDA graph */
+} cg_tuning;
+CG_API int cg_set_tuning(const cg_tuning* tuning);
+CG_API int cg_get_tuning(cg_tuning* out);
+CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view,
+                       cg_tuning* best);
+
+/* ---- served form -----------------------------------------------------------
+ * A request loop over several resident scenes.  Requests are admitted while
+ * their film plus path-state bytes fit the HBM budget, batched with the work
+ * already on the GPU at chunk granularity (continuous batching), and
+ * completed independently.  Per-request sample streams are keyed by
+ * (request seed, pixel, sample), so a request's result does not depend on
+ * what it was batched with. */
+typedef struct cg_server_s* cg_server_t;
+typedef struct cg_request {
+  uint32_t scene;       /* index into the server's scene list */
+  cg_view_desc view;
+} cg_request;
+typedef struct cg_request_result {
+  int32_t status;       /* CG_OK, CG_E_CANCELLED, ...              */
+  uint32_t _pad;
+  double submit_s, start_s, finish_s;   /* host clock (seconds)     */
+} cg_request_result;
+CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count,
+                            uint64_t hbm_budget_bytes, cg_server_t* out);
+CG_API int cg_server_destroy(cg_server_t server);
+/* Queues a request; its XYZ film (width*height*3 floats) is written into
+ * `film_xyz`, which must stay valid until the request completes. */
+CG_API int cg_server_submit(cg_server_t server, const cg_request* request,
+                            float* film_xyz, uint64_t* request_id);
+/* Waits up to timeout_ms (-1 = forever) for the request to complete. */
+CG_API int cg_server_wait(cg_server_t server, uint64_t request_id,
+                          int timeout_ms, cg_request_result* result);
+CG_API int cg_server_cancel(cg_server_t server, uint64_t request_id);
+typedef struct cg_server_stats {
+  uint64_t submitted, completed, cancelled, rejected;
+  uint64_t samples;
+  uint32_t active, pending;
+  uint64_t bytes_in_use, peak_bytes;
+} cg_server_stats;
+CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out);
+
+/* Library version string. */
+CG_API const char* cg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CG_CUDA_H_ */

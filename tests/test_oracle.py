@@ -1,0 +1,146 @@
+"""The oracle (CPU restatement of the reference) checked against the
+reference's own alias_table.h fixtures and against independent Python
+restatements of the reference's small formulas."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from crystalgraphics_b200 import _abi, scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_oracle_alias_matches_reference_golden():
+    g = np.load(os.path.join(ROOT, "tests", "golden", "alias_tables.npz"))
+    for name in sorted({k.split("__")[0] for k in g.files}):
+        out = O.alias_build(g[f"{name}__w"])
+        np.testing.assert_array_equal(out["alias"], g[f"{name}__alias"], err_msg=name)
+        assert out["prob"].tobytes() == g[f"{name}__prob"].tobytes(), name
+
+
+@pytest.mark.skipif(not O.ref_alias_available(), reason="reference tree not built here")
+def test_oracle_alias_matches_reference_live():
+    rng = np.random.default_rng(7)
+    for n in (1, 2, 3, 17, 1000):
+        w = rng.exponential(size=n)
+        a = O.alias_build(w)
+        r = O.ref_alias_build(w)
+        assert a.tobytes() == r.tobytes()
+
+
+def pcg_hash_stream(seed, n):
+    """math/rng.wesl:1-22 in Python integers."""
+    M = 0xFFFFFFFF
+
+    def step(s):
+        s = (s * 747796405 + 2891336453) & M
+        word = (((s >> ((s >> 28) + 4)) ^ s) * 277803737) & M
+        return ((word >> 22) ^ word) & M
+
+    s = step(seed & M)
+    out = []
+    for _ in range(n):
+        s = step(s)
+        out.append(np.float32(np.float32(s) / np.float32(4294967296.0)))
+    return np.array(out, np.float32), s
+
+
+def test_rng_matches_python_restatement():
+    import ctypes as C
+    for seed in (0, 1, 123456, 0xFFFFFFFF):
+        out = np.zeros(64, np.float32)
+        last = O.lib().oracle_rng_sequence(seed, 64, out.ctypes.data)
+        ref, s = pcg_hash_stream(seed, 64)
+        np.testing.assert_array_equal(out, ref)
+        assert last == s
+        assert np.all(out >= 0) and np.all(out <= 1.0)
+
+
+def test_wavelength_sampling_is_monotone_and_in_range():
+    us = np.linspace(0, 1, 257, dtype=np.float32)
+    lam = []
+    for u in us:
+        p = np.float32(0)
+        import ctypes as C
+        pc = C.c_float()
+        w = O.lib().oracle_sample_wavelength(float(u), C.byref(pc))
+        assert 380.0 <= w <= 720.0
+        assert pc.value >= 1e-6
+        lam.append(w)
+    assert np.all(np.diff(lam) >= 0)
+
+
+def test_xyz_match_peaks_like_cie():
+    xyz = np.zeros(3, np.float32)
+    best = {}
+    for w in range(380, 721, 2):
+        O.lib().oracle_xyz_match(float(w), xyz.ctypes.data)
+        for k in range(3):
+            if xyz[k] > best.get(k, (0, -1))[1]:
+                best[k] = (w, float(xyz[k]))
+    assert 590 <= best[0][0] <= 610   # xbar peak
+    assert 550 <= best[1][0] <= 570   # ybar peak
+    assert 435 <= best[2][0] <= 460   # zbar peak
+
+
+def test_smits_quirk_gives_zero_in_deep_red():
+    # wavelengths in [686, 720) index BINS[10]: NaN, dropped by clamp/max
+    rgb = np.array([0.5, 0.5, 0.5], np.float32)
+    for w in (686.5, 700.0, 719.9):
+        assert O.lib().oracle_rgb_to_reflectance(rgb.ctypes.data, w) == 0.0
+        assert O.lib().oracle_rgb_to_radiance(rgb.ctypes.data, w) == 0.0
+    assert O.lib().oracle_rgb_to_reflectance(rgb.ctypes.data, 550.0) > 0.4
+
+
+def test_emissive_buffer_weights_normalised():
+    s = scenes.icosphere_scene(subdiv=2)
+    os_ = O.OracleScene(s)
+    prims, alias, total = os_.emissive()
+    assert len(prims) == 64
+    assert abs(float(prims["weight"].sum(dtype=np.float64)) - 1.0) < 1e-5
+    # alias table is the reference construction on those weights
+    if O.ref_alias_available():
+        ref = O.ref_alias_build(prims["weight"].astype(np.float64))
+        assert ref.tobytes() == alias.tobytes()
+
+
+def test_oracle_closest_hit_on_axis_aligned_box():
+    s = scenes.cornell()
+    os_ = O.OracleScene(s)
+    # a ray from the camera straight at the back wall (y = 1) through x=0.9, z=1.9
+    rays = np.zeros((1, 8), np.float32)
+    rays[0, :3] = (0.9, -3.0, 1.9)
+    rays[0, 4:7] = (0.0, 1.0, 0.0)
+    hits, t2 = os_.trace_closest(rays)
+    assert hits["instance"][0] == 0  # the white walls
+    assert abs(hits["t"][0] - 4.0) < 1e-5
+
+
+def test_oracle_render_reference_and_keyed_agree_statistically():
+    """The keyed streams change which random numbers a sample uses, not the
+    estimator: both modes converge to the same image."""
+    s = scenes.cornell(64, 64)
+    os_ = O.OracleScene(s)
+    conf = _abi.make_conf(64, 64, 64, 2)
+    a, _, _ = os_.render(conf, s.camera, rng=O.RNG_REFERENCE, prune=True)
+    b, _, _ = os_.render(conf, s.camera, rng=O.RNG_KEYED, prune=True)
+    ma, mb = a.mean(axis=(0, 1)), b.mean(axis=(0, 1))
+    assert np.all(np.abs(ma - mb) / mb < 0.03), (ma, mb)
+
+
+def test_oracle_progressive_running_mean():
+    s = scenes.cornell(32, 32)
+    os_ = O.OracleScene(s)
+    conf = _abi.make_conf(32, 32, 1, 2)
+    film = np.zeros((32, 32, 3), np.float32)
+    seeds = np.zeros((32, 32), np.uint32)
+    f0, s0, _ = os_.render(conf, s.camera, film=film.copy(), seeds=seeds.copy(), iter_count=0,
+                           rng=O.RNG_REFERENCE)
+    f1, s1, _ = os_.render(conf, s.camera, film=f0.copy(), seeds=s0.copy(), iter_count=1,
+                           rng=O.RNG_REFERENCE)
+    assert not np.array_equal(s0, s1)
+    # frame 1 holds the mean of two frames: it is between its parts on average
+    assert abs(float(f1.mean()) - float(f0.mean())) < 0.5 * float(f0.mean())
