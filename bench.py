@@ -113,7 +113,12 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            self.samples.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
+
+    def window(self, t0, t1):
+        """Keep the samples taken inside [t0, t1] (the timed region)."""
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
+        self.samples = inside if inside else self.samples[-1:]
 
     def __exit__(self, *a):
         if self.proc:
@@ -126,11 +131,12 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        rows = [s[1] for s in self.samples]
+        sm = [float(s[0]) for s in rows if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in rows if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for s in self.samples:
+        for s in rows:
             for k, n in enumerate(names):
                 if len(s) > 4 + k and s[4 + k].lower() == "active":
                     reasons.add(n)
@@ -222,6 +228,9 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     samples_per_step = W_ * H_ * SPP_
 
+    if args.queue:
+        B.SetTuning(queue_capacity=args.queue)
+    clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         B.View(g, cam)
     # ---- timed region: device-resident ----
@@ -230,17 +239,20 @@ def run_ours(args):
     dev_ms, launches, wall = [], 0, 0.0
     d.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            B.View(g, cam)
-            wall += time.perf_counter() - t0
-            st = B.LastStats()
-            dev_ms.append(st.device_ms)
-            launches += st.kernel_launches
+    t_begin = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        B.View(g, cam)
+        wall += time.perf_counter() - t0
+        st = B.LastStats()
+        dev_ms.append(st.device_ms)
+        launches += st.kernel_launches
     torch.cuda.synchronize()
+    t_end = time.perf_counter()
+    clocks.__exit__()
+    clocks.window(t_begin, t_end)
     d.barrier()
     prof = B.ReadProfile()
     B.SetProfiling(False)
@@ -330,7 +342,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--case", default="full", choices=["full", "small"],
+                    help="small: the same scene at 320x180, 4 spp, with a 2M-ray queue "
+                         "(the case ncu --set full captures)")
+    ap.add_argument("--queue", type=int, default=0, help="ray queue capacity (0 = default)")
     args = ap.parse_args()
+    if args.case == "small":
+        global W_, H_, SPP_, WORKLOAD
+        W_, H_, SPP_ = 320, 180, 4
+        WORKLOAD = WORKLOAD.replace("1280x720, 16 spp", "320x180, 4 spp")
+        args.queue = args.queue or (2 << 20)
     if args.impl == "reference":
         run_reference(args)
     else:

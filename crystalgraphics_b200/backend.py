@@ -53,6 +53,9 @@ def _load():
         "cg_get_conf": (i, [C.POINTER(_abi.CgConf)]),
         "cg_scene_create": (i, [C.POINTER(_abi.CgSceneDesc), C.POINTER(vp)]),
         "cg_scene_destroy": (i, [vp]),
+        "cg_scene_load_gltf": (i, [C.c_char_p, C.POINTER(vp)]),
+        "cg_gltf_parse": (i, [C.c_char_p, C.POINTER(_abi.CgSceneDesc), C.POINTER(vp)]),
+        "cg_gltf_free": (i, [vp]),
         "cg_scene_get_info": (i, [vp, C.POINTER(_abi.CgSceneInfo)]),
         "cg_scene_read_emissive": (i, [vp, vp, vp, u32, C.POINTER(u32)]),
         "cg_alias_build": (i, [vp, u32, vp]),
@@ -171,7 +174,9 @@ class Scene:
         self.source = source
 
     def FilePath(self):
-        return getattr(self.source, "path", None) or getattr(self.source, "name", "")
+        if isinstance(self.source, str):
+            return self.source
+        return getattr(self.source, "name", "")
 
     @property
     def handle(self) -> int:
@@ -210,12 +215,36 @@ def LoadScene(scene) -> Scene:
     """Uploads a scene.  `scene` is an in-memory description
     (crystalgraphics_b200.scenes.Scene) or a path to a .gltf file."""
     if isinstance(scene, (str, os.PathLike)):
-        from . import gltf
-        scene = gltf.load(scene)
+        h = C.c_void_p()
+        _check(lib.cg_scene_load_gltf(os.fspath(scene).encode(), C.byref(h)))
+        return Scene(h.value, os.fspath(scene))
     desc = scene.desc()
     h = C.c_void_p()
     _check(lib.cg_scene_create(C.byref(desc), C.byref(h)))
     return Scene(h.value, scene)
+
+
+def parse_gltf(path) -> "scenes.Scene":
+    """Parses a glTF file with the native loader (no device needed) into an
+    in-memory scene description (copies)."""
+    from . import scenes
+    d = _abi.CgSceneDesc()
+    st = C.c_void_p()
+    _check(lib.cg_gltf_parse(os.fspath(path).encode(), C.byref(d), C.byref(st)))
+    try:
+        def arr(ptr, n, dtype):
+            if n == 0:
+                return np.zeros(0, dtype)
+            buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr)
+            return np.frombuffer(buf, dtype=dtype, count=n).copy()
+        return scenes.Scene(name=os.fspath(path),
+                            vertices=arr(d.vertices, d.vertex_count, _abi.VERTEX_DTYPE),
+                            indices=arr(d.indices, d.index_count, np.uint32),
+                            meshes=arr(d.meshes, d.mesh_count, _abi.MESH_DTYPE),
+                            instances=arr(d.instances, d.instance_count, _abi.INSTANCE_DTYPE),
+                            materials=arr(d.materials, d.material_count, _abi.MATERIAL_DTYPE))
+    finally:
+        lib.cg_gltf_free(st)
 
 
 def View(scene: Scene, camera: Camera | _abi.CgCamera | None = None) -> None:

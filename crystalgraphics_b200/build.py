@@ -60,6 +60,40 @@ def _compile(src: str, verbose: bool, ptxas_v: bool) -> str:
     return obj
 
 
+CXX_DIR = os.path.join(HERE, "cxx")
+CXX_LIB = os.path.join(HERE, "libcrystalgraphics.so")
+CXX_EXE = os.path.join(HERE, "cg_view")
+
+
+def _stale(out: str, deps: list[str]) -> bool:
+    return not os.path.exists(out) or any(os.path.getmtime(d) > os.path.getmtime(out) for d in deps)
+
+
+def build_cxx(verbose: bool = False) -> str:
+    """The C++23 crystal::graphics layer (libcrystalgraphics.so) and the
+    headless example program (cg_view), linked against libcg_cuda.so."""
+    inc = os.path.join(HERE, "..", "include")
+    headers = [os.path.join(inc, "cg_cuda.h")] + [
+        os.path.join(inc, "CrystalGraphics", f) for f in os.listdir(os.path.join(inc, "CrystalGraphics"))]
+    cxx = os.environ.get("CXX", "g++")
+    common = ["-std=c++23", "-O2", "-fPIC", "-I", inc, "-I", os.path.join(inc, "CrystalGraphics", "..")]
+    src = os.path.join(CXX_DIR, "crystal_graphics.cpp")
+    if _stale(CXX_LIB, [src, LIB] + headers):
+        cmd = [cxx] + common + ["-shared", "-o", CXX_LIB, src, "-L", HERE, "-l:libcg_cuda.so",
+                                "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    main = os.path.join(CXX_DIR, "view_main.cpp")
+    if _stale(CXX_EXE, [main, CXX_LIB] + headers):
+        cmd = [cxx] + common + ["-o", CXX_EXE, main, "-L", HERE, "-l:libcrystalgraphics.so",
+                                "-l:libcg_cuda.so", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CXX_LIB
+
+
 def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sources()
@@ -74,6 +108,7 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_cxx(verbose)
     return LIB
 
 

@@ -17,8 +17,10 @@
 // Material extensions read: KHR_materials_emissive_strength, _ior,
 // _transmission, _volume (thickness), _dispersion.  Textured materials are
 // rejected by the scene packer.
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <fstream>
 #include <map>
 #include <memory>
@@ -260,9 +262,11 @@ struct Loader {
 
   std::vector<cg_vertex> vertices;
   std::vector<uint32_t> indices;
-  std::vector<cg_mesh> meshes;              // one per glTF mesh primitive
-  std::vector<uint32_t> prim_material;      // per cg_mesh
-  std::vector<std::vector<uint32_t>> mesh_prims;  // glTF mesh -> cg_mesh ids
+  std::vector<cg_mesh> meshes;  // one per distinct primitive geometry
+  // glTF mesh -> its primitives as (cg_mesh id, material index)
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> mesh_prims;
+  // primitives that name the same accessors share one cg_mesh (and BLAS)
+  std::map<std::array<int64_t, 5>, uint32_t> geometry_ids;
   std::vector<cg_instance> instances;
   std::vector<cg_material> materials;
 
@@ -407,6 +411,16 @@ struct Loader {
         if (pr.integer("mode", 4) != 4) return fail("only triangle primitives are supported");
         const Json* attrs = pr.get("attributes");
         if (!attrs || !attrs->get("POSITION")) return fail("primitive without POSITION");
+        const int64_t mat = pr.integer("material", -1);
+        const uint32_t mat_idx = mat >= 0 ? static_cast<uint32_t>(mat + 1) : 0u;
+        const std::array<int64_t, 5> key = {attrs->integer("POSITION", -1), attrs->integer("NORMAL", -1),
+                                            attrs->integer("TEXCOORD_0", -1),
+                                            attrs->integer("TEXCOORD_1", -1), pr.integer("indices", -1)};
+        auto seen = geometry_ids.find(key);
+        if (seen != geometry_ids.end()) {
+          mesh_prims.back().push_back({seen->second, mat_idx});
+          continue;
+        }
         std::vector<double> pos, nrm, uv0, uv1, idx;
         size_t nv = 0, n2 = 0;
         if (!readAccessor(attrs->integer("POSITION", -1), 3, pos, nv)) return false;
@@ -438,10 +452,10 @@ struct Loader {
           }
         }
         cg_mesh m{voff, static_cast<uint32_t>(nv), ioff, static_cast<uint32_t>(ni)};
-        const int64_t mat = pr.integer("material", -1);
-        mesh_prims.back().push_back(static_cast<uint32_t>(meshes.size()));
+        const uint32_t id = static_cast<uint32_t>(meshes.size());
+        geometry_ids[key] = id;
+        mesh_prims.back().push_back({id, mat_idx});
         meshes.push_back(m);
-        prim_material.push_back(mat >= 0 ? static_cast<uint32_t>(mat + 1) : 0u);
       }
     }
     return true;
@@ -480,12 +494,12 @@ struct Loader {
     const int64_t mesh = n.integer("mesh", -1);
     if (mesh >= 0) {
       if (size_t(mesh) >= mesh_prims.size()) return fail("bad mesh index");
-      for (uint32_t pm : mesh_prims[mesh]) {
+      for (const auto& [geom, mat] : mesh_prims[mesh]) {
         cg_instance in{};
         for (int rr = 0; rr < 3; ++rr)
           for (int c = 0; c < 4; ++c) in.world_from_local[rr * 4 + c] = static_cast<float>(world.m[c * 4 + rr]);
-        in.mesh = pm;
-        in.material = prim_material[pm] < materials.size() ? prim_material[pm] : 0u;
+        in.mesh = geom;
+        in.material = mat < materials.size() ? mat : 0u;
         instances.push_back(in);
       }
     }
@@ -546,21 +560,40 @@ struct Loader {
 
 using namespace cg;
 
+extern "C" CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage) {
+  if (!path || !out || !storage) return fail(CG_E_INVALID, "null argument");
+  *storage = nullptr;
+  auto L = std::make_unique<Loader>();
+  if (!L->load(path)) return fail(CG_E_INVALID, std::string(path) + ": " + L->err);
+  cg_scene_desc d{};
+  d.vertices = L->vertices.data();
+  d.vertex_count = static_cast<uint32_t>(L->vertices.size());
+  d.indices = L->indices.data();
+  d.index_count = static_cast<uint32_t>(L->indices.size());
+  d.meshes = L->meshes.data();
+  d.mesh_count = static_cast<uint32_t>(L->meshes.size());
+  d.instances = L->instances.data();
+  d.instance_count = static_cast<uint32_t>(L->instances.size());
+  d.materials = L->materials.data();
+  d.material_count = static_cast<uint32_t>(L->materials.size());
+  *out = d;
+  *storage = L.release();
+  return CG_OK;
+}
+
+extern "C" CG_API int cg_gltf_free(void* storage) {
+  delete static_cast<Loader*>(storage);
+  return CG_OK;
+}
+
 extern "C" CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out) {
   if (!path || !out) return fail(CG_E_INVALID, "null argument");
   *out = nullptr;
-  Loader L;
-  if (!L.load(path)) return fail(CG_E_INVALID, std::string(path) + ": " + L.err);
   cg_scene_desc d{};
-  d.vertices = L.vertices.data();
-  d.vertex_count = static_cast<uint32_t>(L.vertices.size());
-  d.indices = L.indices.data();
-  d.index_count = static_cast<uint32_t>(L.indices.size());
-  d.meshes = L.meshes.data();
-  d.mesh_count = static_cast<uint32_t>(L.meshes.size());
-  d.instances = L.instances.data();
-  d.instance_count = static_cast<uint32_t>(L.instances.size());
-  d.materials = L.materials.data();
-  d.material_count = static_cast<uint32_t>(L.materials.size());
-  return cg_scene_create(&d, out);
+  void* storage = nullptr;
+  int rc = cg_gltf_parse(path, &d, &storage);
+  if (rc != CG_OK) return rc;
+  rc = cg_scene_create(&d, out);
+  cg_gltf_free(storage);
+  return rc;
 }

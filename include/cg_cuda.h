@@ -172,6 +172,10 @@ CG_API int cg_scene_destroy(cg_scene_t scene);
  * instance per (node, mesh primitive), y-up rotated to z-up — and uploads it
  * as cg_scene_create does. */
 CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out);
+/* The parse step of cg_scene_load_gltf alone (no device needed): fills *out
+ * with arrays owned by *storage, released by cg_gltf_free. */
+CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage);
+CG_API int cg_gltf_free(void* storage);
 
 typedef struct cg_scene_info {
   uint32_t instance_count, mesh_count, triangle_count, material_count;

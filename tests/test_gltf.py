@@ -1,0 +1,96 @@
+"""LoadScene(path): the native glTF loader with the reference's conventions
+(default material first, glTF material i -> i + 1, y-up -> z-up root
+rotation), checked on the host against the in-memory descriptions it was
+written from, and the C++23 crystal::graphics layer's error path."""
+import json
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from crystalgraphics_b200 import backend as B
+from crystalgraphics_b200 import gltf, scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("make", [lambda: scenes.cornell(),
+                                  lambda: scenes.icosphere_scene(subdiv=3)])
+def test_gltf_round_trip_is_exact(tmp_path, make):
+    s = make()
+    path = gltf.write(s, str(tmp_path / "scene.gltf"))
+    p = B.parse_gltf(path)
+    # default material first, then the written ones
+    assert len(p.materials) == len(s.materials) + 1
+    assert p.materials[0]["metallic_factor"] == 1.0 and p.materials[0]["ior"] == np.float32(1.5)
+    for f in ("base_color_factor", "emissive_factor", "emissive_strength", "metallic_factor",
+              "roughness_factor", "ior", "dispersion", "transmission_factor", "thickness_factor"):
+        np.testing.assert_array_equal(p.materials[f][1:], s.materials[f], err_msg=f)
+    # instances: same order, same world matrix bits, material shifted by one
+    assert len(p.instances) == len(s.instances)
+    assert p.instances["world_from_local"].tobytes() == s.instances["world_from_local"].tobytes()
+    np.testing.assert_array_equal(p.instances["material"], s.instances["material"] + 1)
+    # geometry of every instance identical (shared geometry stays shared)
+    assert len(p.meshes) == len(s.meshes)
+    for k in range(len(s.instances)):
+        a, b = s.meshes[s.instances[k]["mesh"]], p.meshes[p.instances[k]["mesh"]]
+        va = s.vertices[a["vertex_offset"]:a["vertex_offset"] + a["vertex_count"]]
+        vb = p.vertices[b["vertex_offset"]:b["vertex_offset"] + b["vertex_count"]]
+        assert va["position"].tobytes() == vb["position"].tobytes()
+        assert va["normal"].tobytes() == vb["normal"].tobytes()
+        ia = s.indices[a["index_offset"]:a["index_offset"] + a["index_count"]] - a["vertex_offset"]
+        ib = p.indices[b["index_offset"]:b["index_offset"] + b["index_count"]] - b["vertex_offset"]
+        np.testing.assert_array_equal(ia, ib)
+
+
+def test_gltf_scene_packs_identically_in_the_oracle(tmp_path):
+    s = scenes.icosphere_scene(subdiv=3)
+    p = B.parse_gltf(gltf.write(s, str(tmp_path / "s.gltf")))
+    a, aa, _ = O.OracleScene(s).emissive()
+    b, ba, _ = O.OracleScene(p).emissive()
+    assert a.tobytes() == b.tobytes() and aa.tobytes() == ba.tobytes()
+
+
+def test_glb_container(tmp_path):
+    s = scenes.cornell()
+    path = gltf.write(s, str(tmp_path / "c.gltf"))
+    doc = json.load(open(path))
+    binary = open(path[:-5] + ".bin", "rb").read()
+    del doc["buffers"][0]["uri"]
+    js = json.dumps(doc).encode()
+    js += b" " * ((-len(js)) % 4)
+    binary += b"\0" * ((-len(binary)) % 4)
+    glb = struct.pack("<4sII", b"glTF", 2, 12 + 8 + len(js) + 8 + len(binary))
+    glb += struct.pack("<II", len(js), 0x4E4F534A) + js + struct.pack("<II", len(binary), 0x004E4942) + binary
+    gp = tmp_path / "c.glb"
+    gp.write_bytes(glb)
+    p = B.parse_gltf(str(gp))
+    assert p.instances["world_from_local"].tobytes() == s.instances["world_from_local"].tobytes()
+
+
+def test_gltf_errors(tmp_path):
+    with pytest.raises(B.Error, match="cannot open"):
+        B.parse_gltf(str(tmp_path / "missing.gltf"))
+    bad = tmp_path / "bad.gltf"
+    bad.write_text("{ this is not json")
+    with pytest.raises(B.Error, match="invalid JSON"):
+        B.parse_gltf(str(bad))
+    lines = tmp_path / "lines.gltf"
+    lines.write_text(json.dumps({"asset": {"version": "2.0"},
+                                 "meshes": [{"primitives": [{"attributes": {"POSITION": 0},
+                                                             "mode": 1}]}]}))
+    with pytest.raises(B.Error, match="triangle"):
+        B.parse_gltf(str(lines))
+
+
+def test_cxx_layer_reports_errors_through_expected(tmp_path):
+    exe = os.path.join(ROOT, "crystalgraphics_b200", "cg_view")
+    if not os.path.exists(exe):
+        pytest.skip("C++ layer not built")
+    r = subprocess.run([exe, str(tmp_path / "missing.gltf"), str(tmp_path / "o.ppm")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1
+    assert ("EnvInit" in r.stderr) or ("LoadScene" in r.stderr)

@@ -1,0 +1,199 @@
+"""The batched and served forms, the autotuner and the C++ layer on the GPU.
+
+Per-sample streams are keyed by (seed, frame, pixel, sample), so a view
+rendered alone, in a batch, or as a served request in a mix produces the same
+samples; results agree up to the order of float atomic additions.
+"""
+import os
+import subprocess
+import time
+
+import numpy as np
+import pytest
+
+from crystalgraphics_b200 import _abi, gltf, scenes
+from crystalgraphics_b200 import backend as B
+
+from gpu_common import small_instanced
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RTOL = 1e-4  # float atomic-add order
+
+
+@pytest.fixture(scope="module")
+def cornell():
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
+    s = scenes.cornell()
+    g = B.LoadScene(s)
+    yield s, g
+    g.close()
+    B.EnvTerm()
+
+
+def _views(s):
+    cam = s.camera
+    sizes = [(33, 17, 1), (64, 64, 4), (100, 40, 2), (16, 16, 8), (128, 96, 3)]
+    return [(cam.position[:], cam.direction[:], w, h, spp, 77 + k, (0.5 * w / h, 0.5))
+            for k, (w, h, spp) in enumerate(sizes)]
+
+
+def _close(a, b):
+    scale = max(float(np.abs(b).mean()), 1e-6)
+    return float(np.abs(a - b).max()) / scale
+
+
+def test_batch_matches_single_views(cornell):
+    s, g = cornell
+    views = _views(s)
+    films = B.batch_render(g, views)
+    for (pos, d, w, h, spp, seed, vp), film in zip(views, films):
+        B.EnvInit(B.PathTraceConf(render_width=w, render_height=h, sample_count=spp, trace_depth=3))
+        B.SetSeed(seed)
+        B.View(g, B.Camera(tuple(pos), tuple(d), vp))
+        single = B.ReadFilm()
+        assert film.shape == single.shape
+        assert _close(film, single) < RTOL, (w, h, spp)
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
+
+
+def test_batch_graph_replay_is_stable(cornell):
+    s, g = cornell
+    B.SetTuning(use_graph=1)
+    views = _views(s)
+    a = B.batch_render(g, views)
+    st1 = B.LastStats()
+    b = B.batch_render(g, views)   # replays the captured graph
+    st2 = B.LastStats()
+    assert st1.samples == st2.samples == sum(w * h * spp for _, _, w, h, spp, _, _ in views)
+    for x, y in zip(a, b):
+        assert _close(x, y) < RTOL
+    films8 = B.batch_render(g, views, rgba=True)[1]
+    assert films8[1].shape == (64, 64, 4) and films8[1][..., 3].min() == 255
+
+
+def test_batch_uneven_views_in_many_chunks(cornell):
+    """A queue small enough that a batch needs many chunks gives the same
+    films as one large chunk."""
+    s, g = cornell
+    views = _views(s)
+    ref = B.batch_render(g, views)
+    B.SetTuning(queue_capacity=8192)
+    small = B.batch_render(g, views)
+    assert B.LastStats().chunks > 3
+    B.SetTuning(queue_capacity=16 << 20)
+    for x, y in zip(ref, small):
+        assert _close(x, y) < RTOL
+
+
+def test_server_results_same_alone_and_in_the_mix(cornell):
+    s, g = cornell
+    s2 = small_instanced()
+    g2 = B.LoadScene(s2)
+    reqs = [(0, 48, 40, 4, 5), (1, 64, 48, 2, 6), (0, 32, 32, 8, 7), (1, 40, 40, 1, 8),
+            (0, 80, 60, 2, 9)]
+    cams = [s.camera, s2.camera]
+
+    def submit(sv, r):
+        si, w, h, spp, seed = r
+        c = cams[si]
+        return sv.submit(si, c.position[:], c.direction[:], w, h, spp, seed)
+
+    alone = []
+    with B.Server([g, g2], 1 << 30) as sv:
+        for r in reqs:
+            film, res = sv.wait(submit(sv, r))
+            assert res.status == 0
+            alone.append(film)
+    with B.Server([g, g2], 1 << 30) as sv:
+        ids = [submit(sv, r) for r in reqs]
+        mixed = [sv.wait(i)[0] for i in ids]
+        st = sv.stats()
+        assert st.completed == len(reqs) and st.samples == sum(w * h * spp for _, w, h, spp, _ in reqs)
+    for a, b in zip(alone, mixed):
+        assert _close(b, a) < RTOL
+    # and a served request equals the same view rendered by the batched form
+    si, w, h, spp, seed = reqs[0]
+    ref = B.batch_render(g, [(s.camera.position[:], s.camera.direction[:], w, h, spp, seed)])[0]
+    assert _close(mixed[0], ref) < RTOL
+
+
+def test_server_admission_under_budget(cornell):
+    s, g = cornell
+    c = s.camera
+    with B.Server([g], 1 << 30) as probe:
+        rid = probe.submit(0, c.position[:], c.direction[:], 64, 64, 2, 1)
+        probe.wait(rid)
+        one = probe.stats().peak_bytes
+    assert one > 0
+    budget = int(one * 1.5)  # room for one request at a time
+    with B.Server([g], budget) as sv:
+        ids = [sv.submit(0, c.position[:], c.direction[:], 64, 64, 2, k) for k in range(6)]
+        for i in ids:
+            sv.wait(i)
+        st = sv.stats()
+        assert st.completed == 6 and st.peak_bytes <= budget
+    with B.Server([g], one // 2) as tiny:  # can never fit
+        rid = tiny.submit(0, c.position[:], c.direction[:], 64, 64, 2, 1)
+        with pytest.raises(B.Error) as e:
+            tiny.wait(rid)
+        assert e.value.code == _abi.CG_E_OOM
+        assert tiny.stats().rejected == 1
+
+
+def test_server_cancel_and_timeout(cornell):
+    s, g = cornell
+    c = s.camera
+    with B.Server([g], 8 << 30) as sv:
+        big = [sv.submit(0, c.position[:], c.direction[:], 512, 512, 16, k) for k in range(4)]
+        last = sv.submit(0, c.position[:], c.direction[:], 512, 512, 16, 99)
+        sv.cancel(last)
+        with pytest.raises(B.Error) as e:
+            sv.wait(last)
+        assert e.value.code in (_abi.CG_E_CANCELLED,)
+        try:
+            sv.wait(big[-1], timeout_ms=0)
+            finished = True
+        except B.Error as err:
+            assert err.code == _abi.CG_E_TIMEOUT
+            finished = False
+        for i in big[:-1]:
+            sv.wait(i)
+        if not finished:
+            sv.wait(big[-1])
+        assert sv.stats().cancelled == 1
+
+
+def test_autotune_returns_a_valid_tuning(cornell):
+    s, g = cornell
+    t = B.autotune(g, (s.camera.position[:], s.camera.direction[:], 96, 96, 4, 1))
+    assert t.queue_capacity >= 4096 and t.extend_block % 32 == 0 and t.shade_block % 32 == 0
+    B.SetTuning(queue_capacity=16 << 20, extend_block=128, shade_block=128, use_graph=1)
+
+
+def test_gltf_scene_renders_like_the_in_memory_scene(tmp_path, cornell):
+    s, g = cornell
+    path = gltf.write(s, str(tmp_path / "c.gltf"))
+    conf = B.PathTraceConf(render_width=64, render_height=64, sample_count=4, trace_depth=3)
+    B.EnvInit(conf)
+    cam = B.Camera.from_c(s.camera)
+    B.View(g, cam)
+    a = B.ReadFilm()
+    gl = B.LoadScene(path)
+    B.View(gl, cam)
+    b = B.ReadFilm()
+    assert _close(b, a) < RTOL
+    # the C++23 layer (LoadScene(path) + View + ReadFilm) end to end
+    exe = os.path.join(ROOT, "crystalgraphics_b200", "cg_view")
+    out = tmp_path / "c.ppm"
+    args = [exe, path, str(out), "64", "64", "4", "3", "1"] + \
+        [str(x) for x in list(cam.position) + list(cam.direction) + list(cam.viewport)]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    data = out.read_bytes()
+    header_end = data.index(b"255\n") + 4
+    img = np.frombuffer(data[header_end:], np.uint8).reshape(64, 64, 3)
+    B.EnvInit(conf)
+    B.View(g, cam)
+    ref = B.ReadFilm(_abi.CG_FILM_RGBA8)[..., :3]
+    assert np.abs(img.astype(int) - ref.astype(int)).max() <= 1
