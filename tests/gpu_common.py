@@ -50,6 +50,44 @@ def ray_set(scene, n, seed=0):
     return rays
 
 
+def camera_rays(camera, W, H):
+    """cameraRay (compute.wesl:64-79) for every pixel, in float32."""
+    f = np.float32
+    d = np.array(camera.direction[:], f)
+    dx = np.cross(d, np.array([0, 0, 1], f)).astype(f)
+    dx = (dx / np.sqrt(np.sum(dx * dx, dtype=f))).astype(f) * f(camera.viewport[0])
+    dy = np.cross(d, dx).astype(f)
+    dy = (dy / np.sqrt(np.sum(dy * dy, dtype=f))).astype(f) * f(camera.viewport[1])
+    px, py = np.meshgrid(np.arange(W, dtype=f), np.arange(H, dtype=f))
+    cx = (px / f(W) * f(2) - f(1))[..., None]
+    cy = (py / f(H) * f(2) - f(1))[..., None]
+    r = (d + cx * dx + cy * dy).astype(f)
+    r = r / np.sqrt(np.sum(r * r, axis=-1, keepdims=True, dtype=f))
+    rays = np.zeros((H * W, 8), f)
+    rays[:, :3] = np.array(camera.position[:], f)
+    rays[:, 4:7] = r.reshape(-1, 3)
+    return rays
+
+
+def primary_tie_mask(oracle_scene, camera, W, H, ulps=4):
+    """Pixels whose camera ray meets two surfaces at the same distance (within
+    `ulps`): the closest hit there depends on traversal order (the reference
+    keeps the first one it finds), so such pixels are excluded from image
+    comparisons and counted, like ties in the hit-id comparison."""
+    hits, t2 = oracle_scene.trace_closest(camera_rays(camera, W, H))
+    t = hits["t"]
+    tie = (hits["instance"] >= 0) & (np.abs(t2 - t) <= ulps * np.spacing(t))
+    return tie.reshape(H, W)
+
+
 def pooled(img, k):
     h, w, c = img.shape
     return img[:h - h % k, :w - w % k].reshape(h // k, k, w // k, k, c).mean(axis=(1, 3))
+
+
+def pooled_masked(img, keep, k):
+    """k x k block means over the pixels where `keep` is set."""
+    h, w, c = img.shape
+    m = keep[:h - h % k, :w - w % k].reshape(h // k, k, w // k, k, 1).astype(np.float64)
+    x = img[:h - h % k, :w - w % k].reshape(h // k, k, w // k, k, c) * m
+    return x.sum(axis=(1, 3)) / np.maximum(m.sum(axis=(1, 3)), 1)

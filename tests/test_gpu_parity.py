@@ -16,7 +16,7 @@ import oracle as O
 from crystalgraphics_b200 import _abi, scenes
 from crystalgraphics_b200 import backend as B
 
-from gpu_common import pooled, ray_set, small_instanced
+from gpu_common import pooled_masked, primary_tie_mask, ray_set, small_instanced
 
 pytestmark = pytest.mark.gpu
 
@@ -89,10 +89,10 @@ def _gpu_frame(g, conf, camera, seed=0, frames=1):
 # Pixels may differ where a 1-ulp difference between CUDA's and glibc's
 # transcendentals flips a branch of a sample tree; that is rare.
 KEYED = [
-    ("cornell_d2", lambda: scenes.cornell(), 256, 256, 1, 2, 0.97),
-    ("cornell_d6", lambda: scenes.cornell(), 96, 96, 4, 6, 0.97),
-    ("icosphere_d8", lambda: scenes.icosphere_scene(subdiv=4), 96, 54, 4, 8, 0.97),
-    ("instanced_d5", lambda: small_instanced(), 96, 64, 2, 5, 0.97),
+    ("cornell_d2", lambda: scenes.cornell(), 256, 256, 1, 2, 0.995),
+    ("cornell_d6", lambda: scenes.cornell(), 96, 96, 4, 6, 0.995),
+    ("icosphere_d8", lambda: scenes.icosphere_scene(subdiv=4), 96, 54, 4, 8, 0.995),
+    ("instanced_d5", lambda: small_instanced(), 96, 64, 2, 5, 0.995),
 ]
 
 
@@ -106,7 +106,10 @@ def test_keyed_streams_match_oracle(case):
     o = O.OracleScene(s)
     ora, _, _ = o.render(conf.to_c(), s.camera, rng=O.RNG_KEYED, prune=True)
     assert np.all(np.isfinite(gpu))
-    lum_g, lum_o = gpu[..., 1], ora[..., 1]
+    tie = primary_tie_mask(o, s.camera, W, H)
+    assert tie.mean() < 0.01, tie.mean()
+    keep = ~tie
+    lum_g, lum_o = gpu[..., 1][keep], ora[..., 1][keep]
     scale = max(float(np.abs(lum_o).mean()), 1e-6)
     diff = (lum_g - lum_o) / scale
     close = float((np.abs(diff) <= 1e-3).mean())
@@ -114,23 +117,26 @@ def test_keyed_streams_match_oracle(case):
     far = diff[np.abs(diff) > 1e-3]
     # pixels that diverged must scatter on both sides (a bug would be biased)
     bias = abs(float(far.mean())) / max(float(np.abs(far).mean()), 1e-12) if len(far) else 0.0
-    print(f"{name}: {close:.4%} pixels within 1e-3, image means {lum_g.mean():.6f} vs "
-          f"{lum_o.mean():.6f}, diverged {len(far)} (bias {bias:.3f})")
+    print(f"{name}: {int(tie.sum())} tie pixels excluded; {close:.4%} of the rest within 1e-3, "
+          f"means {lum_g.mean():.6f} vs {lum_o.mean():.6f}, diverged {len(far)} (bias {bias:.3f})")
     assert close >= min_close, close
-    assert rel_mean < 0.02, rel_mean
+    assert rel_mean < 0.005, rel_mean
     if len(far) >= 50:
         assert bias < 0.5, bias
 
 
 def test_converged_image_matches_reference_order_oracle():
     """GPU (keyed streams) vs the oracle in the reference's own RNG order
-    (per-pixel PCG-hash streams consumed depth first), both converged."""
-    W = H = 48
+    (per-pixel PCG-hash streams consumed depth first), both converged:
+    relative RMSE of 8x8-block means <= 1 %, and at most one block-channel
+    outside 3 sigma.  Primary-ray tie pixels are left out of the blocks."""
+    W = H = 32
     s = scenes.cornell(W, H)
     g = B.LoadScene(s)
     o = O.OracleScene(s)
-    frames, spp, D = 8, 128, 2
+    frames, spp, D = 16, 256, 2
     conf = B.PathTraceConf(render_width=W, render_height=H, sample_count=spp, trace_depth=D)
+    keep = ~primary_tie_mask(o, s.camera, W, H)
     # oracle: independent frames of the reference estimator, seeds chained
     seeds = np.zeros((H, W), np.uint32)
     of = []
@@ -144,16 +150,17 @@ def test_converged_image_matches_reference_order_oracle():
     B.EnvInit(conf)
     gf = B.batch_render(g, views)
     of, gf = np.stack(of), np.stack(gf)
-    k = 4
-    po = np.stack([pooled(f, k) for f in of])
-    pg = np.stack([pooled(f, k) for f in gf])
+    k = 8
+    po = np.stack([pooled_masked(f, keep, k) for f in of])
+    pg = np.stack([pooled_masked(f, keep, k) for f in gf])
     mo, mg = po.mean(0), pg.mean(0)
     se = np.sqrt(po.var(0, ddof=1) / frames + pg.var(0, ddof=1) / frames) + 1e-12
     z = np.abs(mo - mg) / se
     rmse = np.sqrt(np.mean((mo - mg) ** 2)) / np.sqrt(np.mean(mo ** 2))
-    print(f"relative RMSE {rmse:.4%}, |z|>3 in {(z > 3).mean():.3%} of block-channels")
+    print(f"{int((~keep).sum())} tie pixels excluded; relative RMSE {rmse:.4%}, "
+          f"|z|>3 in {int((z > 3).sum())} of {z.size} block-channels")
     assert rmse <= 0.01, rmse
-    assert (z > 3).mean() <= 0.01
+    assert (z > 3).sum() <= 1
 
 
 def test_progressive_accumulation_resets_on_camera_change():

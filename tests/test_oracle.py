@@ -121,14 +121,31 @@ def test_oracle_closest_hit_on_axis_aligned_box():
 
 def test_oracle_render_reference_and_keyed_agree_statistically():
     """The keyed streams change which random numbers a sample uses, not the
-    estimator: both modes converge to the same image."""
-    s = scenes.cornell(64, 64)
-    os_ = O.OracleScene(s)
-    conf = _abi.make_conf(64, 64, 64, 2)
-    a, _, _ = os_.render(conf, s.camera, rng=O.RNG_REFERENCE, prune=True)
-    b, _, _ = os_.render(conf, s.camera, rng=O.RNG_KEYED, prune=True)
-    ma, mb = a.mean(axis=(0, 1)), b.mean(axis=(0, 1))
-    assert np.all(np.abs(ma - mb) / mb < 0.03), (ma, mb)
+    estimator: both RNG orders converge to the same image (8x8-block means of
+    independent frames within 3 sigma, primary-ray tie pixels left out)."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from gpu_common import pooled_masked, primary_tie_mask
+    W = H = 32
+    s = scenes.cornell(W, H)
+    o = O.OracleScene(s)
+    frames, spp = 12, 64
+    conf = _abi.make_conf(W, H, spp, 2)
+    keep = ~primary_tie_mask(o, s.camera, W, H)
+
+    def run(mode, seed):
+        seeds = np.zeros((H, W), np.uint32)
+        out = []
+        for k in range(frames):
+            f, seeds, _ = o.render(conf, s.camera, film=np.zeros((H, W, 3), np.float32), seeds=seeds,
+                                   iter_count=k, rng=mode, seed=seed, prune=True)
+            out.append(pooled_masked(f * (k + 1), keep, 8))
+        return np.stack(out)
+
+    a, b = run(O.RNG_REFERENCE, 0), run(O.RNG_KEYED, 99)
+    se = np.sqrt(a.var(0, ddof=1) / frames + b.var(0, ddof=1) / frames) + 1e-12
+    z = np.abs(a.mean(0) - b.mean(0)) / se
+    assert (z > 3.5).sum() <= 1, z.max()
 
 
 def test_oracle_progressive_running_mean():
