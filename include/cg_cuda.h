@@ -347,6 +347,27 @@ typedef struct cg_server_stats {
 } cg_server_stats;
 CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out);
 
+/* ---- rendering without allocation -------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they render (a host application that owns the memory budget
+ * and hands the renderer only its buffers, a pooled allocator that forbids
+ * driver allocations during a frame, a real-time loop that cannot afford an
+ * allocation's implicit synchronisation): renders one fresh frame of `view`
+ * (frame 0, keyed sample streams of view->seed) of `scene` with the caps of
+ * `conf` into the caller's device film — `film_xyzw` holds float4 (X, Y, Z, 0)
+ * per pixel, `film_rgba8` (may be NULL) uchar4 sRGB — on `stream` (NULL = the
+ * default stream) of the current device, and returns when it is done.
+ * It calls no cudaMalloc or cudaFree: the ray queues and tables live in a
+ * library-owned device array of about 18.6 MB (131072 queued rays) that every
+ * GPU loading the library holds until the process exits.  A view whose spp
+ * cannot fit that array in one chunk is rejected with CG_E_INVALID.  The first
+ * call on a device sets the array up (finds its device address, fills the
+ * wavelength table); make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other threads, other
+ * streams of the same device) race and must be serialised by the caller. */
+CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf, const cg_view_desc* view,
+                             void* film_xyzw, void* film_rgba8, void* stream);
+
 /* Library version string. */
 CG_API const char* cg_version(void);
 
