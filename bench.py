@@ -228,8 +228,8 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     samples_per_step = W_ * H_ * SPP_
 
-    if args.queue:
-        B.SetTuning(queue_capacity=args.queue)
+    if args.queue or args.bvh_width:
+        B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width)
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         B.View(g, cam)
@@ -346,6 +346,8 @@ def main():
                     help="small: the same scene at 320x180, 4 spp, with a 2M-ray queue "
                          "(the case ncu --set full captures)")
     ap.add_argument("--queue", type=int, default=0, help="ray queue capacity (0 = default)")
+    ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4],
+                    help="node width of the traversal (0 = library default, 4)")
     args = ap.parse_args()
     if args.case == "small":
         global W_, H_, SPP_, WORKLOAD

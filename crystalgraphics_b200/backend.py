@@ -299,8 +299,8 @@ def SetSeed(seed: int) -> None:
     _check(lib.cg_set_seed(seed))
 
 
-def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1) -> None:
-    t = _abi.CgTuning(queue_capacity, extend_block, shade_block, use_graph)
+def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_width=0) -> None:
+    t = _abi.CgTuning(queue_capacity, extend_block, shade_block, use_graph, bvh_width)
     _check(lib.cg_set_tuning(C.byref(t)))
 
 

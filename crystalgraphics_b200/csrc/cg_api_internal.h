@@ -79,7 +79,7 @@ struct Renderer {
   float* wl_tree = nullptr;
   float* wl_const = nullptr;
   bool counting = false;
-  cg_tuning tuning{16u << 20, 128u, 128u, 1u};
+  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, {0u, 0u, 0u}};
   DeviceArena wave_arena;
   WaveBuffers wave{};
 

@@ -209,16 +209,19 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* be
   SceneDev* s = reinterpret_cast<SceneDev*>(scene);
   CG_CUDA(cudaSetDevice(env.device));
   const cg_tuning saved = env.tuning;
-  const uint32_t caps_q[] = {4u << 20, 8u << 20, 16u << 20};
-  const uint32_t blocks[] = {64u, 128u, 256u};
+  const uint32_t caps_q[] = {8u << 20, 16u << 20};
+  const uint32_t blocks[] = {128u, 256u};
+  const uint32_t widths[] = {4u, 2u};
   cg_tuning winner = saved;
   float best_ms = 1e30f;
   for (uint32_t q : caps_q) {
     for (uint32_t eb : blocks) {
       for (uint32_t sb : blocks) {
+       for (uint32_t w : widths) {
         env.tuning.queue_capacity = q;
         env.tuning.extend_block = eb;
         env.tuning.shade_block = sb;
+        env.tuning.bvh_width = w;
         env.tuning.use_graph = 0;
         env.dropAllGraphs();
         float t = 0.0f;
@@ -234,6 +237,7 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* be
           best_ms = t;
           winner = env.tuning;
         }
+       }
       }
     }
   }

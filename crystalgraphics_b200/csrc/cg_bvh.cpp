@@ -195,6 +195,73 @@ void padBox(Box& b) {
   }
 }
 
+namespace {
+
+struct Child4 {
+  Box box;
+  int32_t link;
+};
+
+void childrenOf(const BvhNode& n, std::vector<Child4>& out) {
+  const Child4 c0{{{n.c0lx, n.c0ly, n.c0lz}, {n.c0hx, n.c0hy, n.c0hz}}, n.child0};
+  const Child4 c1{{{n.c1lx, n.c1ly, n.c1lz}, {n.c1hx, n.c1hy, n.c1hz}}, n.child1};
+  // an absent child is a leaf of zero primitives
+  if (c0.link >= 0 || leafCount(c0.link) != 0) out.push_back(c0);
+  if (c1.link >= 0 || leafCount(c1.link) != 0) out.push_back(c1);
+}
+
+uint32_t collapse(const std::vector<BvhNode>& b2, uint32_t n2, std::vector<Bvh4Node>& out) {
+  const uint32_t idx = static_cast<uint32_t>(out.size());
+  out.emplace_back();
+  std::vector<Child4> kids;
+  childrenOf(b2[n2], kids);
+  while (kids.size() < 4) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (size_t k = 0; k < kids.size(); ++k) {
+      if (kids[k].link < 0) continue;
+      const float a = boxArea(kids[k].box);
+      if (a > best_area) {
+        best_area = a;
+        best = static_cast<int>(k);
+      }
+    }
+    if (best < 0) break;
+    std::vector<Child4> sub;
+    childrenOf(b2[kids[best].link], sub);
+    if (kids.size() - 1 + sub.size() > 4) break;
+    kids.erase(kids.begin() + best);
+    kids.insert(kids.end(), sub.begin(), sub.end());
+  }
+  int32_t links[4];
+  for (size_t k = 0; k < 4; ++k) {
+    if (k < kids.size())
+      links[k] = kids[k].link >= 0 ? static_cast<int32_t>(collapse(b2, kids[k].link, out))
+                                   : kids[k].link;
+    else
+      links[k] = kEmptyLink;
+  }
+  Bvh4Node& n = out[idx];
+  for (int k = 0; k < 4; ++k) {
+    const bool has = static_cast<size_t>(k) < kids.size();
+    n.lox[k] = has ? kids[k].box.lo[0] : 1e30f;
+    n.loy[k] = has ? kids[k].box.lo[1] : 1e30f;
+    n.loz[k] = has ? kids[k].box.lo[2] : 1e30f;
+    n.hix[k] = has ? kids[k].box.hi[0] : 1e30f;
+    n.hiy[k] = has ? kids[k].box.hi[1] : 1e30f;
+    n.hiz[k] = has ? kids[k].box.hi[2] : 1e30f;
+    n.child[k] = links[k];
+    n._pad[k] = 0;
+  }
+  return idx;
+}
+
+}  // namespace
+
+uint32_t collapseBvh4(const std::vector<BvhNode>& bvh2, uint32_t root2, std::vector<Bvh4Node>& out) {
+  return collapse(bvh2, root2, out);
+}
+
 uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt, uint32_t prim_base,
                   std::vector<BvhNode>& nodes, std::vector<uint32_t>& order,
                   uint32_t* depth_out) {
@@ -243,7 +310,7 @@ uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt, uin
     Box bx = b.tmp[0].box;
     padBox(bx);
     setChild(n, 0, bx, leafLink(b.tmp[0]), b.tmp[0].count);
-    setChild(n, 1, empty, leafLink(b.tmp[0]), 0);
+    setChild(n, 1, empty, kEmptyLink, 0);
     nodes.push_back(n);
     return base;
   }

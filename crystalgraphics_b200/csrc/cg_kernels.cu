@@ -120,8 +120,17 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
 }
 
 // ---- extend: closest hit --------------------------------------------------------
-template <bool kCount>
-__global__ void k_extend(SceneView sc, WaveBuffers wb, int parity) {
+// Any hit / closest hit over the four-wide (kWide) or binary trees.
+template <bool kAny, bool kCount, bool kWide>
+__device__ __forceinline__ HitRec trace(const SceneView& sc, float4 o, float4 d, float tmax,
+                                        TravCounters& cnt, uint32_t* status) {
+  if (kWide) return traceRay4<kAny, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, status);
+  return traceRay<kAny, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, status);
+}
+
+// At most 64 registers per thread (4 blocks of 256 or 8 of 128 per SM).
+template <bool kCount, bool kWide>
+__global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb, int parity) {
   // counts can exceed the capacity after an overflow (the appends are then
   // dropped and the status word set); never read past the queue
   const uint32_t n = min(wb.counts[parity], wb.capacity);
@@ -136,7 +145,7 @@ __global__ void k_extend(SceneView sc, WaveBuffers wb, int parity) {
   for (uint32_t i = tid; i < n; i += stride) {
     const float4 o = wb.ray_o[parity][i];
     const float4 d = wb.ray_d[parity][i];
-    HitRec h = traceRay<false, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, MAXD, cnt, wb.status);
+    HitRec h = trace<false, kCount, kWide>(sc, o, d, MAXD, cnt, wb.status);
     wb.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
     wb.hit_inst[i] = h.inst;
   }
@@ -156,8 +165,8 @@ __global__ void k_extend(SceneView sc, WaveBuffers wb, int parity) {
 }
 
 // ---- shadow: t-bounded any hit (solveEmission, trace.wesl:91-113) ----------------
-template <bool kCount>
-__global__ void k_shadow(SceneView sc, WaveBuffers wb) {
+template <bool kCount, bool kWide>
+__global__ void __launch_bounds__(256, 4) k_shadow(SceneView sc, WaveBuffers wb) {
   const uint32_t n = min(wb.counts[2], wb.capacity);
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid == 0) atomicAdd(&wb.stats[1], static_cast<unsigned long long>(n));
@@ -168,7 +177,7 @@ __global__ void k_shadow(SceneView sc, WaveBuffers wb) {
     const float4 d = wb.sh_d[i];
     // occluded iff the closest hit (< 1e6) is nearer than expected - 1e-3
     const float tmax = fminf(d.w, MAXD);
-    HitRec h = traceRay<true, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, wb.status);
+    HitRec h = trace<true, kCount, kWide>(sc, o, d, tmax, cnt, wb.status);
     if (h.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[i]], o.w);
   }
   if (kCount) {
@@ -539,13 +548,14 @@ __global__ void k_resolve(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
 }
 
 // ---- closest-hit query for parity tests -------------------------------------------
+template <bool kWide>
 __global__ void k_trace_closest(SceneView sc, const float4* rays, uint32_t n, float4* out_tuv,
                                 int4* out_ids, uint32_t* status) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 o = rays[2 * i], d = rays[2 * i + 1];
   TravCounters cnt{0u, 0u, 0u};
-  HitRec h = traceRay<false, false>(sc, o.x, o.y, o.z, d.x, d.y, d.z, MAXD, cnt, status);
+  HitRec h = trace<false, false, kWide>(sc, o, d, MAXD, cnt, status);
   if (h.inst >= 0) {
     const uint32_t orig = __float_as_uint(__ldg(sc.tris + 3u * h.tri).w);
     out_tuv[i] = make_float4(h.t, h.u, h.v, 0.0f);
@@ -587,10 +597,14 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
-  if (counting)
-    k_extend<true><<<grid, block, 0, s>>>(sc, wb, parity);
+  if (counting && ls.wide)
+    k_extend<true, true><<<grid, block, 0, s>>>(sc, wb, parity);
+  else if (counting)
+    k_extend<true, false><<<grid, block, 0, s>>>(sc, wb, parity);
+  else if (ls.wide)
+    k_extend<false, true><<<grid, block, 0, s>>>(sc, wb, parity);
   else
-    k_extend<false><<<grid, block, 0, s>>>(sc, wb, parity);
+    k_extend<false, false><<<grid, block, 0, s>>>(sc, wb, parity);
 }
 
 void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
@@ -604,10 +618,14 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
-  if (counting)
-    k_shadow<true><<<grid, block, 0, s>>>(sc, wb);
+  if (counting && ls.wide)
+    k_shadow<true, true><<<grid, block, 0, s>>>(sc, wb);
+  else if (counting)
+    k_shadow<true, false><<<grid, block, 0, s>>>(sc, wb);
+  else if (ls.wide)
+    k_shadow<false, true><<<grid, block, 0, s>>>(sc, wb);
   else
-    k_shadow<false><<<grid, block, 0, s>>>(sc, wb);
+    k_shadow<false, false><<<grid, block, 0, s>>>(sc, wb);
 }
 
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
@@ -617,9 +635,12 @@ void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc&
 }
 
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
-                        int4* out_ids, uint32_t* status, cudaStream_t s) {
+                        int4* out_ids, uint32_t* status, bool wide, cudaStream_t s) {
   if (n == 0) return;
-  k_trace_closest<<<(n + 127) / 128, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
+  if (wide)
+    k_trace_closest<true><<<(n + 127) / 128, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
+  else
+    k_trace_closest<false><<<(n + 127) / 128, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
 }
 
 }  // namespace cg

@@ -78,6 +78,7 @@ struct LaunchShape {
   uint32_t shade_block = 128;
   uint32_t grid_extend = 0;  // 0: derived from the SM count
   uint32_t grid_shade = 0;
+  bool wide = true;          // traverse the four-wide trees
 };
 
 void launchWavelengthTree(float* tree, float* consts, cudaStream_t s);
@@ -91,7 +92,7 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
                    cudaStream_t s);
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
-                        int4* out_ids, uint32_t* status, cudaStream_t s);
+                        int4* out_ids, uint32_t* status, bool wide, cudaStream_t s);
 
 int smCount();
 

@@ -164,7 +164,8 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
 
   // ---- one BLAS per mesh ------------------------------------------------------
   s.mesh_count = d->mesh_count;
-  std::vector<uint32_t> mesh_root(d->mesh_count), mesh_tri_base(d->mesh_count);
+  std::vector<uint32_t> mesh_root(d->mesh_count), mesh_root4(d->mesh_count),
+      mesh_tri_base(d->mesh_count);
   std::vector<Box> mesh_bounds(d->mesh_count);
   BvhBuildOptions blas_opt;
   blas_opt.max_leaf = 4;
@@ -201,6 +202,7 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
     order.clear();
     uint32_t depth = 0;
     mesh_root[m] = buildBvh(boxes, blas_opt, tri_base, s.blas, order, &depth);
+    mesh_root4[m] = collapseBvh4(s.blas, mesh_root[m], s.blas4);
     s.blas_depth = std::max(s.blas_depth, depth);
     for (uint32_t k = 0; k < nt; ++k) {
       const uint32_t t = order[k];
@@ -250,7 +252,7 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
     di.blas_root = mesh_root[ci.mesh];
     di.material = ci.material;
     di.tri_base = mesh_tri_base[ci.mesh];
-    di.mesh = ci.mesh;
+    di.blas4_root = mesh_root4[ci.mesh];
     s.inst.push_back(di);
     // world box of the mesh box's 8 corners (double, then widened)
     const Box& mb = mesh_bounds[ci.mesh];
@@ -290,6 +292,7 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
       if (n.child0 < 0 && n.cnt0) n.child0 = leafLinkOf(tlas_order[leafFirst(n.child0)], 1);
       if (n.child1 < 0 && n.cnt1) n.child1 = leafLinkOf(tlas_order[leafFirst(n.child1)], 1);
     }
+    collapseBvh4(s.tlas, 0, s.tlas4);  // root 0
   }
 
   // ---- emissive buffer (emissive_buffer.h:44-100) --------------------------------------

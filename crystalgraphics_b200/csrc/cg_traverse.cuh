@@ -192,6 +192,134 @@ __device__ __forceinline__ HitRec traceRay(const SceneView& sc, float wox, float
   return best;
 }
 
+__device__ __forceinline__ void cswap(float& ka, int32_t& la, float& kb, int32_t& lb) {
+  if (kb < ka) {
+    const float tk = ka;
+    ka = kb;
+    kb = tk;
+    const int32_t tl = la;
+    la = lb;
+    lb = tl;
+  }
+}
+
+// The same closest / any hit over Bvh4Node trees: one node visit tests four
+// boxes (six independent 128-bit slab loads), the hit children are ordered
+// by entry distance, the nearest is visited next and the others pushed.
+// Triangle and instance handling is that of traceRay (bit-identical hits).
+template <bool kAny, bool kCount>
+__device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, float woy, float woz,
+                                            float wdx, float wdy, float wdz, float tmax,
+                                            TravCounters& cnt, uint32_t* status) {
+  HitRec best{tmax, 0.0f, 0.0f, -1, 0u};
+  if (!sc.has_tlas) return best;
+  int32_t stack[kStackSize];
+  int sp = 0;
+  const Bvh4Node* nodes = sc.tlas4;
+  bool in_blas = false;
+  int32_t cur_inst = -1;
+  float ox = wox, oy = woy, oz = woz, dx = wdx, dy = wdy, dz = wdz;
+  float idx = safeInv(dx), idy = safeInv(dy), idz = safeInv(dz);
+  float oix = ox * idx, oiy = oy * idy, oiz = oz * idz;
+  int32_t node = 0;
+  while (true) {
+    while (node >= 0) {
+      const float4* np = reinterpret_cast<const float4*>(nodes + node);
+      const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+      if (kCount) ++cnt.nodes;
+      float k[4];
+      const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, hxs[4] = {hx.x, hx.y, hx.z, hx.w};
+      const float lys[4] = {ly.x, ly.y, ly.z, ly.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w};
+      const float lzs[4] = {lz.x, lz.y, lz.z, lz.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float a0 = fmaf(lxs[c], idx, -oix), a1 = fmaf(hxs[c], idx, -oix);
+        const float b0 = fmaf(lys[c], idy, -oiy), b1 = fmaf(hys[c], idy, -oiy);
+        const float c0 = fmaf(lzs[c], idz, -oiz), c1 = fmaf(hzs[c], idz, -oiz);
+        const float tmin = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
+        const float tmx = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), best.t));
+        k[c] = tmin <= tmx ? tmin : INFINITY;
+      }
+      int32_t l0 = ch.x, l1 = ch.y, l2 = ch.z, l3 = ch.w;
+      float k0 = k[0], k1 = k[1], k2 = k[2], k3 = k[3];
+      // sort the four (distance, link) pairs, misses (+inf) last
+      cswap(k0, l0, k1, l1);
+      cswap(k2, l2, k3, l3);
+      cswap(k0, l0, k2, l2);
+      cswap(k1, l1, k3, l3);
+      cswap(k1, l1, k2, l2);
+      if (k0 == INFINITY) {
+        node = sp > 0 ? stack[--sp] : kDone;
+        continue;
+      }
+      const int pushes = (k1 != INFINITY) + (k2 != INFINITY) + (k3 != INFINITY);
+      if (sp + pushes > kStackSize) {
+        atomicOr(status, 1u);
+        return HitRec{tmax, 0.0f, 0.0f, -1, 0u};
+      }
+      if (k3 != INFINITY) stack[sp++] = l3;
+      if (k2 != INFINITY) stack[sp++] = l2;
+      if (k1 != INFINITY) stack[sp++] = l1;
+      node = l0;
+    }
+    if (node == kDone) break;
+    if (node == kToTlas) {
+      nodes = sc.tlas4;
+      in_blas = false;
+      ox = wox; oy = woy; oz = woz;
+      dx = wdx; dy = wdy; dz = wdz;
+      idx = safeInv(dx); idy = safeInv(dy); idz = safeInv(dz);
+      oix = ox * idx; oiy = oy * idy; oiz = oz * idz;
+      node = sp > 0 ? stack[--sp] : kDone;
+      continue;
+    }
+    const uint32_t first = static_cast<uint32_t>(~node) >> 3;
+    const uint32_t count = static_cast<uint32_t>(~node) & 7u;
+    if (!in_blas) {
+      if (count == 0u) {
+        node = sp > 0 ? stack[--sp] : kDone;
+        continue;
+      }
+      const float4* ipf = reinterpret_cast<const float4*>(sc.inst + first);
+      const float4 r0 = __ldg(ipf), r1 = __ldg(ipf + 1), r2 = __ldg(ipf + 2);
+      const uint4 meta = __ldg(reinterpret_cast<const uint4*>(ipf + 3));
+      const float m[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+      if (kCount) ++cnt.insts;
+      toLocal(m, wox, woy, woz, wdx, wdy, wdz, ox, oy, oz, dx, dy, dz);
+      idx = safeInv(dx); idy = safeInv(dy); idz = safeInv(dz);
+      oix = ox * idx; oiy = oy * idy; oiz = oz * idz;
+      if (sp >= kStackSize) {
+        atomicOr(status, 1u);
+        return HitRec{tmax, 0.0f, 0.0f, -1, 0u};
+      }
+      stack[sp++] = kToTlas;
+      nodes = sc.blas4;
+      in_blas = true;
+      cur_inst = static_cast<int32_t>(first);
+      node = static_cast<int32_t>(meta.w);  // blas4_root
+      continue;
+    }
+    for (uint32_t kk = 0; kk < count; ++kk) {
+      const float4* tp = sc.tris + 3u * (first + kk);
+      const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
+      if (kCount) ++cnt.tris;
+      float t, u, v;
+      if (intersectTri(ox, oy, oz, dx, dy, dz, ta, tb, tc, t, u, v) && t < best.t) {
+        best.t = t;
+        best.u = u;
+        best.v = v;
+        best.inst = cur_inst;
+        best.tri = first + kk;
+        if (kAny) return best;
+      }
+    }
+    node = sp > 0 ? stack[--sp] : kDone;
+  }
+  return best;
+}
+
 }  // namespace dev
 }  // namespace cg
 

@@ -35,12 +35,24 @@ struct alignas(16) BvhNode {
 };
 static_assert(sizeof(BvhNode) == 64, "BvhNode is 64 bytes");
 
+// Four-wide node: the slabs of four children, structure-of-arrays so each
+// axis bound is one 128-bit load; links as in BvhNode (leaf count in the low
+// 3 bits of ~link).  An absent child has link kEmptyLink and a point box at
+// 1e30.  Collapsed from the SAH BVH2, it halves the dependent node fetches of
+// a ray.
+struct alignas(16) Bvh4Node {
+  float lox[4], hix[4], loy[4], hiy[4], loz[4], hiz[4];
+  int32_t child[4];
+  uint32_t _pad[4];
+};
+static_assert(sizeof(Bvh4Node) == 128, "Bvh4Node is 128 bytes");
+
 struct alignas(16) DevInstance {
   float inv[12];        // row-major world -> local (3x4)
-  uint32_t blas_root;   // node index of the mesh BLAS root
+  uint32_t blas_root;   // node index of the mesh BLAS root (BVH2)
   uint32_t material;
   uint32_t tri_base;    // first triangle of the mesh in the global arrays
-  uint32_t mesh;
+  uint32_t blas4_root;  // node index of the mesh BLAS root (BVH4)
 };
 static_assert(sizeof(DevInstance) == 64, "DevInstance is 64 bytes");
 
@@ -94,6 +106,8 @@ struct DevAlias {
 struct SceneView {
   const BvhNode* tlas;         // TLAS nodes (root 0); leaves hold instances
   const BvhNode* blas;         // all BLAS nodes
+  const Bvh4Node* tlas4;       // the same trees, four-wide (root 0)
+  const Bvh4Node* blas4;
   const float4* tris;          // 3 float4 per triangle: (v0, orig id bits) (e1) (e2)
   const uint4* tri_vidx;       // vertex indices per triangle (i0, i1, i2, _)
   const float4* vnormal;       // vertex normals

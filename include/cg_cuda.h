@@ -305,6 +305,8 @@ typedef struct cg_tuning {
   uint32_t extend_block;
   uint32_t shade_block;
   uint32_t use_graph;   /* 1 = capture the chunk pipeline as a CUDA graph */
+  uint32_t bvh_width;   /* 4 (default) or 2: node width the traversal walks */
+  uint32_t _pad[3];
 } cg_tuning;
 CG_API int cg_set_tuning(const cg_tuning* tuning);
 CG_API int cg_get_tuning(cg_tuning* out);

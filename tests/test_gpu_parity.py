@@ -35,13 +35,16 @@ SCENES = {
 }
 
 
+@pytest.mark.parametrize("width", [4, 2])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_closest_hits_bit_exact(name):
+def test_closest_hits_bit_exact(name, width):
     s = SCENES[name]()
     g = B.LoadScene(s)
     o = O.OracleScene(s)
     rays = ray_set(s, 20000, seed=11)
+    B.SetTuning(bvh_width=width)
     gh = B.trace_closest(g, rays)
+    B.SetTuning(bvh_width=4)
     oh, t2 = o.trace_closest(rays)
     # exclude ulp-level ties: the second-best hit within 1 ulp of the best
     tie = (oh["instance"] >= 0) & (np.abs(t2 - oh["t"]) <= np.spacing(oh["t"]))
