@@ -44,10 +44,16 @@ WORKLOAD = ("displaced dispersive icosphere: 1,310,720 tris, rough dispersive di
             "ground + 64 emissive tris, 1280x720, 16 spp, depth 8 (plain View())")
 W_, H_, SPP_, DEPTH_ = 1280, 720, 16, 8
 # bytes the traversal reads per unit of work (the device layout): a node
-# visit reads one 64 B BvhNode (both child boxes), a triangle test one 48 B
-# triangle record, an instance entry one 64 B DevInstance; per ray the
-# kernel reads 32 B of ray and writes 20 B of hit
-NODE_B, TRI_B, INST_B, RAY_B = 64, 48, 64, 52
+# visit reads one 128 B Bvh4Node (four child boxes and links; 64 B BvhNode with
+# two child boxes on the binary trees), a triangle test one 48 B triangle
+# record, an instance entry one 64 B DevInstance; per ray the kernel reads
+# 32 B of ray and writes 20 B of hit
+NODE_B = {4: 128, 2: 64}
+TRI_B, INST_B, RAY_B = 48, 64, 52
+# DRAM bytes (read + write) per k_extend launch of this workload, mean of the
+# seven launches of one chunk in profiles/dram_traffic_icosphere_1280x720_16spp_d8.md
+# (ncu, cold caches: an upper bound)
+EXTEND_TRAFFIC_B = 183e6
 
 
 def dist_env():
@@ -58,30 +64,47 @@ def dist_env():
 
 
 class Dist:
-    def __init__(self, ws, rank, local):
+    """One process per GPU: barriers around the timed region and the max over
+    ranks of each rank's device time.  No collective touches the render data
+    (every rank renders its own frames).  backend "gloo" runs the same logic
+    on CPU ranks."""
+
+    def __init__(self, ws, rank, local, backend="nccl"):
         self.ws, self.rank, self.local = ws, rank, local
         self.pg = None
+        self.device = "cuda" if backend == "nccl" else "cpu"
         if ws > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", local))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                kw["device_id"] = torch.device("cuda", local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600), **kw)
             self.pg = dist
 
     def barrier(self):
         if self.pg:
             self.pg.barrier()
 
-    def max(self, x: float) -> float:
-        if not self.pg:
-            return x
+    def _reduce(self, x: float, op) -> float:
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=op)
         return float(t.item())
+
+    def max(self, x: float) -> float:
+        return self._reduce(x, self.pg.ReduceOp.MAX) if self.pg else x
+
+    def sum(self, x: float) -> float:
+        return self._reduce(x, self.pg.ReduceOp.SUM) if self.pg else x
+
+    def job_rate(self, units: float, seconds: float) -> float:
+        """Whole-job throughput: the units all ranks processed over the
+        slowest rank's time."""
+        return self.sum(units) / self.max(seconds)
 
     def close(self):
         if self.pg:
@@ -210,6 +233,165 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ---- batched and served forms against the plain one-view-per-View() path ----------------------
+BATCH_DEPTH = 12     # the instanced scene's trace depth
+SERVE_DEPTH = 12     # one conf serves all four resident scenes
+SERVE_RATES = (50, 200, 2000)
+SERVE_REQUESTS = 48
+
+
+def _rel_diff(a, b):
+    return float(np.abs(a - b).max()) / max(float(np.abs(b).mean()), 1e-6)
+
+
+def _tuning_kwargs(t):
+    return dict(queue_capacity=int(t.queue_capacity), extend_block=int(t.extend_block),
+                shade_block=int(t.shade_block), use_graph=int(t.use_graph),
+                bvh_width=int(t.bvh_width), persistent=bool(t.persistent),
+                shade_sort=int(t.shade_sort) != 2)
+
+
+def _plain_render(B, g, pos, d, w, h, spp, seed, depth, tuning=None):
+    """One view the plain way: EnvInit for its film size, View, ReadFilm.
+    Returns (film, host wall seconds, device ms of the View launches)."""
+    t0 = time.perf_counter()
+    B.EnvInit(B.PathTraceConf(render_width=w, render_height=h, sample_count=spp,
+                              trace_depth=depth))
+    if tuning:
+        B.SetTuning(**tuning)
+    B.SetSeed(seed)
+    B.View(g, B.Camera(tuple(pos), tuple(d), (0.5 * w / h, 0.5)))
+    film = B.ReadFilm()
+    return film, time.perf_counter() - t0, B.LastStats().device_ms
+
+
+def batched_form(B, torch):
+    """256 views of the instanced scene (sides log-uniform 64-1024, spp in
+    {1,4,16,64}, poses on an r=150 sphere) in one wavefront replayed from a
+    captured CUDA graph, against 256 plain View() calls of the same views
+    with the same keyed sample streams (so the same image RMSE)."""
+    from crystalgraphics_b200 import scenes
+    s = scenes.instanced_scene()
+    views = scenes.batch_views(256)
+    B.EnvInit(B.PathTraceConf(render_width=1920, render_height=1080, sample_count=64,
+                              trace_depth=BATCH_DEPTH))
+    g = B.LoadScene(s)
+    p0, d0 = views[0][0], views[0][1]
+    t_tune = time.perf_counter()
+    best = B.autotune(g, (p0, d0, 512, 512, 4, 0))
+    t_tune = time.perf_counter() - t_tune
+    tuning = _tuning_kwargs(best)
+    samples = sum(w * h * spp for _, _, w, h, spp, _ in views)
+    small = [v for v in views if v[2] * v[3] * v[4] <= 1 << 18]
+    small_samples = sum(w * h * spp for _, _, w, h, spp, _ in small)
+
+    def batch(vs):
+        arr = B.make_views(vs)
+        B.batch_render(g, arr)                     # captures the graph
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        films = B.batch_render(g, arr)             # replays it
+        wall = time.perf_counter() - t0
+        return films, wall, B.LastStats().device_ms
+
+    films, b_wall, b_dev = batch(views)
+    _, bs_wall, bs_dev = batch(small)
+    small_ids = {id(v) for v in small}
+    p_wall = p_dev = ps_wall = ps_dev = 0.0
+    worst = 0.0
+    for v, bf in zip(views, films):
+        film, wall, dev = _plain_render(B, g, *v, BATCH_DEPTH, tuning)
+        p_wall += wall
+        p_dev += dev
+        if id(v) in small_ids:
+            ps_wall += wall
+            ps_dev += dev
+        worst = max(worst, _rel_diff(bf, film))
+    g.close()
+    B.EnvTerm()
+    msps = lambda n, sec: n / sec / 1e6
+    return {
+        "workload": "instanced scene (4096 instances of 8 meshes, 10k emissive tris), 256 views, "
+                    "side log-uniform 64-1024, spp in {1,4,16,64}, depth 12",
+        "views": len(views), "samples": samples,
+        "batched_msamples_per_s": msps(samples, b_dev / 1e3),
+        "batched_wall_msamples_per_s": msps(samples, b_wall),
+        "plain_msamples_per_s": msps(samples, p_dev / 1e3),
+        "plain_wall_msamples_per_s": msps(samples, p_wall),
+        "speedup_device": p_dev / b_dev, "speedup_wall": p_wall / b_wall,
+        "small_views": {"views": len(small), "samples": small_samples,
+                        "rule": "w*h*spp <= 262144",
+                        "batched_msamples_per_s": msps(small_samples, bs_dev / 1e3),
+                        "plain_msamples_per_s": msps(small_samples, ps_dev / 1e3),
+                        "speedup_device": ps_dev / bs_dev, "speedup_wall": ps_wall / bs_wall},
+        "max_rel_diff_vs_plain": worst,
+        "tuning": tuning, "autotune_s": t_tune,
+        "timing": "device: CUDA events around the launches (graph replay / View chunks); "
+                  "wall: host clock incl. film readback (and EnvInit per plain view)",
+    }
+
+
+def served_form(B, torch):
+    """Poisson request streams over four resident scenes (the icosphere and
+    three instanced scenes with 4096, 2048 and 8192 instances) through the
+    continuous-batching server; the plain baseline serves the same requests one
+    at a time through EnvInit/View/ReadFilm in arrival order."""
+    from crystalgraphics_b200 import scenes
+    resident = [scenes.icosphere_scene(), scenes.instanced_scene(),
+                scenes.instanced_scene(instances=2048, seed=5),
+                scenes.instanced_scene(instances=8192, seed=6)]
+    B.EnvInit(B.PathTraceConf(render_width=1920, render_height=1080, sample_count=16,
+                              trace_depth=SERVE_DEPTH))
+    gs = [B.LoadScene(x) for x in resident]
+    base = scenes.request_stream(SERVE_REQUESTS, 1.0)   # arrivals at 1 req/s, scaled per rate
+    req_samples = [w * h * spp for _, _, _, _, w, h, spp, _ in base]
+    total = sum(req_samples)
+    out = {"workload": "4 resident scenes, requests of {256^2, 512^2, 1280x720, 1920x1080} x "
+                       "spp {1,4,16}, random poses, Poisson arrivals, depth 12",
+           "requests_per_rate": SERVE_REQUESTS, "samples_per_rate": total, "rates": []}
+    # warm the server path once
+    with B.Server(gs, 32 << 30) as sv:
+        _, si, p, d, w, h, spp, seed = base[0]
+        sv.wait(sv.submit(si, p, d, w, h, spp, seed))
+    for rate in SERVE_RATES:
+        with B.Server(gs, 32 << 30) as sv:
+            ids = []
+            t_start = time.perf_counter()
+            for (t_arr, si, p, d, w, h, spp, seed) in base:
+                delay = t_start + t_arr / rate - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                ids.append(sv.submit(si, p, d, w, h, spp, seed))
+            res = [sv.wait(i)[1] for i in ids]
+            peak = sv.stats().peak_bytes
+        lat = np.array([r.finish_s - r.submit_s for r in res]) * 1e3
+        span = max(r.finish_s for r in res) - min(r.submit_s for r in res)
+        out["rates"].append({"rate_hz": rate, "msamples_per_s": total / span / 1e6,
+                             "p50_ms": float(np.percentile(lat, 50)),
+                             "p99_ms": float(np.percentile(lat, 99)),
+                             "peak_admitted_bytes": int(peak)})
+    # plain: per-request service time measured, FIFO over the same arrivals
+    service = []
+    for (_, si, p, d, w, h, spp, seed) in base:
+        _, wall, _ = _plain_render(B, gs[si], p, d, w, h, spp, seed, SERVE_DEPTH)
+        service.append(wall)
+    for entry, rate in zip(out["rates"], SERVE_RATES):
+        free_at, lat, first = 0.0, [], base[0][0] / rate
+        for (t_arr, *_), sv_s in zip(base, service):
+            arr = t_arr / rate
+            free_at = max(free_at, arr) + sv_s
+            lat.append((free_at - arr) * 1e3)
+        entry["plain_p50_ms"] = float(np.percentile(lat, 50))
+        entry["plain_p99_ms"] = float(np.percentile(lat, 99))
+        entry["plain_msamples_per_s"] = total / (free_at - first) / 1e6
+    out["plain"] = ("one request at a time through EnvInit/View/ReadFilm: service times "
+                    "measured, latencies from the same arrival times in FIFO order")
+    for g in gs:
+        g.close()
+    B.EnvTerm()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -228,8 +410,10 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     samples_per_step = W_ * H_ * SPP_
 
-    if args.queue or args.bvh_width:
-        B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width)
+    if args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort >= 0:
+        B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width,
+                    persistent=None if args.persistent < 0 else bool(args.persistent),
+                    shade_sort=None if args.shade_sort < 0 else bool(args.shade_sort))
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         B.View(g, cam)
@@ -257,7 +441,7 @@ def run_ours(args):
     prof = B.ReadProfile()
     B.SetProfiling(False)
     t_dev = d.max(sum(dev_ms) / 1e3)
-    value = samples_per_step * args.steps * ws / t_dev / 1e6
+    value = d.job_rate(samples_per_step * args.steps, sum(dev_ms) / 1e3) / 1e6
     rays = st.extend_rays
     shadow = st.shadow_rays
 
@@ -270,8 +454,7 @@ def run_ours(args):
         B.View(g, cam)
         B.ReadFilm(_abi.CG_FILM_XYZ32F, out=host)
     torch.cuda.synchronize()
-    t_e2e = d.max(time.perf_counter() - t0)
-    e2e = samples_per_step * args.steps * ws / t_e2e / 1e6
+    e2e = d.job_rate(samples_per_step * args.steps, time.perf_counter() - t0) / 1e6
 
     # ---- counting pass: algorithmic work of the traversal kernels ----
     B.SetCounting(True)
@@ -284,7 +467,9 @@ def run_ours(args):
     sh_ms, sh_n = prof["shadow"]
     # counting pass totals cover extend + shadow; split the node/tri work by ray count
     per_frame_launch = max(ext_n // max(args.steps, 1), 1)
-    trav_bytes = NODE_B * cst.node_visits + TRI_B * cst.tri_tests + INST_B * cst.inst_visits
+    width = int(B.GetTuning().bvh_width) or 4
+    trav_bytes = (NODE_B[width] * cst.node_visits + TRI_B * cst.tri_tests +
+                  INST_B * cst.inst_visits)
     ext_share = cst.extend_rays / max(cst.extend_rays + cst.shadow_rays, 1)
     ext_bytes_frame = trav_bytes * ext_share + RAY_B * cst.extend_rays
     bytes_per_launch = ext_bytes_frame / per_frame_launch
@@ -297,6 +482,14 @@ def run_ours(args):
         peak, peak_src = 6650.0, "fallback"
 
     cpu = cpu_rate(scene, budget_s=12.0) if (rank == 0 and ws == 1 and not args.no_cpu) else None
+    queue_capacity = int(B.GetTuning().queue_capacity)
+    forms = None
+    if rank == 0 and (args.forms == "on" or (args.forms == "auto" and ws == 1)):
+        del g
+        g = None
+        t_forms = time.perf_counter()
+        forms = {"batched": batched_form(B, torch), "served": served_form(B, torch)}
+        forms["seconds"] = time.perf_counter() - t_forms
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": ws,
@@ -305,7 +498,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "samples_per_step": samples_per_step,
                        "l2": "flushed between steps (256 MiB write)",
-                       "queue_capacity": int(B.GetTuning().queue_capacity),
+                       "queue_capacity": queue_capacity,
                        "parallelism": f"replicas x{ws}"},
             "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": 48,
                     "d2h_bytes_per_step": W_ * H_ * 12},
@@ -313,7 +506,11 @@ def run_ours(args):
             "roofline": {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": None,
+                         "traffic": (EXTEND_TRAFFIC_B if args.case == "full" and width == 4
+                                     else None),
+                         "traffic_source": "ncu dram__bytes_read+write per launch, cold "
+                                           "caches (profiles/dram_traffic_icosphere_"
+                                           "1280x720_16spp_d8.md)",
                          "bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": avg_launch_s * 1e3},
             "kernels_ms": {k: round(v[0], 3) for k, v in prof.items()},
@@ -329,6 +526,8 @@ def run_ours(args):
         }
         if cpu:
             out["cpu_baseline"] = cpu
+        if forms:
+            out["forms"] = forms
         print(json.dumps(out), flush=True)
     del g
     B.EnvTerm()
@@ -348,6 +547,12 @@ def main():
     ap.add_argument("--queue", type=int, default=0, help="ray queue capacity (0 = default)")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4],
                     help="node width of the traversal (0 = library default, 4)")
+    ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
+                    help="persistent lane-refill traversal (-1 = library default)")
+    ap.add_argument("--forms", default="auto", choices=["auto", "on", "off"],
+                    help="batched and served forms vs plain (auto: on at one GPU)")
+    ap.add_argument("--shade-sort", type=int, default=-1, choices=[-1, 0, 1],
+                    help="group rays by material kind before shading (-1 = library default)")
     args = ap.parse_args()
     if args.case == "small":
         global W_, H_, SPP_, WORKLOAD

@@ -189,12 +189,22 @@ int Renderer::init(int dev) {
   CG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CG_CUDA(cudaEventCreate(&ev0));
   CG_CUDA(cudaEventCreate(&ev1));
+  if (wl_tree) return CG_OK;  // adopted from a previous renderer
   CG_CUDA(cudaMalloc(&wl_tree, 65535 * sizeof(float)));
   CG_CUDA(cudaMalloc(&wl_const, 4 * sizeof(float)));
   launchWavelengthTree(wl_tree, wl_const, stream);
   CG_CUDA(cudaGetLastError());
   CG_CUDA(cudaStreamSynchronize(stream));
   return CG_OK;
+}
+
+void Renderer::adoptBuffers(Renderer& prev) {
+  if (prev.stream) cudaStreamSynchronize(prev.stream);
+  std::swap(wl_tree, prev.wl_tree);
+  std::swap(wl_const, prev.wl_const);
+  std::swap(wave_arena.base, prev.wave_arena.base);
+  std::swap(wave_arena.size, prev.wave_arena.size);
+  std::swap(wave, prev.wave);
 }
 
 Renderer::~Renderer() {
@@ -274,6 +284,8 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.extend_block = tuning.extend_block;
   ls.shade_block = tuning.shade_block;
   ls.wide = tuning.bvh_width != 2u;
+  ls.persistent = tuning.persistent != 0u;
+  ls.shade_sort = tuning.shade_sort != 2u;
   profBegin(CG_K_GEN, s);
   launchGen(fc, wave, ch, s);
   profEnd(s);
@@ -428,7 +440,10 @@ Env::~Env() {
   if (rgba) cudaFree(rgba);
 }
 
-static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& out) {
+// `prev` (may be null) is the environment being replaced: on the same device
+// its wavelength tables and ray queues, which do not depend on the film size,
+// move to the new environment instead of being freed and allocated again.
+static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& out, Env* prev) {
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) {
@@ -442,6 +457,11 @@ static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& o
   auto env = std::make_unique<Env>();
   env->conf = conf_in;
   env->conf.trace_depth = std::clamp(conf_in.trace_depth, 1u, 64u);
+  if (prev && prev->device == device) {
+    if (prev->stream) cudaStreamSynchronize(prev->stream);
+    prev->graphs.clear();  // captured graphs point at the adopted queues
+    env->adoptBuffers(*prev);
+  }
   int rc = env->init(device);
   if (rc != CG_OK) return rc;
   const size_t npx = size_t(env->conf.render_width) * env->conf.render_height;
@@ -466,10 +486,11 @@ CG_API const char* cg_last_error(void) { return tl_error.c_str(); }
 CG_API int cg_init(const cg_conf* conf, int device) {
   if (!conf) return fail(CG_E_INVALID, "conf is null");
   std::lock_guard<std::mutex> lk(g_env_mu);
-  delete g_env;
+  std::unique_ptr<Env> prev(g_env);
   g_env = nullptr;
   std::unique_ptr<Env> env;
-  int rc = createEnv(*conf, device, env);
+  int rc = createEnv(*conf, device, env, prev.get());
+  prev.reset();
   if (rc != CG_OK) return rc;
   g_env = env.release();
   return CG_OK;
@@ -738,6 +759,8 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
   if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
   if (t->bvh_width) g_env->tuning.bvh_width = t->bvh_width;
+  g_env->tuning.persistent = t->persistent ? 1u : 0u;
+  if (t->shade_sort) g_env->tuning.shade_sort = t->shade_sort == 2u ? 2u : 1u;
   g_env->tuning.use_graph = t->use_graph;
   g_env->dropAllGraphs();
   return CG_OK;

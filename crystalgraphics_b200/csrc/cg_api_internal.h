@@ -79,11 +79,14 @@ struct Renderer {
   float* wl_tree = nullptr;
   float* wl_const = nullptr;
   bool counting = false;
-  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, {0u, 0u, 0u}};
+  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, 0u, 1u, 0u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
 
   int init(int dev);
+  // Takes over prev's wavelength tables and ray queues (after its stream has
+  // drained); call before init().
+  void adoptBuffers(Renderer& prev);
   int ensureWave(uint32_t capacity);
   // Samples one chunk may hold for this scene and caps (whole trees fit the
   // queues).

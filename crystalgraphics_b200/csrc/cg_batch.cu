@@ -211,17 +211,20 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* be
   const cg_tuning saved = env.tuning;
   const uint32_t caps_q[] = {8u << 20, 16u << 20};
   const uint32_t blocks[] = {128u, 256u};
-  const uint32_t widths[] = {4u, 2u};
+  // kernel variants: (node width, persistent lane refill, shade sort 1 on / 2 off)
+  const uint32_t variants[][3] = {{4u, 0u, 1u}, {4u, 0u, 2u}, {2u, 0u, 1u}, {2u, 1u, 1u}};
   cg_tuning winner = saved;
   float best_ms = 1e30f;
   for (uint32_t q : caps_q) {
     for (uint32_t eb : blocks) {
       for (uint32_t sb : blocks) {
-       for (uint32_t w : widths) {
+       for (const auto& var : variants) {
         env.tuning.queue_capacity = q;
         env.tuning.extend_block = eb;
         env.tuning.shade_block = sb;
-        env.tuning.bvh_width = w;
+        env.tuning.bvh_width = var[0];
+        env.tuning.persistent = var[1];
+        env.tuning.shade_sort = var[2];
         env.tuning.use_graph = 0;
         env.dropAllGraphs();
         float t = 0.0f;

@@ -288,7 +288,7 @@ __device__ __forceinline__ Mat decode(const DevMaterial& m, float w, const Smits
   e.microfacet_roughness = m.roughness * m.roughness;
   e.ior = IOR{real_ior, metallic * im};
   e.transmission = transmission;
-  e.volume = m.volume != 0u;
+  e.volume = (m.volume & 1u) != 0u;
   e.emission = rgbToReflectance(V3{m.emission[0], m.emission[1], m.emission[2]}, sp);
   return e;
 }

@@ -89,6 +89,8 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   if (i == 0) {
     wb.counts[0] = ch.sample_count;
     wb.counts[2] = 0u;
+    wb.counts[3] = 0u;  // work counters of the persistent traversal
+    wb.counts[4] = 0u;
   }
   if (i >= ch.sample_count) return;
   const uint64_t g = ch.sample_begin + i;
@@ -138,6 +140,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
   if (tid == 0) {
     wb.counts[parity ^ 1] = 0u;
     wb.counts[2] = 0u;
+    wb.counts[4] = 0u;
     atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
   }
   TravCounters cnt{0u, 0u, 0u};
@@ -162,6 +165,96 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
       atomicAdd(&wb.stats[4], c);
     }
   }
+}
+
+// ---- persistent traversal with lane refill -------------------------------------
+// Secondary rays of one warp need very different numbers of steps; with one
+// ray per lane the warp waits for its longest ray.  Here each warp loops over
+// the queue: lanes advance their ray a bounded number of steps, and once at
+// least kRefill lanes are idle the warp takes that many new rays from a
+// per-launch work counter (one atomicAdd per refill).  kAny: shadow rays.
+constexpr int kStepBudget = 16;
+constexpr int kRefill = 8;
+
+template <bool kAny, bool kCount>
+__device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuffers& wb, uint32_t n,
+                                                   uint32_t* work, int parity) {
+  const uint32_t lane = threadIdx.x & 31u;
+  TravCounters cnt{0u, 0u, 0u};
+  int32_t stack[kStackSize];
+  TravState st;
+  int32_t ray = -1;
+  bool exhausted = false;
+  while (true) {
+    const unsigned idle = __ballot_sync(kFull, ray < 0);
+    if (!exhausted && __popc(idle) >= kRefill) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(work, static_cast<uint32_t>(__popc(idle)));
+      base = __shfl_sync(kFull, base, 0);
+      if (base + static_cast<uint32_t>(__popc(idle)) >= n) exhausted = true;
+      if (ray < 0) {
+        const uint32_t i = base + static_cast<uint32_t>(__popc(idle & ((1u << lane) - 1u)));
+        if (i < n) {
+          ray = static_cast<int32_t>(i);
+          if (kAny) {
+            const float4 o = wb.sh_o[i], d = wb.sh_d[i];
+            travInit(st, o, d, fminf(d.w, MAXD));
+          } else {
+            travInit(st, wb.ray_o[parity][i], wb.ray_d[parity][i], MAXD);
+          }
+        }
+      }
+    }
+    if (__ballot_sync(kFull, ray >= 0) == 0) {
+      if (exhausted) break;
+      continue;
+    }
+    if (ray >= 0 && travSteps<kAny, kCount>(sc, st, stack, kStepBudget, cnt, wb.status)) {
+      if (kAny) {
+        if (st.best.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[ray]], wb.sh_o[ray].w);
+      } else {
+        wb.hit[ray] = make_float4(st.best.t, st.best.u, st.best.v, __uint_as_float(st.best.tri));
+        wb.hit_inst[ray] = st.best.inst;
+      }
+      ray = -1;
+    }
+  }
+  if (kCount) {
+    unsigned long long a = cnt.nodes, b = cnt.tris, c = cnt.insts;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(kFull, a, o);
+      b += __shfl_down_sync(kFull, b, o);
+      c += __shfl_down_sync(kFull, c, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&wb.stats[2], a);
+      atomicAdd(&wb.stats[3], b);
+      atomicAdd(&wb.stats[4], c);
+    }
+  }
+}
+
+// counts[3] (extend) and counts[4] (shadow) are the work counters; each is
+// zeroed by the kernel before its user in stream order (k_gen for depth 0,
+// k_shade for the next extend, k_extend for the shadow launch after it).
+template <bool kCount>
+__global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, WaveBuffers wb,
+                                                              int parity) {
+  const uint32_t n = min(wb.counts[parity], wb.capacity);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    wb.counts[parity ^ 1] = 0u;
+    wb.counts[2] = 0u;
+    wb.counts[4] = 0u;
+    atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
+  }
+  persistentTraverse<false, kCount>(sc, wb, n, &wb.counts[3], parity);
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(256, 4) k_shadow_persistent(SceneView sc, WaveBuffers wb) {
+  const uint32_t n = min(wb.counts[2], wb.capacity);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wb.stats[1], static_cast<unsigned long long>(n));
+  persistentTraverse<true, kCount>(sc, wb, n, &wb.counts[4], 0);
 }
 
 // ---- shadow: t-bounded any hit (solveEmission, trace.wesl:91-113) ----------------
@@ -321,17 +414,57 @@ struct Child {
 };
 
 // ---- shade: one tree node per ray ------------------------------------------------
-__global__ void k_shade(SceneView sc, FrameConst fc, WaveBuffers wb, int depth, int parity) {
+// Shading keys: 0 miss, 1 hit beyond the depth cut (no work), 2 + material
+// kind; kNumKeys - 1 marks an empty slot.
+constexpr int kNumKeys = 19;
+
+__device__ __forceinline__ int shadeKey(const SceneView& sc, const WaveBuffers& wb, uint32_t i,
+                                        bool cut) {
+  const int32_t inst = wb.hit_inst[i];
+  if (inst < 0) return 0;
+  if (cut) return 1;
+  const uint4 meta = __ldg(reinterpret_cast<const uint4*>(sc.inst + inst) + 3);
+  return 2 + static_cast<int>((sc.mat[meta.y].volume >> kKindShift) & 15u);
+}
+
+// kSort: before shading, every block sorts its slice of the queue by shading
+// key in shared memory (counting sort), so a warp shades misses, cut hits or
+// one material kind rather than a mix of code paths.
+template <bool kSort>
+__global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
+                                               int depth, int parity) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const int out = parity ^ 1;
+  __shared__ int s_cnt[kNumKeys];
+  __shared__ int s_off[kNumKeys];
+  __shared__ uint16_t s_order[256];
   const uint32_t cut_depth = max(1u, min(fc.caps.trace_depth, 64u)) - 1u;
   const SampleCaps caps{fc.caps.trace_depth, fc.caps.transport_cap, fc.caps.emission_cap,
                         fc.caps.diffuse_cap, fc.caps.rough_cap};
-  for (uint32_t base = warp * 32u; base < n; base += nwarps * 32u) {
-    const uint32_t i = base + lane;
+  if (blockIdx.x == 0 && threadIdx.x == 0) wb.counts[3] = 0u;  // next extend's work counter
+  for (uint32_t bbase = blockIdx.x * blockDim.x; bbase < n; bbase += gridDim.x * blockDim.x) {
+    uint32_t i = bbase + threadIdx.x;
+    if (kSort) {
+      const int key = i < n ? shadeKey(sc, wb, i, static_cast<uint32_t>(depth) >= cut_depth)
+                            : kNumKeys - 1;
+      if (threadIdx.x < kNumKeys) s_cnt[threadIdx.x] = 0;
+      __syncthreads();
+      const int rank = atomicAdd(&s_cnt[key], 1);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < kNumKeys; ++k) {
+          s_off[k] = acc;
+          acc += s_cnt[k];
+        }
+      }
+      __syncthreads();
+      s_order[s_off[key] + rank] = static_cast<uint16_t>(threadIdx.x);
+      __syncthreads();
+      i = bbase + s_order[threadIdx.x];
+      __syncthreads();  // s_order / s_cnt are rewritten by the next slice
+    }
     Child ch[4];
     uint32_t nch = 0;
     bool shadow = false;
@@ -596,6 +729,14 @@ void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
+  if (ls.persistent) {  // one resident grid: 64 registers -> 65536 / (64 * block) blocks per SM
+    const uint32_t pgrid = gridFor(1024u / block);
+    if (counting)
+      k_extend_persistent<true><<<pgrid, block, 0, s>>>(sc, wb, parity);
+    else
+      k_extend_persistent<false><<<pgrid, block, 0, s>>>(sc, wb, parity);
+    return;
+  }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
   if (counting && ls.wide)
     k_extend<true, true><<<grid, block, 0, s>>>(sc, wb, parity);
@@ -609,14 +750,25 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
 
 void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
                  int parity, const LaunchShape& ls, cudaStream_t s) {
-  const uint32_t block = ls.shade_block;
+  const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
-  k_shade<<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+  if (ls.shade_sort)
+    k_shade<true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+  else
+    k_shade<false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
 }
 
 void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
+  if (ls.persistent) {
+    const uint32_t pgrid = gridFor(1024u / block);
+    if (counting)
+      k_shadow_persistent<true><<<pgrid, block, 0, s>>>(sc, wb);
+    else
+      k_shadow_persistent<false><<<pgrid, block, 0, s>>>(sc, wb);
+    return;
+  }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
   if (counting && ls.wide)
     k_shadow<true, true><<<grid, block, 0, s>>>(sc, wb);

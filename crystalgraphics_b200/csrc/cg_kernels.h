@@ -79,6 +79,8 @@ struct LaunchShape {
   uint32_t grid_extend = 0;  // 0: derived from the SM count
   uint32_t grid_shade = 0;
   bool wide = true;          // traverse the four-wide trees
+  bool persistent = false;   // persistent warps with lane refill (binary trees)
+  bool shade_sort = true;    // group a block's rays by shading key before shading
 };
 
 void launchWavelengthTree(float* tree, float* consts, cudaStream_t s);

@@ -236,6 +236,13 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
     dm.dispersion = m.dispersion;
     dm.transmission = clamp01(m.transmission_factor);
     dm.volume = m.thickness_factor > 0.0f ? 1u : 0u;
+    {
+      uint32_t kind = 0;
+      if ((1.0f - dm.metallic) * (1.0f - dm.transmission) > 0.0f) kind |= 1u;
+      kind |= dm.roughness == 0.0f ? 2u : 4u;
+      if (dm.transmission > 1e-6f) kind |= 8u;
+      dm.volume |= kind << kKindShift;
+    }
     s.mat.push_back(dm);
     uint32_t lobes = 1;  // a reflection lobe
     if ((1.0f - dm.metallic) * (1.0f - dm.transmission) > 0.0f) ++lobes;

@@ -192,6 +192,134 @@ __device__ __forceinline__ HitRec traceRay(const SceneView& sc, float wox, float
   return best;
 }
 
+// Traversal state of one ray, advanced a bounded number of steps at a time so
+// a warp can refill lanes whose ray finished (persistent threads with
+// dynamic fetch): the closest-hit walk of traceRay, resumable.
+struct TravState {
+  float wox, woy, woz, wdx, wdy, wdz;  // world ray
+  float ox, oy, oz, dx, dy, dz;        // ray in the current (world or instance) space
+  float idx, idy, idz, oix, oiy, oiz;
+  int32_t node;
+  int32_t sp;
+  int32_t cur_inst;                    // -1 in the TLAS
+  HitRec best;
+};
+
+__device__ __forceinline__ void travInit(TravState& s, float4 o, float4 d, float tmax) {
+  s.wox = s.ox = o.x; s.woy = s.oy = o.y; s.woz = s.oz = o.z;
+  s.wdx = s.dx = d.x; s.wdy = s.dy = d.y; s.wdz = s.dz = d.z;
+  s.idx = safeInv(s.dx); s.idy = safeInv(s.dy); s.idz = safeInv(s.dz);
+  s.oix = s.ox * s.idx; s.oiy = s.oy * s.idy; s.oiz = s.oz * s.idz;
+  s.node = 0;
+  s.sp = 0;
+  s.cur_inst = -1;
+  s.best = HitRec{tmax, 0.0f, 0.0f, -1, 0u};
+}
+
+// Runs at most `budget` steps (a node visit, a leaf, or a return to the
+// TLAS); returns true when the ray is finished (s.best holds its hit; with
+// kAny the first hit below s.best.t finishes it).
+template <bool kAny, bool kCount>
+__device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int32_t* stack,
+                                          int budget, TravCounters& cnt, uint32_t* status) {
+  for (int step = 0; step < budget; ++step) {
+    const int32_t node = s.node;
+    if (node >= 0) {
+      const BvhNode* nodes = s.cur_inst < 0 ? sc.tlas : sc.blas;
+      const float4* np = reinterpret_cast<const float4*>(nodes + node);
+      const float4 n0 = __ldg(np);
+      const float4 n1 = __ldg(np + 1);
+      const float4 n2 = __ldg(np + 2);
+      const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+      if (kCount) ++cnt.nodes;
+      const float a0 = fmaf(n0.x, s.idx, -s.oix), a1 = fmaf(n0.y, s.idx, -s.oix);
+      const float b0 = fmaf(n0.z, s.idy, -s.oiy), b1 = fmaf(n0.w, s.idy, -s.oiy);
+      const float c0 = fmaf(n2.x, s.idz, -s.oiz), c1 = fmaf(n2.y, s.idz, -s.oiz);
+      const float t0min = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
+      const float t0max = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), s.best.t));
+      const float d0 = fmaf(n1.x, s.idx, -s.oix), d1 = fmaf(n1.y, s.idx, -s.oix);
+      const float e0 = fmaf(n1.z, s.idy, -s.oiy), e1 = fmaf(n1.w, s.idy, -s.oiy);
+      const float f0 = fmaf(n2.z, s.idz, -s.oiz), f1 = fmaf(n2.w, s.idz, -s.oiz);
+      const float t1min = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), 0.0f));
+      const float t1max = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), s.best.t));
+      const bool h0 = t0min <= t0max;
+      const bool h1 = t1min <= t1max;
+      if (h0 && h1) {
+        int32_t near = n3.x, far = n3.y;
+        if (t1min < t0min) {
+          near = n3.y;
+          far = n3.x;
+        }
+        if (s.sp >= kStackSize) {
+          atomicOr(status, 1u);
+          s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
+          return true;
+        }
+        stack[s.sp++] = far;
+        s.node = near;
+      } else if (h0) {
+        s.node = n3.x;
+      } else if (h1) {
+        s.node = n3.y;
+      } else {
+        s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+      }
+      continue;
+    }
+    if (node == kDone) return true;
+    if (node == kToTlas) {
+      s.cur_inst = -1;
+      s.ox = s.wox; s.oy = s.woy; s.oz = s.woz;
+      s.dx = s.wdx; s.dy = s.wdy; s.dz = s.wdz;
+      s.idx = safeInv(s.dx); s.idy = safeInv(s.dy); s.idz = safeInv(s.dz);
+      s.oix = s.ox * s.idx; s.oiy = s.oy * s.idy; s.oiz = s.oz * s.idz;
+      s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+      continue;
+    }
+    const uint32_t first = static_cast<uint32_t>(~node) >> 3;
+    const uint32_t count = static_cast<uint32_t>(~node) & 7u;
+    if (s.cur_inst < 0) {
+      if (count == 0u) {
+        s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+        continue;
+      }
+      const float4* ipf = reinterpret_cast<const float4*>(sc.inst + first);
+      const float4 r0 = __ldg(ipf), r1 = __ldg(ipf + 1), r2 = __ldg(ipf + 2);
+      const uint4 meta = __ldg(reinterpret_cast<const uint4*>(ipf + 3));
+      const float m[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+      if (kCount) ++cnt.insts;
+      toLocal(m, s.wox, s.woy, s.woz, s.wdx, s.wdy, s.wdz, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz);
+      s.idx = safeInv(s.dx); s.idy = safeInv(s.dy); s.idz = safeInv(s.dz);
+      s.oix = s.ox * s.idx; s.oiy = s.oy * s.idy; s.oiz = s.oz * s.idz;
+      if (s.sp >= kStackSize) {
+        atomicOr(status, 1u);
+        s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
+        return true;
+      }
+      stack[s.sp++] = kToTlas;
+      s.cur_inst = static_cast<int32_t>(first);
+      s.node = static_cast<int32_t>(meta.x);  // blas_root
+      continue;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+      const float4* tp = sc.tris + 3u * (first + k);
+      const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
+      if (kCount) ++cnt.tris;
+      float t, u, v;
+      if (intersectTri(s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, ta, tb, tc, t, u, v) && t < s.best.t) {
+        s.best.t = t;
+        s.best.u = u;
+        s.best.v = v;
+        s.best.inst = s.cur_inst;
+        s.best.tri = first + k;
+        if (kAny) return true;
+      }
+    }
+    s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+  }
+  return false;
+}
+
 __device__ __forceinline__ void cswap(float& ka, int32_t& la, float& kb, int32_t& lb) {
   if (kb < ka) {
     const float tk = ka;

@@ -67,8 +67,12 @@ struct alignas(16) DevMaterial {
   float ior;
   float dispersion;
   float transmission;     // clamp(transmission, 0, 1)
-  uint32_t volume;        // thickness_factor > 0
+  uint32_t volume;        // bit 0: thickness_factor > 0; bits 8..11: shading kind
 };
+// Shading kind of a material: which lobe code paths a hit on it can take
+// (bit 0 diffuse, bit 1 specular, bit 2 rough, bit 3 transmission).  Hits are
+// grouped by kind before shading so a warp runs one path.
+constexpr uint32_t kKindShift = 8u;
 static_assert(sizeof(DevMaterial) == 48, "DevMaterial is 48 bytes");
 
 // Emissive triangle for the light-pdf sum (pdf/emission.wesl:120-179):

@@ -306,7 +306,11 @@ typedef struct cg_tuning {
   uint32_t shade_block;
   uint32_t use_graph;   /* 1 = capture the chunk pipeline as a CUDA graph */
   uint32_t bvh_width;   /* 4 (default) or 2: node width the traversal walks */
-  uint32_t _pad[3];
+  uint32_t persistent;  /* 1 = persistent traversal warps that refill idle lanes
+                           (binary trees), 0 = one ray per thread */
+  uint32_t shade_sort;  /* 1 (default) = group rays by material kind before
+                           shading, 2 = do not, 0 = keep */
+  uint32_t _pad;
 } cg_tuning;
 CG_API int cg_set_tuning(const cg_tuning* tuning);
 CG_API int cg_get_tuning(cg_tuning* out);

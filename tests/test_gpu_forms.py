@@ -164,6 +164,31 @@ def test_server_cancel_and_timeout(cornell):
         assert sv.stats().cancelled == 1
 
 
+@pytest.mark.parametrize("variant", [dict(bvh_width=2, persistent=False),
+                                     dict(bvh_width=2, persistent=True),
+                                     dict(bvh_width=4, persistent=False),
+                                     dict(bvh_width=4, persistent=False, shade_sort=False)])
+def test_traversal_variants_render_the_same_samples(variant):
+    """Binary or four-wide trees, one ray per thread or persistent warps, rays
+    grouped by material before shading or not: the closest hits and the keyed
+    samples are the same, so the frames are (up to float atomic order)."""
+    s = scenes.icosphere_scene(subdiv=4)
+    B.EnvInit(B.PathTraceConf(render_width=96, render_height=54, sample_count=4, trace_depth=8))
+    g = B.LoadScene(s)
+    cam = B.Camera.from_c(s.camera)
+    B.SetTuning(bvh_width=4, persistent=False, shade_sort=True)
+    B.View(g, cam)
+    ref = B.ReadFilm()
+    B.EnvInit(B.PathTraceConf(render_width=96, render_height=54, sample_count=4, trace_depth=8))
+    B.SetTuning(**variant)
+    B.View(g, cam)
+    out = B.ReadFilm()
+    st = B.LastStats()
+    assert _close(out, ref) < RTOL
+    assert st.extend_rays > 0 and st.shadow_rays > 0
+    g.close()
+
+
 def test_autotune_returns_a_valid_tuning(cornell):
     s, g = cornell
     t = B.autotune(g, (s.camera.position[:], s.camera.direction[:], 96, 96, 4, 1))
