@@ -44,12 +44,15 @@ WORKLOAD = ("displaced dispersive icosphere: 1,310,720 tris, rough dispersive di
             "ground + 64 emissive tris, 1280x720, 16 spp, depth 8 (plain View())")
 W_, H_, SPP_, DEPTH_ = 1280, 720, 16, 8
 # bytes the traversal reads per unit of work (the device layout): a node
-# visit reads one 128 B Bvh4Node (four child boxes and links; 64 B BvhNode with
-# two child boxes on the binary trees), a triangle test one 48 B triangle
+# visit reads one 128 B Bvh4Node (four float child boxes and links; 64 B
+# Bvh4QNode with 8-bit boxes; 64 B BvhNode with two child boxes on the binary
+# trees), a triangle test one 48 B triangle
 # record, an instance entry one 64 B DevInstance; per ray the kernel reads
 # 32 B of ray and writes 20 B of hit
-NODE_B = {4: 128, 2: 64}
+NODE_B = {4: 128, "4q": 64, 2: 64}
 TRI_B, INST_B, RAY_B = 48, 64, 52
+# non-tensor FP32 peak (nominal; no measured figure exists for it)
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # DRAM bytes (read + write) per k_extend launch of this workload, mean of the
 # seven launches of one chunk in profiles/dram_traffic_icosphere_1280x720_16spp_d8.md
 # (ncu, cold caches: an upper bound)
@@ -168,8 +171,27 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+# --workload: the plain-path configurations (the icosphere frame is the default
+# and the headline; the others fill the per-configuration table)
+WORKLOADS = {
+    "icosphere": (1280, 720, 16, 8, WORKLOAD),
+    "cornell": (256, 256, 1, 2, "Cornell box: 5 wall quads, a diffuse and a specular-conductor box, "
+                                "0.25x0.25 ceiling light of radiance 15; 256x256, 1 spp, depth 2 "
+                                "(plain View())"),
+    "instanced": (1920, 1080, 64, 12, "instanced scene: 4096 instances of 8 noise-displaced "
+                                      "spheres/tori (10k-200k tris), 40/30/20/10 material mix, "
+                                      "10k emissive tris; 1920x1080, 64 spp, depth 12 "
+                                      "(plain View())"),
+}
+WORKLOAD_NAME = "icosphere"
+
+
 def make_workload():
     from crystalgraphics_b200 import scenes
+    if WORKLOAD_NAME == "cornell":
+        return scenes.cornell(width=W_, height=H_, spp=SPP_, depth=DEPTH_)
+    if WORKLOAD_NAME == "instanced":
+        return scenes.instanced_scene(width=W_, height=H_, spp=SPP_, depth=DEPTH_)
     return scenes.icosphere_scene(width=W_, height=H_, spp=SPP_, depth=DEPTH_)
 
 
@@ -193,7 +215,8 @@ def cpu_rate(scene, budget_s=12.0, threads=0):
     film = np.zeros((H_, W_, 3), np.float32)
     seeds = np.zeros((H_, W_), np.uint32)
     while spent < budget_s:
-        start = int(rng.integers(0, W_ * H_ - n))
+        n = min(n, W_ * H_)
+        start = int(rng.integers(0, W_ * H_ - n + 1))
         t0 = time.perf_counter()
         o.render(conf, scene.camera, film=film, seeds=seeds, rng=O.RNG_REFERENCE,
                  threads=threads, pixel_range=(start, start + n))
@@ -405,15 +428,19 @@ def run_ours(args):
     conf = B.PathTraceConf(render_width=W_, render_height=H_, sample_count=SPP_, trace_depth=DEPTH_)
     B.EnvInit(conf, device=local)
     B.SetSeed(1000 * rank)
+    t_load = time.perf_counter()
     g = B.LoadScene(scene)
+    t_load = time.perf_counter() - t_load
     cam = B.Camera.from_c(scene.camera)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     samples_per_step = W_ * H_ * SPP_
 
-    if args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort >= 0:
+    if (args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort >= 0 or
+            args.box_bits):
         B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width,
                     persistent=None if args.persistent < 0 else bool(args.persistent),
-                    shade_sort=None if args.shade_sort < 0 else bool(args.shade_sort))
+                    shade_sort=None if args.shade_sort < 0 else bool(args.shade_sort),
+                    box_bits=args.box_bits)
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         B.View(g, cam)
@@ -467,14 +494,21 @@ def run_ours(args):
     sh_ms, sh_n = prof["shadow"]
     # counting pass totals cover extend + shadow; split the node/tri work by ray count
     per_frame_launch = max(ext_n // max(args.steps, 1), 1)
-    width = int(B.GetTuning().bvh_width) or 4
-    trav_bytes = (NODE_B[width] * cst.node_visits + TRI_B * cst.tri_tests +
+    tun = B.GetTuning()
+    width = int(tun.bvh_width) or 4
+    node_b = NODE_B["4q"] if width == 4 and int(tun.box_bits) == 8 else NODE_B[width]
+    trav_bytes = (node_b * cst.node_visits + TRI_B * cst.tri_tests +
                   INST_B * cst.inst_visits)
     ext_share = cst.extend_rays / max(cst.extend_rays + cst.shadow_rays, 1)
     ext_bytes_frame = trav_bytes * ext_share + RAY_B * cst.extend_rays
     bytes_per_launch = ext_bytes_frame / per_frame_launch
     avg_launch_s = ext_ms / 1e3 / max(ext_n, 1)
     achieved = bytes_per_launch / avg_launch_s / 1e9
+    # FP32 work of the same launches: 16 flops per child box tested (6 sub, 6 mul,
+    # 4 min/max folded) and 40 per Moller-Trumbore test
+    boxes = (width if width == 2 else 4) * cst.node_visits
+    flops_per_launch = (16 * boxes + 40 * cst.tri_tests) * ext_share / per_frame_launch
+    fp32_achieved = flops_per_launch / avg_launch_s / 1e12
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
@@ -484,7 +518,8 @@ def run_ours(args):
     cpu = cpu_rate(scene, budget_s=12.0) if (rank == 0 and ws == 1 and not args.no_cpu) else None
     queue_capacity = int(B.GetTuning().queue_capacity)
     forms = None
-    if rank == 0 and (args.forms == "on" or (args.forms == "auto" and ws == 1)):
+    if rank == 0 and (args.forms == "on" or (args.forms == "auto" and ws == 1 and
+                                              WORKLOAD_NAME == "icosphere" and args.case == "full")):
         del g
         g = None
         t_forms = time.perf_counter()
@@ -506,13 +541,19 @@ def run_ours(args):
             "roofline": {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": (EXTEND_TRAFFIC_B if args.case == "full" and width == 4
+                         "traffic": (EXTEND_TRAFFIC_B if (args.case == "full" and width == 4 and
+                                                          node_b == NODE_B[4] and
+                                                          WORKLOAD_NAME == "icosphere")
                                      else None),
                          "traffic_source": "ncu dram__bytes_read+write per launch, cold "
                                            "caches (profiles/dram_traffic_icosphere_"
                                            "1280x720_16spp_d8.md)",
                          "bytes_per_launch": bytes_per_launch,
-                         "avg_launch_ms": avg_launch_s * 1e3},
+                         "avg_launch_ms": avg_launch_s * 1e3,
+                         "fp32": {"achieved": fp32_achieved, "peak": FP32_PEAK_TFLOPS,
+                                  "unit": "TFLOP/s", "frac": fp32_achieved / FP32_PEAK_TFLOPS,
+                                  "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x "
+                                                 "1.965 GHz (not measured)"}},
             "kernels_ms": {k: round(v[0], 3) for k, v in prof.items()},
             "kernels_launches": {k: int(v[1]) for k, v in prof.items()},
             "dominant_kernel": dominant,
@@ -522,6 +563,7 @@ def run_ours(args):
                                            "tri_tests": int(cst.tri_tests),
                                            "inst_visits": int(cst.inst_visits)},
             "wall_ms_per_step": wall / args.steps * 1e3,
+            "load_scene_s": t_load,
             "clocks": clocks.summary(),
         }
         if cpu:
@@ -541,24 +583,37 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="full", choices=["full", "small"],
-                    help="small: the same scene at 320x180, 4 spp, with a 2M-ray queue "
-                         "(the case ncu --set full captures)")
+    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS),
+                    help="plain-path configuration (default: the icosphere frame)")
+    ap.add_argument("--case", default="full", choices=["full", "medium", "small"],
+                    help="small: the same scene at 320x180, 4 spp, with a 2M-ray queue; "
+                         "medium: 640x360, 16 spp with the default queue (two chunks per "
+                         "frame of the same size as the full frame's eight): the cases "
+                         "ncu --set full captures")
     ap.add_argument("--queue", type=int, default=0, help="ray queue capacity (0 = default)")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4],
                     help="node width of the traversal (0 = library default, 4)")
     ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
                     help="persistent lane-refill traversal (-1 = library default)")
+    ap.add_argument("--box-bits", type=int, default=0, choices=[0, 8, 32],
+                    help="four-wide child box precision (0 = library default, 32)")
     ap.add_argument("--forms", default="auto", choices=["auto", "on", "off"],
                     help="batched and served forms vs plain (auto: on at one GPU)")
     ap.add_argument("--shade-sort", type=int, default=-1, choices=[-1, 0, 1],
                     help="group rays by material kind before shading (-1 = library default)")
     args = ap.parse_args()
+    global W_, H_, SPP_, DEPTH_, WORKLOAD, WORKLOAD_NAME
+    WORKLOAD_NAME = args.workload
+    W_, H_, SPP_, DEPTH_, WORKLOAD = WORKLOADS[args.workload]
+    if args.case != "full" and args.workload != "icosphere":
+        ap.error("--case applies to the icosphere workload")
     if args.case == "small":
-        global W_, H_, SPP_, WORKLOAD
         W_, H_, SPP_ = 320, 180, 4
         WORKLOAD = WORKLOAD.replace("1280x720, 16 spp", "320x180, 4 spp")
         args.queue = args.queue or (2 << 20)
+    elif args.case == "medium":
+        W_, H_ = 640, 360
+        WORKLOAD = WORKLOAD.replace("1280x720", "640x360")
     if args.impl == "reference":
         run_reference(args)
     else:

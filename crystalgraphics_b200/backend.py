@@ -300,7 +300,7 @@ def SetSeed(seed: int) -> None:
 
 
 def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_width=0,
-              persistent=None, shade_sort=None) -> None:
+              persistent=None, shade_sort=None, box_bits=0) -> None:
     """0 (or None for the two switches) keeps the current value."""
     if persistent is None:
         cur = _abi.CgTuning()
@@ -308,7 +308,7 @@ def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_
         persistent = cur.persistent
     sort = 0 if shade_sort is None else (1 if shade_sort else 2)
     t = _abi.CgTuning(queue_capacity, extend_block, shade_block, use_graph, bvh_width,
-                      1 if persistent else 0, sort)
+                      1 if persistent else 0, sort, box_bits)
     _check(lib.cg_set_tuning(C.byref(t)))
 
 

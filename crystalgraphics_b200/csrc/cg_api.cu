@@ -75,7 +75,8 @@ int uploadScene(const HostScene& h, SceneDev& s) {
       {h.mat.data(), bytesOf(h.mat), 0},         {h.eprim.data(), bytesOf(h.eprim), 0},
       {h.alias.data(), bytesOf(h.alias), 0},     {h.light_bvh.data(), bytesOf(h.light_bvh), 0},
       {h.ltri.data(), bytesOf(h.ltri), 0},       {h.env.data(), bytesOf(h.env), 0},
-      {h.tlas4.data(), bytesOf(h.tlas4), 0},     {h.blas4.data(), bytesOf(h.blas4), 0}};
+      {h.tlas4.data(), bytesOf(h.tlas4), 0},     {h.blas4.data(), bytesOf(h.blas4), 0},
+      {h.tlas4q.data(), bytesOf(h.tlas4q), 0},   {h.blas4q.data(), bytesOf(h.blas4q), 0}};
   size_t total = 0;
   for (auto& p : parts) {
     p.off = total;
@@ -101,6 +102,8 @@ int uploadScene(const HostScene& h, SceneDev& s) {
   v.env = reinterpret_cast<const float4*>(base + parts[11].off);
   v.tlas4 = reinterpret_cast<const Bvh4Node*>(base + parts[12].off);
   v.blas4 = reinterpret_cast<const Bvh4Node*>(base + parts[13].off);
+  v.tlas4q = reinterpret_cast<const Bvh4QNode*>(base + parts[14].off);
+  v.blas4q = reinterpret_cast<const Bvh4QNode*>(base + parts[15].off);
   v.env_w = h.env_w;
   v.env_h = h.env_h;
   v.emissive_count = static_cast<uint32_t>(h.eprim.size());
@@ -283,7 +286,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   LaunchShape ls;
   ls.extend_block = tuning.extend_block;
   ls.shade_block = tuning.shade_block;
-  ls.wide = tuning.bvh_width != 2u;
+  ls.nodes = nodeFormatOf(tuning);
   ls.persistent = tuning.persistent != 0u;
   ls.shade_sort = tuning.shade_sort != 2u;
   profBegin(CG_K_GEN, s);
@@ -553,6 +556,7 @@ CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
   HostScene& h = sd->host;
   std::vector<BvhNode>().swap(h.blas);
   std::vector<Bvh4Node>().swap(h.blas4);
+  std::vector<Bvh4QNode>().swap(h.blas4q);
   std::vector<float>().swap(h.tris);
   std::vector<uint32_t>().swap(h.tri_vidx);
   std::vector<float>().swap(h.vnormal);
@@ -756,6 +760,9 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (t->queue_capacity) g_env->tuning.queue_capacity = t->queue_capacity;
   if (t->bvh_width && t->bvh_width != 2 && t->bvh_width != 4)
     return fail(CG_E_INVALID, "bvh_width must be 2 or 4");
+  if (t->box_bits && t->box_bits != 8 && t->box_bits != 32)
+    return fail(CG_E_INVALID, "box_bits must be 8 or 32");
+  if (t->box_bits) g_env->tuning.box_bits = t->box_bits;
   if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
   if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
   if (t->bvh_width) g_env->tuning.bvh_width = t->bvh_width;
@@ -793,7 +800,7 @@ CG_API int cg_trace_closest(cg_scene_t scene, const float* rays, uint32_t n, cg_
   uint32_t* d_status = reinterpret_cast<uint32_t*>(p + align256(rb) + 2 * align256(ob));
   CG_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, env.stream));
   CG_CUDA(cudaMemsetAsync(d_status, 0, 4, env.stream));
-  launchTraceClosest(s->view, d_rays, n, d_tuv, d_ids, d_status, env.tuning.bvh_width != 2u,
+  launchTraceClosest(s->view, d_rays, n, d_tuv, d_ids, d_status, nodeFormatOf(env.tuning),
                      env.stream);
   CG_CUDA(cudaGetLastError());
   std::vector<float4> tuv(n);

@@ -53,6 +53,13 @@ struct SceneDev {
 
 int uploadScene(const HostScene& h, SceneDev& s);
 
+// The traversal's node format for a tuning (binary, or four-wide with 32-bit
+// or 8-bit child boxes).
+inline int nodeFormatOf(const cg_tuning& t) {
+  if (t.bvh_width == 2u) return kNodesBinary;
+  return t.box_bits == 8u ? kNodesWide4Q : kNodesWide4;
+}
+
 struct LevelPlan {
   uint32_t levels = 0;      // depths that can hold rays
   bool shadow[64] = {};     // depths that can draw a light sample
@@ -79,7 +86,7 @@ struct Renderer {
   float* wl_tree = nullptr;
   float* wl_const = nullptr;
   bool counting = false;
-  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, 0u, 1u, 0u};
+  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, 0u, 1u, 32u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
 

@@ -211,8 +211,10 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* be
   const cg_tuning saved = env.tuning;
   const uint32_t caps_q[] = {8u << 20, 16u << 20};
   const uint32_t blocks[] = {128u, 256u};
-  // kernel variants: (node width, persistent lane refill, shade sort 1 on / 2 off)
-  const uint32_t variants[][3] = {{4u, 0u, 1u}, {4u, 0u, 2u}, {2u, 0u, 1u}, {2u, 1u, 1u}};
+  // kernel variants: (node width, persistent lane refill, shade sort 1 on / 2 off,
+  // bits per child box bound)
+  const uint32_t variants[][4] = {
+      {4u, 0u, 1u, 8u}, {4u, 0u, 1u, 32u}, {4u, 0u, 2u, 8u}, {2u, 0u, 1u, 8u}, {2u, 1u, 1u, 8u}};
   cg_tuning winner = saved;
   float best_ms = 1e30f;
   for (uint32_t q : caps_q) {
@@ -225,6 +227,7 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* be
         env.tuning.bvh_width = var[0];
         env.tuning.persistent = var[1];
         env.tuning.shade_sort = var[2];
+        env.tuning.box_bits = var[3];
         env.tuning.use_graph = 0;
         env.dropAllGraphs();
         float t = 0.0f;

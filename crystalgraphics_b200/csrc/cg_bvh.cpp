@@ -262,6 +262,64 @@ uint32_t collapseBvh4(const std::vector<BvhNode>& bvh2, uint32_t root2, std::vec
   return collapse(bvh2, root2, out);
 }
 
+void quantizeBvh4(const std::vector<Bvh4Node>& in, std::vector<Bvh4QNode>& out) {
+  out.resize(in.size());
+  for (size_t i = 0; i < in.size(); ++i) {
+    const Bvh4Node& n = in[i];
+    Bvh4QNode q{};
+    const float* lo[3] = {n.lox, n.loy, n.loz};
+    const float* hi[3] = {n.hix, n.hiy, n.hiz};
+    float org[3] = {0.0f, 0.0f, 0.0f};
+    int exps[3] = {0, 0, 0};
+    uint32_t qlo[3] = {0u, 0u, 0u}, qhi[3] = {0u, 0u, 0u};
+    for (int a = 0; a < 3; ++a) {
+      float mn = std::numeric_limits<float>::infinity(), mx = -mn;
+      for (int c = 0; c < 4; ++c) {
+        if (n.child[c] == kEmptyLink) continue;
+        mn = std::min(mn, lo[a][c]);
+        mx = std::max(mx, hi[a][c]);
+      }
+      if (!(mn <= mx)) mn = mx = 0.0f;  // no children
+      org[a] = mn;
+      // smallest power of two s with 255 * s >= extent (s >= 2^-126)
+      const double ext = static_cast<double>(mx) - static_cast<double>(mn);
+      int k = -126;
+      if (ext > 0.0) {
+        k = static_cast<int>(std::ceil(std::log2(ext / 255.0)));
+        while (k > -126 && std::ldexp(255.0, k - 1) >= ext) --k;
+        while (std::ldexp(255.0, k) < ext) ++k;
+        k = std::max(k, -126);
+      }
+      exps[a] = k;
+      const double s = std::ldexp(1.0, k);
+      for (int c = 0; c < 4; ++c) {
+        if (n.child[c] == kEmptyLink) continue;
+        // outward rounding: org + ql * s <= lo and org + qh * s >= hi exactly,
+        // and a float rounding of either stays on the same side
+        const double fl = std::floor((static_cast<double>(lo[a][c]) - mn) / s);
+        const double ch = std::ceil((static_cast<double>(hi[a][c]) - mn) / s);
+        const uint32_t ql = static_cast<uint32_t>(std::clamp(fl, 0.0, 255.0));
+        const uint32_t qh = static_cast<uint32_t>(std::clamp(ch, 0.0, 255.0));
+        qlo[a] |= ql << (8 * c);
+        qhi[a] |= qh << (8 * c);
+      }
+    }
+    q.ox = org[0];
+    q.oy = org[1];
+    q.oz = org[2];
+    q.scale_bits = static_cast<uint32_t>(exps[0] + 127) | (static_cast<uint32_t>(exps[1] + 127) << 8) |
+                   (static_cast<uint32_t>(exps[2] + 127) << 16);
+    q.qlox = qlo[0];
+    q.qhix = qhi[0];
+    q.qloy = qlo[1];
+    q.qhiy = qhi[1];
+    q.qloz = qlo[2];
+    q.qhiz = qhi[2];
+    for (int c = 0; c < 4; ++c) q.child[c] = n.child[c];
+    out[i] = q;
+  }
+}
+
 uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt, uint32_t prim_base,
                   std::vector<BvhNode>& nodes, std::vector<uint32_t>& order,
                   uint32_t* depth_out) {

@@ -47,14 +47,17 @@ inline uint32_t leafCount(int32_t link) { return static_cast<uint32_t>(~link) & 
 // never reject a primitive that lies on the box boundary.
 void padBox(Box& b);
 
-// Link of an absent Bvh4Node child (a leaf of zero primitives).
-constexpr int32_t kEmptyLink = -1;
-
 // Collapses the BVH2 subtree at `root2` of `bvh2` into four-wide nodes
 // appended to `out` (each node takes up to four descendants, expanding the
 // inner child of largest surface area first); returns the new root's index.
 // Leaf links are kept as they are.
 uint32_t collapseBvh4(const std::vector<BvhNode>& bvh2, uint32_t root2, std::vector<Bvh4Node>& out);
+
+// Quantises every node of a four-wide tree into Bvh4QNode (same indices and
+// links): per node the union of its children's boxes gives the origin, each
+// axis a power-of-two scale with 255 steps covering the extent, and the
+// child bounds are rounded outwards to those steps.
+void quantizeBvh4(const std::vector<Bvh4Node>& in, std::vector<Bvh4QNode>& out);
 
 }  // namespace cg
 

@@ -122,16 +122,19 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
 }
 
 // ---- extend: closest hit --------------------------------------------------------
-// Any hit / closest hit over the four-wide (kWide) or binary trees.
-template <bool kAny, bool kCount, bool kWide>
+// Any hit / closest hit over the trees of node format kNodes (NodeFormat).
+template <bool kAny, bool kCount, int kNodes>
 __device__ __forceinline__ HitRec trace(const SceneView& sc, float4 o, float4 d, float tmax,
                                         TravCounters& cnt, uint32_t* status) {
-  if (kWide) return traceRay4<kAny, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, status);
+  if (kNodes == kNodesWide4Q)
+    return traceRay4<kAny, kCount, true>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, status);
+  if (kNodes == kNodesWide4)
+    return traceRay4<kAny, kCount, false>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, status);
   return traceRay<kAny, kCount>(sc, o.x, o.y, o.z, d.x, d.y, d.z, tmax, cnt, status);
 }
 
 // At most 64 registers per thread (4 blocks of 256 or 8 of 128 per SM).
-template <bool kCount, bool kWide>
+template <bool kCount, int kNodes>
 __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb, int parity) {
   // counts can exceed the capacity after an overflow (the appends are then
   // dropped and the status word set); never read past the queue
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
   for (uint32_t i = tid; i < n; i += stride) {
     const float4 o = wb.ray_o[parity][i];
     const float4 d = wb.ray_d[parity][i];
-    HitRec h = trace<false, kCount, kWide>(sc, o, d, MAXD, cnt, wb.status);
+    HitRec h = trace<false, kCount, kNodes>(sc, o, d, MAXD, cnt, wb.status);
     wb.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
     wb.hit_inst[i] = h.inst;
   }
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow_persistent(SceneView sc, Wave
 }
 
 // ---- shadow: t-bounded any hit (solveEmission, trace.wesl:91-113) ----------------
-template <bool kCount, bool kWide>
+template <bool kCount, int kNodes>
 __global__ void __launch_bounds__(256, 4) k_shadow(SceneView sc, WaveBuffers wb) {
   const uint32_t n = min(wb.counts[2], wb.capacity);
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(SceneView sc, WaveBuffers wb)
     const float4 d = wb.sh_d[i];
     // occluded iff the closest hit (< 1e6) is nearer than expected - 1e-3
     const float tmax = fminf(d.w, MAXD);
-    HitRec h = trace<true, kCount, kWide>(sc, o, d, tmax, cnt, wb.status);
+    HitRec h = trace<true, kCount, kNodes>(sc, o, d, tmax, cnt, wb.status);
     if (h.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[i]], o.w);
   }
   if (kCount) {
@@ -681,14 +684,14 @@ __global__ void k_resolve(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
 }
 
 // ---- closest-hit query for parity tests -------------------------------------------
-template <bool kWide>
+template <int kNodes>
 __global__ void k_trace_closest(SceneView sc, const float4* rays, uint32_t n, float4* out_tuv,
                                 int4* out_ids, uint32_t* status) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 o = rays[2 * i], d = rays[2 * i + 1];
   TravCounters cnt{0u, 0u, 0u};
-  HitRec h = trace<false, false, kWide>(sc, o, d, MAXD, cnt, status);
+  HitRec h = trace<false, false, kNodes>(sc, o, d, MAXD, cnt, status);
   if (h.inst >= 0) {
     const uint32_t orig = __float_as_uint(__ldg(sc.tris + 3u * h.tri).w);
     out_tuv[i] = make_float4(h.t, h.u, h.v, 0.0f);
@@ -738,14 +741,14 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
     return;
   }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
-  if (counting && ls.wide)
-    k_extend<true, true><<<grid, block, 0, s>>>(sc, wb, parity);
-  else if (counting)
-    k_extend<true, false><<<grid, block, 0, s>>>(sc, wb, parity);
-  else if (ls.wide)
-    k_extend<false, true><<<grid, block, 0, s>>>(sc, wb, parity);
-  else
-    k_extend<false, false><<<grid, block, 0, s>>>(sc, wb, parity);
+  switch (ls.nodes * 2 + (counting ? 1 : 0)) {
+    case kNodesBinary * 2: k_extend<false, kNodesBinary><<<grid, block, 0, s>>>(sc, wb, parity); break;
+    case kNodesBinary * 2 + 1: k_extend<true, kNodesBinary><<<grid, block, 0, s>>>(sc, wb, parity); break;
+    case kNodesWide4 * 2: k_extend<false, kNodesWide4><<<grid, block, 0, s>>>(sc, wb, parity); break;
+    case kNodesWide4 * 2 + 1: k_extend<true, kNodesWide4><<<grid, block, 0, s>>>(sc, wb, parity); break;
+    case kNodesWide4Q * 2 + 1: k_extend<true, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb, parity); break;
+    default: k_extend<false, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb, parity); break;
+  }
 }
 
 void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
@@ -770,14 +773,14 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
     return;
   }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
-  if (counting && ls.wide)
-    k_shadow<true, true><<<grid, block, 0, s>>>(sc, wb);
-  else if (counting)
-    k_shadow<true, false><<<grid, block, 0, s>>>(sc, wb);
-  else if (ls.wide)
-    k_shadow<false, true><<<grid, block, 0, s>>>(sc, wb);
-  else
-    k_shadow<false, false><<<grid, block, 0, s>>>(sc, wb);
+  switch (ls.nodes * 2 + (counting ? 1 : 0)) {
+    case kNodesBinary * 2: k_shadow<false, kNodesBinary><<<grid, block, 0, s>>>(sc, wb); break;
+    case kNodesBinary * 2 + 1: k_shadow<true, kNodesBinary><<<grid, block, 0, s>>>(sc, wb); break;
+    case kNodesWide4 * 2: k_shadow<false, kNodesWide4><<<grid, block, 0, s>>>(sc, wb); break;
+    case kNodesWide4 * 2 + 1: k_shadow<true, kNodesWide4><<<grid, block, 0, s>>>(sc, wb); break;
+    case kNodesWide4Q * 2 + 1: k_shadow<true, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb); break;
+    default: k_shadow<false, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb); break;
+  }
 }
 
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
@@ -787,12 +790,15 @@ void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc&
 }
 
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
-                        int4* out_ids, uint32_t* status, bool wide, cudaStream_t s) {
+                        int4* out_ids, uint32_t* status, int nodes, cudaStream_t s) {
   if (n == 0) return;
-  if (wide)
-    k_trace_closest<true><<<(n + 127) / 128, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
+  const uint32_t g = (n + 127) / 128;
+  if (nodes == kNodesBinary)
+    k_trace_closest<kNodesBinary><<<g, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
+  else if (nodes == kNodesWide4)
+    k_trace_closest<kNodesWide4><<<g, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
   else
-    k_trace_closest<false><<<(n + 127) / 128, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
+    k_trace_closest<kNodesWide4Q><<<g, 128, 0, s>>>(sc, rays, n, out_tuv, out_ids, status);
 }
 
 }  // namespace cg

@@ -73,12 +73,19 @@ struct ChunkDesc {
   uint32_t pixel_count;
 };
 
+// Node format the traversal walks.
+enum NodeFormat : int {
+  kNodesBinary = 0,  // BvhNode, two children
+  kNodesWide4 = 1,   // Bvh4Node, four children with full-precision boxes
+  kNodesWide4Q = 2,  // Bvh4QNode, four children with 8-bit boxes
+};
+
 struct LaunchShape {
   uint32_t extend_block = 128;
   uint32_t shade_block = 128;
   uint32_t grid_extend = 0;  // 0: derived from the SM count
   uint32_t grid_shade = 0;
-  bool wide = true;          // traverse the four-wide trees
+  int nodes = kNodesWide4;   // NodeFormat of the traversal
   bool persistent = false;   // persistent warps with lane refill (binary trees)
   bool shade_sort = true;    // group a block's rays by shading key before shading
 };
@@ -94,7 +101,7 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
                    cudaStream_t s);
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
-                        int4* out_ids, uint32_t* status, bool wide, cudaStream_t s);
+                        int4* out_ids, uint32_t* status, int nodes, cudaStream_t s);
 
 int smCount();
 

@@ -38,6 +38,48 @@ F3 transformPoint(const float* m, F3 p) {
 
 float luminance(F3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
 
+// A cut of a mesh's BVH2 of at most `target` boxes (the inner node of largest
+// surface area is replaced by its two children first).  Their union contains
+// every triangle, and transformed corner by corner they bound a rotated
+// instance far tighter than the corners of the mesh's single box.
+void bvhCut(const std::vector<BvhNode>& nodes, uint32_t root, size_t target, std::vector<Box>& out) {
+  struct Item {
+    Box box;
+    int32_t link;
+  };
+  auto kids = [&](int32_t n, std::vector<Item>& v) {
+    const BvhNode& b = nodes[static_cast<size_t>(n)];
+    const Item c0{{{b.c0lx, b.c0ly, b.c0lz}, {b.c0hx, b.c0hy, b.c0hz}}, b.child0};
+    const Item c1{{{b.c1lx, b.c1ly, b.c1lz}, {b.c1hx, b.c1hy, b.c1hz}}, b.child1};
+    if (c0.link >= 0 || leafCount(c0.link) != 0) v.push_back(c0);
+    if (c1.link >= 0 || leafCount(c1.link) != 0) v.push_back(c1);
+  };
+  auto area = [](const Box& b) {
+    const float x = b.hi[0] - b.lo[0], y = b.hi[1] - b.lo[1], z = b.hi[2] - b.lo[2];
+    return x * y + y * z + z * x;
+  };
+  std::vector<Item> items;
+  kids(static_cast<int32_t>(root), items);
+  while (items.size() < target) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (size_t k = 0; k < items.size(); ++k) {
+      if (items[k].link < 0) continue;
+      const float a = area(items[k].box);
+      if (a > best_area) {
+        best_area = a;
+        best = static_cast<int>(k);
+      }
+    }
+    if (best < 0) break;
+    const int32_t n = items[best].link;
+    items.erase(items.begin() + best);
+    kids(n, items);
+  }
+  out.clear();
+  for (const Item& it : items) out.push_back(it.box);
+}
+
 }  // namespace
 
 void invertAffine(const float* m, float* out) {
@@ -251,6 +293,9 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
   }
 
   // ---- instances and the TLAS ---------------------------------------------------------
+  std::vector<std::vector<Box>> mesh_cut(d->mesh_count);
+  for (uint32_t m = 0; m < d->mesh_count; ++m)
+    if (mesh_bounds[m].lo[0] <= mesh_bounds[m].hi[0]) bvhCut(s.blas, mesh_root[m], 64, mesh_cut[m]);
   std::vector<Box> inst_boxes(d->instance_count);
   for (uint32_t i = 0; i < d->instance_count; ++i) {
     const cg_instance& ci = d->instances[i];
@@ -261,7 +306,8 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
     di.tri_base = mesh_tri_base[ci.mesh];
     di.blas4_root = mesh_root4[ci.mesh];
     s.inst.push_back(di);
-    // world box of the mesh box's 8 corners (double, then widened)
+    // world box: the corners of the mesh's BVH cut boxes, transformed in
+    // double and widened by one float step
     const Box& mb = mesh_bounds[ci.mesh];
     Box wb;
     for (int a = 0; a < 3; ++a) {
@@ -269,14 +315,17 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
       wb.hi[a] = -std::numeric_limits<float>::infinity();
     }
     if (mb.lo[0] <= mb.hi[0]) {
-      for (int c = 0; c < 8; ++c) {
-        double p[3] = {(c & 1) ? mb.hi[0] : mb.lo[0], (c & 2) ? mb.hi[1] : mb.lo[1],
-                       (c & 4) ? mb.hi[2] : mb.lo[2]};
-        for (int a = 0; a < 3; ++a) {
-          const float* r = ci.world_from_local + 4 * a;
-          double w = double(r[0]) * p[0] + double(r[1]) * p[1] + double(r[2]) * p[2] + double(r[3]);
-          wb.lo[a] = std::min(wb.lo[a], std::nextafter(static_cast<float>(w), -INFINITY));
-          wb.hi[a] = std::max(wb.hi[a], std::nextafter(static_cast<float>(w), INFINITY));
+      for (const Box& cb : mesh_cut[ci.mesh]) {
+        for (int c = 0; c < 8; ++c) {
+          double p[3] = {(c & 1) ? cb.hi[0] : cb.lo[0], (c & 2) ? cb.hi[1] : cb.lo[1],
+                         (c & 4) ? cb.hi[2] : cb.lo[2]};
+          for (int a = 0; a < 3; ++a) {
+            const float* r = ci.world_from_local + 4 * a;
+            double w =
+                double(r[0]) * p[0] + double(r[1]) * p[1] + double(r[2]) * p[2] + double(r[3]);
+            wb.lo[a] = std::min(wb.lo[a], std::nextafter(static_cast<float>(w), -INFINITY));
+            wb.hi[a] = std::max(wb.hi[a], std::nextafter(static_cast<float>(w), INFINITY));
+          }
         }
       }
     } else {
@@ -301,6 +350,8 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
     }
     collapseBvh4(s.tlas, 0, s.tlas4);  // root 0
   }
+  quantizeBvh4(s.tlas4, s.tlas4q);
+  quantizeBvh4(s.blas4, s.blas4q);
 
   // ---- emissive buffer (emissive_buffer.h:44-100) --------------------------------------
   for (uint32_t p = 0; p < d->instance_count; ++p) {

@@ -18,6 +18,7 @@ namespace cg {
 struct HostScene {
   std::vector<BvhNode> tlas, blas, light_bvh;
   std::vector<Bvh4Node> tlas4, blas4;  // the TLAS and BLAS collapsed four-wide
+  std::vector<Bvh4QNode> tlas4q, blas4q;  // the same, child boxes quantised to 8 bits
   std::vector<float> tris;          // 12 floats per triangle (3 x float4)
   std::vector<uint32_t> tri_vidx;   // 4 per triangle
   std::vector<float> vnormal;       // 4 per vertex

@@ -335,15 +335,88 @@ __device__ __forceinline__ void cswap(float& ka, int32_t& la, float& kb, int32_t
 // boxes (six independent 128-bit slab loads), the hit children are ordered
 // by entry distance, the nearest is visited next and the others pushed.
 // Triangle and instance handling is that of traceRay (bit-identical hits).
-template <bool kAny, bool kCount>
+// Byte c of w as a float (exact): the byte under the exponent of 2^23, minus 2^23.
+__device__ __forceinline__ float byteToFloat(uint32_t w, uint32_t c) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | c)) - 8388608.0f;
+}
+
+// The two four-wide node formats: full-precision child slabs, or 8-bit
+// offsets from the node origin (decoded to world-space bounds that contain
+// the full-precision ones: fmaf rounds q * scale + origin to nearest, and the
+// exact value is already outside the child's box).  fetch() returns, per
+// axis, the near and far bound of each child for a ray whose inverse
+// direction has the given signs (near = lo where the inverse direction is
+// >= 0): the slab distances then need no min/max per axis.  With FMA rounding
+// monotonic in the bound, near <= far along the ray, so the entry and exit
+// distances equal min/max of the two slab planes bit for bit.
+template <bool kQuant>
+struct Wide;
+
+template <>
+struct Wide<false> {
+  using Node = Bvh4Node;
+  static __device__ __forceinline__ const Node* tlas(const SceneView& sc) { return sc.tlas4; }
+  static __device__ __forceinline__ const Node* blas(const SceneView& sc) { return sc.blas4; }
+  static __device__ __forceinline__ int4 fetch(const Node* n, bool negx, bool negy, bool negz,
+                                               float nx[4], float fx[4], float ny[4], float fy[4],
+                                               float nz[4], float fz[4]) {
+    const float4* np = reinterpret_cast<const float4*>(n);
+    // float4 rows: lo.x, hi.x, lo.y, hi.y, lo.z, hi.z
+    const float4 a = __ldg(np + (negx ? 1 : 0)), b = __ldg(np + (negx ? 0 : 1));
+    const float4 c = __ldg(np + (negy ? 3 : 2)), d = __ldg(np + (negy ? 2 : 3));
+    const float4 e = __ldg(np + (negz ? 5 : 4)), f = __ldg(np + (negz ? 4 : 5));
+    nx[0] = a.x; nx[1] = a.y; nx[2] = a.z; nx[3] = a.w;
+    fx[0] = b.x; fx[1] = b.y; fx[2] = b.z; fx[3] = b.w;
+    ny[0] = c.x; ny[1] = c.y; ny[2] = c.z; ny[3] = c.w;
+    fy[0] = d.x; fy[1] = d.y; fy[2] = d.z; fy[3] = d.w;
+    nz[0] = e.x; nz[1] = e.y; nz[2] = e.z; nz[3] = e.w;
+    fz[0] = f.x; fz[1] = f.y; fz[2] = f.z; fz[3] = f.w;
+    return __ldg(reinterpret_cast<const int4*>(np + 6));
+  }
+};
+
+template <>
+struct Wide<true> {
+  using Node = Bvh4QNode;
+  static __device__ __forceinline__ const Node* tlas(const SceneView& sc) { return sc.tlas4q; }
+  static __device__ __forceinline__ const Node* blas(const SceneView& sc) { return sc.blas4q; }
+  static __device__ __forceinline__ int4 fetch(const Node* n, bool negx, bool negy, bool negz,
+                                               float nx[4], float fx[4], float ny[4], float fy[4],
+                                               float nz[4], float fz[4]) {
+    const float4* np = reinterpret_cast<const float4*>(n);
+    const float4 h = __ldg(np);
+    const uint4 qa = __ldg(reinterpret_cast<const uint4*>(np + 1));  // lo.x hi.x lo.y hi.y
+    const uint4 qb = __ldg(reinterpret_cast<const uint4*>(np + 2));  // lo.z hi.z
+    const uint32_t sb = __float_as_uint(h.w);
+    const float sx = __uint_as_float((sb & 0xffu) << 23);
+    const float sy = __uint_as_float(((sb >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((sb >> 16) & 0xffu) << 23);
+    const uint32_t wnx = negx ? qa.y : qa.x, wfx = negx ? qa.x : qa.y;
+    const uint32_t wny = negy ? qa.w : qa.z, wfy = negy ? qa.z : qa.w;
+    const uint32_t wnz = negz ? qb.y : qb.x, wfz = negz ? qb.x : qb.y;
+#pragma unroll
+    for (uint32_t c = 0; c < 4; ++c) {
+      nx[c] = fmaf(byteToFloat(wnx, c), sx, h.x);
+      fx[c] = fmaf(byteToFloat(wfx, c), sx, h.x);
+      ny[c] = fmaf(byteToFloat(wny, c), sy, h.y);
+      fy[c] = fmaf(byteToFloat(wfy, c), sy, h.y);
+      nz[c] = fmaf(byteToFloat(wnz, c), sz, h.z);
+      fz[c] = fmaf(byteToFloat(wfz, c), sz, h.z);
+    }
+    return __ldg(reinterpret_cast<const int4*>(np + 3));
+  }
+};
+
+template <bool kAny, bool kCount, bool kQuant = false>
 __device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, float woy, float woz,
                                             float wdx, float wdy, float wdz, float tmax,
                                             TravCounters& cnt, uint32_t* status) {
+  using W = Wide<kQuant>;
   HitRec best{tmax, 0.0f, 0.0f, -1, 0u};
   if (!sc.has_tlas) return best;
   int32_t stack[kStackSize];
   int sp = 0;
-  const Bvh4Node* nodes = sc.tlas4;
+  const typename W::Node* nodes = W::tlas(sc);
   bool in_blas = false;
   int32_t cur_inst = -1;
   float ox = wox, oy = woy, oz = woz, dx = wdx, dy = wdy, dz = wdz;
@@ -352,23 +425,22 @@ __device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, floa
   int32_t node = 0;
   while (true) {
     while (node >= 0) {
-      const float4* np = reinterpret_cast<const float4*>(nodes + node);
-      const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
-      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
-      const int4 ch = __ldg(reinterpret_cast<const int4*>(np + 6));
+      float nxs[4], fxs[4], nys[4], fys[4], nzs[4], fzs[4];
+      const int4 ch = W::fetch(nodes + node, idx < 0.0f, idy < 0.0f, idz < 0.0f, nxs, fxs, nys, fys,
+                               nzs, fzs);
       if (kCount) ++cnt.nodes;
       float k[4];
-      const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, hxs[4] = {hx.x, hx.y, hx.z, hx.w};
-      const float lys[4] = {ly.x, ly.y, ly.z, ly.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w};
-      const float lzs[4] = {lz.x, lz.y, lz.z, lz.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
+      const int32_t links[4] = {ch.x, ch.y, ch.z, ch.w};
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        const float a0 = fmaf(lxs[c], idx, -oix), a1 = fmaf(hxs[c], idx, -oix);
-        const float b0 = fmaf(lys[c], idy, -oiy), b1 = fmaf(hys[c], idy, -oiy);
-        const float c0 = fmaf(lzs[c], idz, -oiz), c1 = fmaf(hzs[c], idz, -oiz);
-        const float tmin = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
-        const float tmx = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), best.t));
-        k[c] = tmin <= tmx ? tmin : INFINITY;
+        const float a0 = fmaf(nxs[c], idx, -oix), a1 = fmaf(fxs[c], idx, -oix);
+        const float b0 = fmaf(nys[c], idy, -oiy), b1 = fmaf(fys[c], idy, -oiy);
+        const float c0 = fmaf(nzs[c], idz, -oiz), c1 = fmaf(fzs[c], idz, -oiz);
+        const float tmin = fmaxf(fmaxf(a0, b0), fmaxf(c0, 0.0f));
+        const float tmx = fminf(fminf(a1, b1), fminf(c1, best.t));
+        // absent children: a point box at 1e30 (full precision) or the link (quantised)
+        const bool hit = kQuant ? (tmin <= tmx && links[c] != kEmptyLink) : tmin <= tmx;
+        k[c] = hit ? tmin : INFINITY;
       }
       int32_t l0 = ch.x, l1 = ch.y, l2 = ch.z, l3 = ch.w;
       float k0 = k[0], k1 = k[1], k2 = k[2], k3 = k[3];
@@ -394,7 +466,7 @@ __device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, floa
     }
     if (node == kDone) break;
     if (node == kToTlas) {
-      nodes = sc.tlas4;
+      nodes = W::tlas(sc);
       in_blas = false;
       ox = wox; oy = woy; oz = woz;
       dx = wdx; dy = wdy; dz = wdz;
@@ -423,7 +495,7 @@ __device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, floa
         return HitRec{tmax, 0.0f, 0.0f, -1, 0u};
       }
       stack[sp++] = kToTlas;
-      nodes = sc.blas4;
+      nodes = W::blas(sc);
       in_blas = true;
       cur_inst = static_cast<int32_t>(first);
       node = static_cast<int32_t>(meta.w);  // blas4_root

@@ -35,6 +35,9 @@ struct alignas(16) BvhNode {
 };
 static_assert(sizeof(BvhNode) == 64, "BvhNode is 64 bytes");
 
+// Link of an absent four-wide child (a leaf of zero primitives).
+constexpr int32_t kEmptyLink = -1;
+
 // Four-wide node: the slabs of four children, structure-of-arrays so each
 // axis bound is one 128-bit load; links as in BvhNode (leaf count in the low
 // 3 bits of ~link).  An absent child has link kEmptyLink and a point box at
@@ -46,6 +49,22 @@ struct alignas(16) Bvh4Node {
   uint32_t _pad[4];
 };
 static_assert(sizeof(Bvh4Node) == 128, "Bvh4Node is 128 bytes");
+
+// Compressed four-wide node (64 B, four 128-bit loads per visit instead of
+// eight): the node's box origin, one power-of-two scale per axis, and the
+// four child boxes as 8-bit offsets in units of that scale, rounded outwards
+// (child lo = origin + qlo * scale <= the child's box, hi likewise >=), so a
+// quantised box always contains the full-precision one.  Same indices and
+// links as the Bvh4Node array it is built from; an absent child
+// (kEmptyLink) is skipped by its link, not by its box.
+struct alignas(16) Bvh4QNode {
+  float ox, oy, oz;
+  uint32_t scale_bits;    // biased float exponents of the x, y, z scales (bytes 0..2)
+  uint32_t qlox, qhix, qloy, qhiy;  // byte c = child c
+  uint32_t qloz, qhiz, _pad0, _pad1;
+  int32_t child[4];
+};
+static_assert(sizeof(Bvh4QNode) == 64, "Bvh4QNode is 64 bytes");
 
 struct alignas(16) DevInstance {
   float inv[12];        // row-major world -> local (3x4)
@@ -112,6 +131,8 @@ struct SceneView {
   const BvhNode* blas;         // all BLAS nodes
   const Bvh4Node* tlas4;       // the same trees, four-wide (root 0)
   const Bvh4Node* blas4;
+  const Bvh4QNode* tlas4q;     // the four-wide trees with 8-bit child boxes
+  const Bvh4QNode* blas4q;
   const float4* tris;          // 3 float4 per triangle: (v0, orig id bits) (e1) (e2)
   const uint4* tri_vidx;       // vertex indices per triangle (i0, i1, i2, _)
   const float4* vnormal;       // vertex normals

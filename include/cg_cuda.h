@@ -310,7 +310,8 @@ typedef struct cg_tuning {
                            (binary trees), 0 = one ray per thread */
   uint32_t shade_sort;  /* 1 (default) = group rays by material kind before
                            shading, 2 = do not, 0 = keep */
-  uint32_t _pad;
+  uint32_t box_bits;    /* four-wide child boxes: 32 (default) = floats in
+                           128-byte nodes, 8 = 8-bit offsets in 64-byte nodes */
 } cg_tuning;
 CG_API int cg_set_tuning(const cg_tuning* tuning);
 CG_API int cg_get_tuning(cg_tuning* out);

@@ -167,7 +167,8 @@ def test_server_cancel_and_timeout(cornell):
 @pytest.mark.parametrize("variant", [dict(bvh_width=2, persistent=False),
                                      dict(bvh_width=2, persistent=True),
                                      dict(bvh_width=4, persistent=False),
-                                     dict(bvh_width=4, persistent=False, shade_sort=False)])
+                                     dict(bvh_width=4, persistent=False, shade_sort=False),
+                                     dict(bvh_width=4, persistent=False, box_bits=8)])
 def test_traversal_variants_render_the_same_samples(variant):
     """Binary or four-wide trees, one ray per thread or persistent warps, rays
     grouped by material before shading or not: the closest hits and the keyed
@@ -176,7 +177,7 @@ def test_traversal_variants_render_the_same_samples(variant):
     B.EnvInit(B.PathTraceConf(render_width=96, render_height=54, sample_count=4, trace_depth=8))
     g = B.LoadScene(s)
     cam = B.Camera.from_c(s.camera)
-    B.SetTuning(bvh_width=4, persistent=False, shade_sort=True)
+    B.SetTuning(bvh_width=4, persistent=False, shade_sort=True, box_bits=32)
     B.View(g, cam)
     ref = B.ReadFilm()
     B.EnvInit(B.PathTraceConf(render_width=96, render_height=54, sample_count=4, trace_depth=8))

@@ -35,16 +35,18 @@ SCENES = {
 }
 
 
-@pytest.mark.parametrize("width", [4, 2])
+@pytest.mark.parametrize("nodes", [(4, 8), (4, 32), (2, 8)], ids=["wide4q", "wide4", "binary"])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_closest_hits_bit_exact(name, width):
+def test_closest_hits_bit_exact(name, nodes):
+    """Every node format (four-wide with 8-bit or float child boxes, binary)
+    finds the oracle's closest hit to the bit."""
     s = SCENES[name]()
     g = B.LoadScene(s)
     o = O.OracleScene(s)
     rays = ray_set(s, 20000, seed=11)
-    B.SetTuning(bvh_width=width)
+    B.SetTuning(bvh_width=nodes[0], box_bits=nodes[1])
     gh = B.trace_closest(g, rays)
-    B.SetTuning(bvh_width=4)
+    B.SetTuning(bvh_width=4, box_bits=32)
     oh, t2 = o.trace_closest(rays)
     # exclude ulp-level ties: the second-best hit within 1 ulp of the best
     tie = (oh["instance"] >= 0) & (np.abs(t2 - oh["t"]) <= np.spacing(oh["t"]))
