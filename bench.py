@@ -270,7 +270,7 @@ def _rel_diff(a, b):
 def _tuning_kwargs(t):
     return dict(queue_capacity=int(t.queue_capacity), extend_block=int(t.extend_block),
                 shade_block=int(t.shade_block), use_graph=int(t.use_graph),
-                bvh_width=int(t.bvh_width), persistent=bool(t.persistent),
+                bvh_width=int(t.bvh_width), persistent=int(t.persistent) != 2,
                 shade_sort=int(t.shade_sort) != 2)
 
 
@@ -299,9 +299,8 @@ def batched_form(B, torch):
     B.EnvInit(B.PathTraceConf(render_width=1920, render_height=1080, sample_count=64,
                               trace_depth=BATCH_DEPTH))
     g = B.LoadScene(s)
-    p0, d0 = views[0][0], views[0][1]
     t_tune = time.perf_counter()
-    best = B.autotune(g, (p0, d0, 512, 512, 4, 0))
+    best = B.autotune_views(g, views[::32])   # 8 probe views of the batch
     t_tune = time.perf_counter() - t_tune
     tuning = _tuning_kwargs(best)
     samples = sum(w * h * spp for _, _, w, h, spp, _ in views)
@@ -431,6 +430,19 @@ def run_ours(args):
     t_load = time.perf_counter()
     g = B.LoadScene(scene)
     t_load = time.perf_counter() - t_load
+    info = g.info()
+    load = {"seconds": t_load, "bvh_build_seconds": info.bvh_build_seconds,
+            "bvh_device_builds": int(info.bvh_device_builds),
+            "bvh_host_builds": int(info.bvh_host_builds)}
+    if rank == 0 and ws == 1:
+        # the same load with every tree built on the host, for comparison
+        B.SetBvhBuild(_abi.CG_BVH_BUILD_HOST)
+        t_h = time.perf_counter()
+        gh = B.LoadScene(scene)
+        load["host_build_seconds"] = time.perf_counter() - t_h
+        load["host_bvh_build_seconds"] = gh.info().bvh_build_seconds
+        gh.close()
+        B.SetBvhBuild(_abi.CG_BVH_BUILD_AUTO)
     cam = B.Camera.from_c(scene.camera)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     samples_per_step = W_ * H_ * SPP_
@@ -563,7 +575,7 @@ def run_ours(args):
                                            "tri_tests": int(cst.tri_tests),
                                            "inst_visits": int(cst.inst_visits)},
             "wall_ms_per_step": wall / args.steps * 1e3,
-            "load_scene_s": t_load,
+            "load_scene": load,
             "clocks": clocks.summary(),
         }
         if cpu:

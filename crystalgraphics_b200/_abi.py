@@ -62,6 +62,8 @@ class CgSceneInfo(C.Structure):
         ("material_count", u32), ("emissive_count", u32),
         ("blas_node_count", u32), ("tlas_node_count", u32), ("light_node_count", u32),
         ("device_bytes", C.c_uint64), ("tag", C.c_uint64),
+        ("bvh_build_seconds", C.c_double), ("bvh_host_builds", u32),
+        ("bvh_device_builds", u32),
     ]
 
 
@@ -152,3 +154,5 @@ def make_camera(position, direction, viewport):
     cam.direction[:] = [float(x) for x in direction]
     cam.viewport[:] = [float(x) for x in viewport]
     return cam
+
+CG_BVH_BUILD_AUTO, CG_BVH_BUILD_HOST, CG_BVH_BUILD_DEVICE = 0, 1, 2

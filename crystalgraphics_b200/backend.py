@@ -72,6 +72,9 @@ def _load():
         "cg_set_tuning": (i, [C.POINTER(_abi.CgTuning)]),
         "cg_get_tuning": (i, [C.POINTER(_abi.CgTuning)]),
         "cg_autotune": (i, [vp, C.POINTER(_abi.CgViewDesc), C.POINTER(_abi.CgTuning)]),
+        "cg_autotune_views": (i, [vp, vp, u32, C.POINTER(_abi.CgTuning)]),
+        "cg_set_bvh_build": (i, [i]),
+        "cg_bvh_build": (i, [vp, u32, i, vp, u32, C.POINTER(u32), vp]),
         "cg_server_create": (i, [vp, u32, C.c_uint64, C.POINTER(vp)]),
         "cg_server_destroy": (i, [vp]),
         "cg_server_submit": (i, [vp, C.POINTER(_abi.CgRequest), vp, C.POINTER(C.c_uint64)]),
@@ -302,14 +305,30 @@ def SetSeed(seed: int) -> None:
 def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_width=0,
               persistent=None, shade_sort=None, box_bits=0) -> None:
     """0 (or None for the two switches) keeps the current value."""
-    if persistent is None:
-        cur = _abi.CgTuning()
-        _check(lib.cg_get_tuning(C.byref(cur)))
-        persistent = cur.persistent
     sort = 0 if shade_sort is None else (1 if shade_sort else 2)
     t = _abi.CgTuning(queue_capacity, extend_block, shade_block, use_graph, bvh_width,
-                      1 if persistent else 0, sort, box_bits)
+                      0 if persistent is None else (1 if persistent else 2), sort, box_bits)
     _check(lib.cg_set_tuning(C.byref(t)))
+
+
+def SetBvhBuild(mode: int) -> None:
+    """Where LoadScene builds BVHs: _abi.CG_BVH_BUILD_AUTO (GPU for large trees),
+    CG_BVH_BUILD_HOST or CG_BVH_BUILD_DEVICE."""
+    _check(lib.cg_set_bvh_build(mode))
+
+
+def bvh_build(boxes: np.ndarray, mode: int):
+    """One BVH over (n, 6) float32 boxes built on the host (1) or the GPU (2):
+    returns (nodes as (m, 16) uint32 words of the 64-byte records, order)."""
+    boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    n = boxes.shape[0]
+    order = np.empty(n, np.uint32)
+    cnt = C.c_uint32()
+    _check(lib.cg_bvh_build(boxes.ctypes.data, n, mode, None, 0, C.byref(cnt), order.ctypes.data))
+    nodes = np.empty((cnt.value, 16), np.uint32)
+    _check(lib.cg_bvh_build(boxes.ctypes.data, n, mode, nodes.ctypes.data, cnt.value, C.byref(cnt),
+                            order.ctypes.data))
+    return nodes, order
 
 
 def GetTuning() -> _abi.CgTuning:
@@ -370,6 +389,14 @@ def autotune(scene: Scene, view) -> _abi.CgTuning:
     arr = make_views([view])
     best = _abi.CgTuning()
     _check(lib.cg_autotune(scene.handle, C.byref(arr[0]), C.byref(best)))
+    return best
+
+
+def autotune_views(scene: Scene, views) -> _abi.CgTuning:
+    """The autotuner timed on several probe views (e.g. a sample of a batch)."""
+    arr = views if isinstance(views, C.Array) else make_views(views)
+    best = _abi.CgTuning()
+    _check(lib.cg_autotune_views(scene.handle, arr, len(arr), C.byref(best)))
     return best
 
 

@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -17,6 +18,7 @@
 
 #include "../../include/cg_cuda.h"
 #include "cg_api_internal.h"
+#include "cg_bvh.h"
 #include "cg_kernels.h"
 #include "cg_scene.h"
 
@@ -287,7 +289,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.extend_block = tuning.extend_block;
   ls.shade_block = tuning.shade_block;
   ls.nodes = nodeFormatOf(tuning);
-  ls.persistent = tuning.persistent != 0u;
+  ls.persistent = tuning.persistent != 2u;
   ls.shade_sort = tuning.shade_sort != 2u;
   profBegin(CG_K_GEN, s);
   launchGen(fc, wave, ch, s);
@@ -524,8 +526,19 @@ CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
   *out = nullptr;
   auto sd = std::make_unique<SceneDev>();
   std::string err;
-  int rc = packScene(desc, sd->host, err);
+  int rc = CG_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (g_env) cudaSetDevice(g_env->device);  // device BVH builds run there too
+  }
+  resetBvhBuildStats();
+  try {
+    rc = packScene(desc, sd->host, err);
+  } catch (const std::exception& e) {
+    return fail(CG_E_CUDA, std::string("scene build: ") + e.what());
+  }
   if (rc != CG_OK) return fail(rc, err);
+  const BvhBuildStats bstats = bvhBuildStats();
   if (sd->host.blas_depth + sd->host.tlas_depth + 2 > 64)
     return fail(CG_E_INVALID, "BVH too deep for the 64-entry traversal stack");
   int ndev = 0;
@@ -552,6 +565,9 @@ CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
   in.light_node_count = static_cast<uint32_t>(sd->host.light_bvh.size());
   in.device_bytes = sd->arena.size;
   in.tag = sd->tag;
+  in.bvh_build_seconds = bstats.seconds;
+  in.bvh_host_builds = bstats.host_builds;
+  in.bvh_device_builds = bstats.device_builds;
   // the device holds the geometry now
   HostScene& h = sd->host;
   std::vector<BvhNode>().swap(h.blas);
@@ -561,6 +577,38 @@ CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
   std::vector<uint32_t>().swap(h.tri_vidx);
   std::vector<float>().swap(h.vnormal);
   *out = reinterpret_cast<cg_scene_t>(sd.release());
+  return CG_OK;
+}
+
+CG_API int cg_bvh_build(const float* boxes, uint32_t count, int mode, void* nodes_out,
+                        uint32_t node_capacity, uint32_t* node_count, uint32_t* order_out) {
+  if (!boxes || !node_count || (count && !order_out))
+    return fail(CG_E_INVALID, "null argument");
+  if (mode != kBuildHost && mode != kBuildDevice) return fail(CG_E_INVALID, "mode must be host or device");
+  std::vector<Box> bx(count);
+  std::memcpy(bx.data(), boxes, sizeof(Box) * size_t(count));
+  std::vector<BvhNode> nodes;
+  std::vector<uint32_t> order;
+  const int saved = bvhBuildMode();
+  setBvhBuildMode(mode);
+  try {
+    BvhBuildOptions opt;
+    buildBvh(bx, opt, 0, nodes, order);
+  } catch (const std::exception& e) {
+    setBvhBuildMode(saved);
+    return fail(CG_E_CUDA, std::string("bvh build: ") + e.what());
+  }
+  setBvhBuildMode(saved);
+  *node_count = static_cast<uint32_t>(nodes.size());
+  if (nodes_out && node_capacity >= nodes.size())
+    std::memcpy(nodes_out, nodes.data(), sizeof(BvhNode) * nodes.size());
+  if (count) std::memcpy(order_out, order.data(), 4 * size_t(count));
+  return CG_OK;
+}
+
+CG_API int cg_set_bvh_build(int mode) {
+  if (mode < kBuildAuto || mode > kBuildDevice) return fail(CG_E_INVALID, "unknown BVH build mode");
+  setBvhBuildMode(mode);
   return CG_OK;
 }
 
@@ -766,7 +814,7 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
   if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
   if (t->bvh_width) g_env->tuning.bvh_width = t->bvh_width;
-  g_env->tuning.persistent = t->persistent ? 1u : 0u;
+  if (t->persistent) g_env->tuning.persistent = t->persistent == 2u ? 2u : 1u;
   if (t->shade_sort) g_env->tuning.shade_sort = t->shade_sort == 2u ? 2u : 1u;
   g_env->tuning.use_graph = t->use_graph;
   g_env->dropAllGraphs();

@@ -86,7 +86,7 @@ struct Renderer {
   float* wl_tree = nullptr;
   float* wl_const = nullptr;
   bool counting = false;
-  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, 0u, 1u, 32u};
+  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
 

@@ -201,50 +201,80 @@ CG_API int cg_batch_render(cg_scene_t scene, const cg_view_desc* views, uint32_t
   return CG_OK;
 }
 
-CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* best) {
-  if (!scene || !view) return fail(CG_E_INVALID, "null argument");
+CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32_t count,
+                             cg_tuning* best) {
+  if (!scene || !views || count == 0) return fail(CG_E_INVALID, "null argument or no views");
   std::lock_guard<std::mutex> lk(g_env_mu);
   if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
   Env& env = *g_env;
   SceneDev* s = reinterpret_cast<SceneDev*>(scene);
   CG_CUDA(cudaSetDevice(env.device));
   const cg_tuning saved = env.tuning;
-  const uint32_t caps_q[] = {8u << 20, 16u << 20};
-  const uint32_t blocks[] = {128u, 256u};
-  // kernel variants: (node width, persistent lane refill, shade sort 1 on / 2 off,
-  // bits per child box bound)
-  const uint32_t variants[][4] = {
-      {4u, 0u, 1u, 8u}, {4u, 0u, 1u, 32u}, {4u, 0u, 2u, 8u}, {2u, 0u, 1u, 8u}, {2u, 1u, 1u, 8u}};
+  // Time of the probe views under tuning t: one untimed run, then two timed
+  // (un-captured, so every launch shape change takes effect); +inf if a run fails.
+  auto measure = [&](const cg_tuning& t) {
+    env.tuning = t;
+    env.tuning.use_graph = 0;
+    env.dropAllGraphs();
+    float total = 0.0f;
+    for (int rep = 0; rep < 3; ++rep) {
+      BatchGraph* g = nullptr;
+      RenderRecord rec;
+      float ms = 0.0f;
+      if (runBatch(env, *s, views, count, g, rec, ms) != CG_OK) return 1e30f;
+      if (rep > 0) total += ms;
+    }
+    return total;
+  };
+  // Coordinate descent from the current tuning: kernel variant, then queue
+  // capacity, then the traversal and shading block sizes.
   cg_tuning winner = saved;
-  float best_ms = 1e30f;
-  for (uint32_t q : caps_q) {
-    for (uint32_t eb : blocks) {
-      for (uint32_t sb : blocks) {
-       for (const auto& var : variants) {
-        env.tuning.queue_capacity = q;
-        env.tuning.extend_block = eb;
-        env.tuning.shade_block = sb;
-        env.tuning.bvh_width = var[0];
-        env.tuning.persistent = var[1];
-        env.tuning.shade_sort = var[2];
-        env.tuning.box_bits = var[3];
-        env.tuning.use_graph = 0;
-        env.dropAllGraphs();
-        float t = 0.0f;
-        bool ok = true;
-        for (int rep = 0; rep < 3 && ok; ++rep) {
-          BatchGraph* g = nullptr;
-          RenderRecord rec;
-          float ms = 0.0f;
-          if (runBatch(env, *s, view, 1, g, rec, ms) != CG_OK) ok = false;
-          if (rep > 0) t += ms;  // first run warms up
-        }
-        if (ok && t < best_ms) {
-          best_ms = t;
-          winner = env.tuning;
-        }
-       }
-      }
+  float best_ms = measure(winner);
+  auto consider = [&](cg_tuning t) {
+    const float ms = measure(t);
+    if (ms < best_ms) {
+      best_ms = ms;
+      winner = t;
+    }
+  };
+  // kernel variants: (node width, persistent lane refill 1 on / 2 off, shade sort
+  // 1 on / 2 off, bits per child box bound)
+  const uint32_t variants[][4] = {
+      {4u, 1u, 1u, 32u}, {4u, 2u, 1u, 32u}, {4u, 1u, 1u, 8u},
+      {4u, 1u, 2u, 32u}, {2u, 1u, 1u, 32u}, {2u, 2u, 1u, 32u}};
+  {
+    const cg_tuning base = winner;
+    for (const auto& var : variants) {
+      cg_tuning t = base;
+      t.bvh_width = var[0];
+      t.persistent = var[1];
+      t.shade_sort = var[2];
+      t.box_bits = var[3];
+      consider(t);
+    }
+  }
+  {
+    const cg_tuning base = winner;
+    for (uint32_t q : {8u << 20, 16u << 20, 32u << 20}) {
+      cg_tuning t = base;
+      t.queue_capacity = q;
+      consider(t);
+    }
+  }
+  {
+    const cg_tuning base = winner;
+    for (uint32_t b : {64u, 128u, 256u}) {
+      cg_tuning t = base;
+      t.extend_block = b;
+      consider(t);
+    }
+  }
+  {
+    const cg_tuning base = winner;
+    for (uint32_t b : {64u, 128u, 256u}) {
+      cg_tuning t = base;
+      t.shade_block = b;
+      consider(t);
     }
   }
   env.dropAllGraphs();
@@ -258,6 +288,10 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* be
   if (best) *best = winner;
   if (best_ms >= 1e30f) return fail(CG_E_CUDA, "autotune: no configuration ran");
   return CG_OK;
+}
+
+CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* best) {
+  return cg_autotune_views(scene, view, view ? 1u : 0u, best);
 }
 
 }  // extern "C"

@@ -1,14 +1,20 @@
 // cg_bvh.cpp — binned-SAH BVH builder for the device BvhNode layout.
 #include "cg_bvh.h"
 
+#include <cuda_runtime.h>
+
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <limits>
+#include <stdexcept>
 
 namespace cg {
 namespace {
 
 constexpr float kInf = std::numeric_limits<float>::infinity();
+constexpr uint32_t kMaxBins = 64;
 
 inline void boxReset(Box& b) {
   for (int a = 0; a < 3; ++a) {
@@ -34,11 +40,7 @@ inline float boxArea(const Box& b) {
   return 2.0f * (dx * dy + dy * dz + dz * dx);
 }
 
-struct TmpNode {
-  Box box;
-  int32_t left = -1, right = -1;  // TmpNode indices (inner)
-  uint32_t first = 0, count = 0;  // leaf range in order[]
-};
+using TmpNode = BvhTmpNode;
 
 struct Builder {
   const std::vector<Box>& boxes;
@@ -60,14 +62,14 @@ struct Builder {
     Box cb;
     boxReset(cb);
     for (uint32_t i = begin; i < end; ++i) boxGrowPt(cb, &centers[3 * order[i]]);
-    const uint32_t B = opt.bins;
+    const uint32_t B = std::min<uint32_t>(std::max<uint32_t>(opt.bins, 2u), kMaxBins);
     float best_cost = kInf;
     int best_axis = -1;
     uint32_t best_bin = 0;
-    std::vector<Box> bin_box(B);
-    std::vector<uint32_t> bin_cnt(B);
-    std::vector<float> right_area(B);
-    std::vector<uint32_t> right_cnt(B);
+    Box bin_box[kMaxBins];
+    uint32_t bin_cnt[kMaxBins];
+    float right_area[kMaxBins];
+    uint32_t right_cnt[kMaxBins];
     for (int a = 0; a < 3; ++a) {
       float ext = cb.hi[a] - cb.lo[a];
       if (!(ext > 0.0f)) continue;
@@ -119,7 +121,7 @@ struct Builder {
     }
     if (n <= opt.max_leaf && leaf_cost <= split_cost) return end;
     const int a = best_axis;
-    const float scale = static_cast<float>(B) / (cb.hi[a] - cb.lo[a]);
+    const float scale = static_cast<float>(B) / (cb.hi[a] - cb.lo[a]);  // as when binning
     auto mid = std::partition(order.begin() + begin, order.begin() + end, [&](uint32_t p) {
       uint32_t k = static_cast<uint32_t>((centers[3 * p + a] - cb.lo[a]) * scale);
       if (k >= B) k = B - 1;
@@ -202,54 +204,65 @@ struct Child4 {
   int32_t link;
 };
 
-void childrenOf(const BvhNode& n, std::vector<Child4>& out) {
+// A node's children (at most four while collapsing), without allocation.
+struct Kids {
+  Child4 c[4];
+  size_t size = 0;
+  void push(const Child4& k) { c[size++] = k; }
+  void erase(size_t i) {
+    for (size_t k = i; k + 1 < size; ++k) c[k] = c[k + 1];
+    --size;
+  }
+};
+
+void childrenOf(const BvhNode& n, Kids& out) {
   const Child4 c0{{{n.c0lx, n.c0ly, n.c0lz}, {n.c0hx, n.c0hy, n.c0hz}}, n.child0};
   const Child4 c1{{{n.c1lx, n.c1ly, n.c1lz}, {n.c1hx, n.c1hy, n.c1hz}}, n.child1};
   // an absent child is a leaf of zero primitives
-  if (c0.link >= 0 || leafCount(c0.link) != 0) out.push_back(c0);
-  if (c1.link >= 0 || leafCount(c1.link) != 0) out.push_back(c1);
+  if (c0.link >= 0 || leafCount(c0.link) != 0) out.push(c0);
+  if (c1.link >= 0 || leafCount(c1.link) != 0) out.push(c1);
 }
 
 uint32_t collapse(const std::vector<BvhNode>& b2, uint32_t n2, std::vector<Bvh4Node>& out) {
   const uint32_t idx = static_cast<uint32_t>(out.size());
   out.emplace_back();
-  std::vector<Child4> kids;
+  Kids kids;
   childrenOf(b2[n2], kids);
-  while (kids.size() < 4) {
+  while (kids.size < 4) {
     int best = -1;
     float best_area = -1.0f;
-    for (size_t k = 0; k < kids.size(); ++k) {
-      if (kids[k].link < 0) continue;
-      const float a = boxArea(kids[k].box);
+    for (size_t k = 0; k < kids.size; ++k) {
+      if (kids.c[k].link < 0) continue;
+      const float a = boxArea(kids.c[k].box);
       if (a > best_area) {
         best_area = a;
         best = static_cast<int>(k);
       }
     }
     if (best < 0) break;
-    std::vector<Child4> sub;
-    childrenOf(b2[kids[best].link], sub);
-    if (kids.size() - 1 + sub.size() > 4) break;
-    kids.erase(kids.begin() + best);
-    kids.insert(kids.end(), sub.begin(), sub.end());
+    Kids sub;
+    childrenOf(b2[kids.c[best].link], sub);
+    if (kids.size - 1 + sub.size > 4) break;
+    kids.erase(static_cast<size_t>(best));
+    for (size_t k = 0; k < sub.size; ++k) kids.push(sub.c[k]);
   }
   int32_t links[4];
   for (size_t k = 0; k < 4; ++k) {
-    if (k < kids.size())
-      links[k] = kids[k].link >= 0 ? static_cast<int32_t>(collapse(b2, kids[k].link, out))
-                                   : kids[k].link;
+    if (k < kids.size)
+      links[k] = kids.c[k].link >= 0 ? static_cast<int32_t>(collapse(b2, kids.c[k].link, out))
+                                     : kids.c[k].link;
     else
       links[k] = kEmptyLink;
   }
   Bvh4Node& n = out[idx];
   for (int k = 0; k < 4; ++k) {
-    const bool has = static_cast<size_t>(k) < kids.size();
-    n.lox[k] = has ? kids[k].box.lo[0] : 1e30f;
-    n.loy[k] = has ? kids[k].box.lo[1] : 1e30f;
-    n.loz[k] = has ? kids[k].box.lo[2] : 1e30f;
-    n.hix[k] = has ? kids[k].box.hi[0] : 1e30f;
-    n.hiy[k] = has ? kids[k].box.hi[1] : 1e30f;
-    n.hiz[k] = has ? kids[k].box.hi[2] : 1e30f;
+    const bool has = static_cast<size_t>(k) < kids.size;
+    n.lox[k] = has ? kids.c[k].box.lo[0] : 1e30f;
+    n.loy[k] = has ? kids.c[k].box.lo[1] : 1e30f;
+    n.loz[k] = has ? kids.c[k].box.lo[2] : 1e30f;
+    n.hix[k] = has ? kids.c[k].box.hi[0] : 1e30f;
+    n.hiy[k] = has ? kids.c[k].box.hi[1] : 1e30f;
+    n.hiz[k] = has ? kids.c[k].box.hi[2] : 1e30f;
     n.child[k] = links[k];
     n._pad[k] = 0;
   }
@@ -320,13 +333,61 @@ void quantizeBvh4(const std::vector<Bvh4Node>& in, std::vector<Bvh4QNode>& out) 
   }
 }
 
+namespace {
+std::atomic<int> g_build_mode{kBuildAuto};
+thread_local BvhBuildStats tl_build_stats;
+
+bool deviceAvailable() {
+  static const bool ok = [] {
+    int n = 0;
+    const bool has = cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+    cudaGetLastError();
+    return has;
+  }();
+  return ok;
+}
+}  // namespace
+
+void setBvhBuildMode(int mode) { g_build_mode.store(mode); }
+int bvhBuildMode() { return g_build_mode.load(); }
+void resetBvhBuildStats() { tl_build_stats = BvhBuildStats{}; }
+BvhBuildStats bvhBuildStats() { return tl_build_stats; }
+
 uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt, uint32_t prim_base,
                   std::vector<BvhNode>& nodes, std::vector<uint32_t>& order,
                   uint32_t* depth_out) {
   const uint32_t base = static_cast<uint32_t>(nodes.size());
   const size_t order_base = order.size();
+  const auto t0 = std::chrono::steady_clock::now();
   Builder b(boxes, opt, order);
-  if (!boxes.empty()) b.run();
+  const int mode = g_build_mode.load();
+  const bool device = !boxes.empty() && opt.bins == 16 &&
+                      (mode == kBuildDevice ||
+                       (mode == kBuildAuto && boxes.size() >= kDeviceBuildMinPrims &&
+                        deviceAvailable()));
+  bool built = false;
+  if (device) {
+    std::vector<uint32_t> local;
+    std::string err;
+    uint32_t depth = 0;
+    if (buildBvhTmpDevice(boxes, opt, b.tmp, local, &depth, err)) {
+      for (TmpNode& t : b.tmp)
+        if (t.left < 0) t.first += static_cast<uint32_t>(order_base);
+      order.insert(order.end(), local.begin(), local.end());
+      b.max_depth = depth;
+      built = true;
+      ++tl_build_stats.device_builds;
+    } else if (mode == kBuildDevice) {
+      throw std::runtime_error(err);
+    }
+  }
+  if (!built && !boxes.empty()) {
+    b.tmp.clear();
+    b.run();
+    ++tl_build_stats.host_builds;
+  }
+  tl_build_stats.seconds +=
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (depth_out) *depth_out = b.max_depth;
   // Emit: every inner TmpNode becomes one BvhNode; DFS order keeps siblings'
   // subtrees contiguous.  A root that is a leaf gets a node with one child.

@@ -9,6 +9,7 @@
 #define CG_BVH_H_
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "cg_types.h"
@@ -29,10 +30,45 @@ struct BvhBuildOptions {
 // Builds a BVH over `boxes`.  Appends nodes to `nodes` (child indices are
 // absolute, offset by nodes.size() at entry) and returns the root index.
 // `order` receives the primitive permutation: leaf ranges index `order`,
-// offset by `prim_base` (the caller's global primitive offset).
+// offset by `prim_base` (the caller's global primitive offset).  The split
+// structure comes from the GPU (buildBvhTmpDevice) or the host builder, as
+// the build mode selects.
 uint32_t buildBvh(const std::vector<Box>& boxes, const BvhBuildOptions& opt,
                   uint32_t prim_base, std::vector<BvhNode>& nodes,
                   std::vector<uint32_t>& order, uint32_t* depth_out = nullptr);
+
+// The split structure a builder produces before emission: node 0 is the
+// root; an inner node has two children (indices into the same array), a leaf
+// the range [first, first + count) of the primitive permutation.
+struct BvhTmpNode {
+  Box box;
+  int32_t left = -1, right = -1;
+  uint32_t first = 0, count = 0;
+};
+
+// Binned-SAH build on the current CUDA device with the host builder's split
+// rule; `order_local` receives the permutation of 0-based primitive ids and
+// leaf ranges index it from 0.  Returns false (with `err`) on a CUDA error.
+bool buildBvhTmpDevice(const std::vector<Box>& boxes, const BvhBuildOptions& opt,
+                       std::vector<BvhTmpNode>& tmp, std::vector<uint32_t>& order_local,
+                       uint32_t* depth_out, std::string& err);
+
+// Where buildBvh builds: kBuildAuto = on the GPU for trees of at least
+// kDeviceBuildMinPrims primitives when a CUDA device is present, else on the
+// host; kBuildHost / kBuildDevice force one (a failed device build then makes
+// buildBvh throw std::runtime_error).
+enum BvhBuildMode : int { kBuildAuto = 0, kBuildHost = 1, kBuildDevice = 2 };
+constexpr uint32_t kDeviceBuildMinPrims = 16384;
+void setBvhBuildMode(int mode);
+int bvhBuildMode();
+// Statistics of the calling thread's builds since the last reset: host and
+// device builds and the seconds they took.
+struct BvhBuildStats {
+  uint32_t host_builds = 0, device_builds = 0;
+  double seconds = 0.0;
+};
+void resetBvhBuildStats();
+BvhBuildStats bvhBuildStats();
 
 // Leaf links: ~((first << 3) | count), count <= 7 (so the values INT_MIN and
 // INT_MIN + 1, i.e. count 7 and 6 with first = 2^28 - 1, never occur and

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
 constexpr int kStepBudget = 16;
 constexpr int kRefill = 8;
 
-template <bool kAny, bool kCount>
+template <bool kAny, bool kCount, int kNodes>
 __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuffers& wb, uint32_t n,
                                                    uint32_t* work, int parity) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -212,7 +212,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
       if (exhausted) break;
       continue;
     }
-    if (ray >= 0 && travSteps<kAny, kCount>(sc, st, stack, kStepBudget, cnt, wb.status)) {
+    if (ray >= 0 && travSteps<kAny, kCount, kNodes>(sc, st, stack, kStepBudget, cnt, wb.status)) {
       if (kAny) {
         if (st.best.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[ray]], wb.sh_o[ray].w);
       } else {
@@ -240,7 +240,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
 // counts[3] (extend) and counts[4] (shadow) are the work counters; each is
 // zeroed by the kernel before its user in stream order (k_gen for depth 0,
 // k_shade for the next extend, k_extend for the shadow launch after it).
-template <bool kCount>
+template <bool kCount, int kNodes>
 __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, WaveBuffers wb,
                                                               int parity) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
@@ -250,14 +250,14 @@ __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, Wave
     wb.counts[4] = 0u;
     atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
   }
-  persistentTraverse<false, kCount>(sc, wb, n, &wb.counts[3], parity);
+  persistentTraverse<false, kCount, kNodes>(sc, wb, n, &wb.counts[3], parity);
 }
 
-template <bool kCount>
+template <bool kCount, int kNodes>
 __global__ void __launch_bounds__(256, 4) k_shadow_persistent(SceneView sc, WaveBuffers wb) {
   const uint32_t n = min(wb.counts[2], wb.capacity);
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wb.stats[1], static_cast<unsigned long long>(n));
-  persistentTraverse<true, kCount>(sc, wb, n, &wb.counts[4], 0);
+  persistentTraverse<true, kCount, kNodes>(sc, wb, n, &wb.counts[4], 0);
 }
 
 // ---- shadow: t-bounded any hit (solveEmission, trace.wesl:91-113) ----------------
@@ -733,11 +733,15 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
   if (ls.persistent) {  // one resident grid: 64 registers -> 65536 / (64 * block) blocks per SM
-    const uint32_t pgrid = gridFor(1024u / block);
-    if (counting)
-      k_extend_persistent<true><<<pgrid, block, 0, s>>>(sc, wb, parity);
-    else
-      k_extend_persistent<false><<<pgrid, block, 0, s>>>(sc, wb, parity);
+    const uint32_t g = gridFor(1024u / block);
+    switch (ls.nodes * 2 + (counting ? 1 : 0)) {
+      case kNodesBinary * 2: k_extend_persistent<false, kNodesBinary><<<g, block, 0, s>>>(sc, wb, parity); break;
+      case kNodesBinary * 2 + 1: k_extend_persistent<true, kNodesBinary><<<g, block, 0, s>>>(sc, wb, parity); break;
+      case kNodesWide4 * 2: k_extend_persistent<false, kNodesWide4><<<g, block, 0, s>>>(sc, wb, parity); break;
+      case kNodesWide4 * 2 + 1: k_extend_persistent<true, kNodesWide4><<<g, block, 0, s>>>(sc, wb, parity); break;
+      case kNodesWide4Q * 2 + 1: k_extend_persistent<true, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb, parity); break;
+      default: k_extend_persistent<false, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb, parity); break;
+    }
     return;
   }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
@@ -765,11 +769,15 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
   if (ls.persistent) {
-    const uint32_t pgrid = gridFor(1024u / block);
-    if (counting)
-      k_shadow_persistent<true><<<pgrid, block, 0, s>>>(sc, wb);
-    else
-      k_shadow_persistent<false><<<pgrid, block, 0, s>>>(sc, wb);
+    const uint32_t g = gridFor(1024u / block);
+    switch (ls.nodes * 2 + (counting ? 1 : 0)) {
+      case kNodesBinary * 2: k_shadow_persistent<false, kNodesBinary><<<g, block, 0, s>>>(sc, wb); break;
+      case kNodesBinary * 2 + 1: k_shadow_persistent<true, kNodesBinary><<<g, block, 0, s>>>(sc, wb); break;
+      case kNodesWide4 * 2: k_shadow_persistent<false, kNodesWide4><<<g, block, 0, s>>>(sc, wb); break;
+      case kNodesWide4 * 2 + 1: k_shadow_persistent<true, kNodesWide4><<<g, block, 0, s>>>(sc, wb); break;
+      case kNodesWide4Q * 2 + 1: k_shadow_persistent<true, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb); break;
+      default: k_shadow_persistent<false, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb); break;
+    }
     return;
   }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);

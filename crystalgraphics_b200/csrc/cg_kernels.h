@@ -73,20 +73,13 @@ struct ChunkDesc {
   uint32_t pixel_count;
 };
 
-// Node format the traversal walks.
-enum NodeFormat : int {
-  kNodesBinary = 0,  // BvhNode, two children
-  kNodesWide4 = 1,   // Bvh4Node, four children with full-precision boxes
-  kNodesWide4Q = 2,  // Bvh4QNode, four children with 8-bit boxes
-};
-
 struct LaunchShape {
   uint32_t extend_block = 128;
   uint32_t shade_block = 128;
   uint32_t grid_extend = 0;  // 0: derived from the SM count
   uint32_t grid_shade = 0;
   int nodes = kNodesWide4;   // NodeFormat of the traversal
-  bool persistent = false;   // persistent warps with lane refill (binary trees)
+  bool persistent = true;    // persistent warps with lane refill
   bool shade_sort = true;    // group a block's rays by shading key before shading
 };
 

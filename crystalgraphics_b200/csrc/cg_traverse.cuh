@@ -192,6 +192,90 @@ __device__ __forceinline__ HitRec traceRay(const SceneView& sc, float wox, float
   return best;
 }
 
+__device__ __forceinline__ void cswap(float& ka, int32_t& la, float& kb, int32_t& lb) {
+  if (kb < ka) {
+    const float tk = ka;
+    ka = kb;
+    kb = tk;
+    const int32_t tl = la;
+    la = lb;
+    lb = tl;
+  }
+}
+
+
+// Byte c of w as a float (exact): the byte under the exponent of 2^23, minus 2^23.
+__device__ __forceinline__ float byteToFloat(uint32_t w, uint32_t c) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | c)) - 8388608.0f;
+}
+
+// The two four-wide node formats: full-precision child slabs, or 8-bit
+// offsets from the node origin (decoded to world-space bounds that contain
+// the full-precision ones: fmaf rounds q * scale + origin to nearest, and the
+// exact value is already outside the child's box).  fetch() returns, per
+// axis, the near and far bound of each child for a ray whose inverse
+// direction has the given signs (near = lo where the inverse direction is
+// >= 0): the slab distances then need no min/max per axis.  With FMA rounding
+// monotonic in the bound, near <= far along the ray, so the entry and exit
+// distances equal min/max of the two slab planes bit for bit.
+template <bool kQuant>
+struct Wide;
+
+template <>
+struct Wide<false> {
+  using Node = Bvh4Node;
+  static __device__ __forceinline__ const Node* tlas(const SceneView& sc) { return sc.tlas4; }
+  static __device__ __forceinline__ const Node* blas(const SceneView& sc) { return sc.blas4; }
+  static __device__ __forceinline__ int4 fetch(const Node* n, bool negx, bool negy, bool negz,
+                                               float nx[4], float fx[4], float ny[4], float fy[4],
+                                               float nz[4], float fz[4]) {
+    const float4* np = reinterpret_cast<const float4*>(n);
+    // float4 rows: lo.x, hi.x, lo.y, hi.y, lo.z, hi.z
+    const float4 a = __ldg(np + (negx ? 1 : 0)), b = __ldg(np + (negx ? 0 : 1));
+    const float4 c = __ldg(np + (negy ? 3 : 2)), d = __ldg(np + (negy ? 2 : 3));
+    const float4 e = __ldg(np + (negz ? 5 : 4)), f = __ldg(np + (negz ? 4 : 5));
+    nx[0] = a.x; nx[1] = a.y; nx[2] = a.z; nx[3] = a.w;
+    fx[0] = b.x; fx[1] = b.y; fx[2] = b.z; fx[3] = b.w;
+    ny[0] = c.x; ny[1] = c.y; ny[2] = c.z; ny[3] = c.w;
+    fy[0] = d.x; fy[1] = d.y; fy[2] = d.z; fy[3] = d.w;
+    nz[0] = e.x; nz[1] = e.y; nz[2] = e.z; nz[3] = e.w;
+    fz[0] = f.x; fz[1] = f.y; fz[2] = f.z; fz[3] = f.w;
+    return __ldg(reinterpret_cast<const int4*>(np + 6));
+  }
+};
+
+template <>
+struct Wide<true> {
+  using Node = Bvh4QNode;
+  static __device__ __forceinline__ const Node* tlas(const SceneView& sc) { return sc.tlas4q; }
+  static __device__ __forceinline__ const Node* blas(const SceneView& sc) { return sc.blas4q; }
+  static __device__ __forceinline__ int4 fetch(const Node* n, bool negx, bool negy, bool negz,
+                                               float nx[4], float fx[4], float ny[4], float fy[4],
+                                               float nz[4], float fz[4]) {
+    const float4* np = reinterpret_cast<const float4*>(n);
+    const float4 h = __ldg(np);
+    const uint4 qa = __ldg(reinterpret_cast<const uint4*>(np + 1));  // lo.x hi.x lo.y hi.y
+    const uint4 qb = __ldg(reinterpret_cast<const uint4*>(np + 2));  // lo.z hi.z
+    const uint32_t sb = __float_as_uint(h.w);
+    const float sx = __uint_as_float((sb & 0xffu) << 23);
+    const float sy = __uint_as_float(((sb >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((sb >> 16) & 0xffu) << 23);
+    const uint32_t wnx = negx ? qa.y : qa.x, wfx = negx ? qa.x : qa.y;
+    const uint32_t wny = negy ? qa.w : qa.z, wfy = negy ? qa.z : qa.w;
+    const uint32_t wnz = negz ? qb.y : qb.x, wfz = negz ? qb.x : qb.y;
+#pragma unroll
+    for (uint32_t c = 0; c < 4; ++c) {
+      nx[c] = fmaf(byteToFloat(wnx, c), sx, h.x);
+      fx[c] = fmaf(byteToFloat(wfx, c), sx, h.x);
+      ny[c] = fmaf(byteToFloat(wny, c), sy, h.y);
+      fy[c] = fmaf(byteToFloat(wfy, c), sy, h.y);
+      nz[c] = fmaf(byteToFloat(wnz, c), sz, h.z);
+      fz[c] = fmaf(byteToFloat(wfz, c), sz, h.z);
+    }
+    return __ldg(reinterpret_cast<const int4*>(np + 3));
+  }
+};
+
 // Traversal state of one ray, advanced a bounded number of steps at a time so
 // a warp can refill lanes whose ray finished (persistent threads with
 // dynamic fetch): the closest-hit walk of traceRay, resumable.
@@ -219,11 +303,54 @@ __device__ __forceinline__ void travInit(TravState& s, float4 o, float4 d, float
 // Runs at most `budget` steps (a node visit, a leaf, or a return to the
 // TLAS); returns true when the ray is finished (s.best holds its hit; with
 // kAny the first hit below s.best.t finishes it).
-template <bool kAny, bool kCount>
+template <bool kAny, bool kCount, int kNodes = kNodesBinary>
 __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int32_t* stack,
                                           int budget, TravCounters& cnt, uint32_t* status) {
   for (int step = 0; step < budget; ++step) {
     const int32_t node = s.node;
+    if (kNodes != kNodesBinary && node >= 0) {  // a four-wide node (traceRay4's inner step)
+      using W = Wide<kNodes == kNodesWide4Q>;
+      const typename W::Node* nodes = s.cur_inst < 0 ? W::tlas(sc) : W::blas(sc);
+      float nxs[4], fxs[4], nys[4], fys[4], nzs[4], fzs[4];
+      const int4 ch = W::fetch(nodes + node, s.idx < 0.0f, s.idy < 0.0f, s.idz < 0.0f, nxs, fxs,
+                               nys, fys, nzs, fzs);
+      if (kCount) ++cnt.nodes;
+      float k[4];
+      const int32_t links[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float a0 = fmaf(nxs[c], s.idx, -s.oix), a1 = fmaf(fxs[c], s.idx, -s.oix);
+        const float b0 = fmaf(nys[c], s.idy, -s.oiy), b1 = fmaf(fys[c], s.idy, -s.oiy);
+        const float c0 = fmaf(nzs[c], s.idz, -s.oiz), c1 = fmaf(fzs[c], s.idz, -s.oiz);
+        const float tmin = fmaxf(fmaxf(a0, b0), fmaxf(c0, 0.0f));
+        const float tmx = fminf(fminf(a1, b1), fminf(c1, s.best.t));
+        const bool hit = kNodes == kNodesWide4Q ? (tmin <= tmx && links[c] != kEmptyLink)
+                                                : tmin <= tmx;
+        k[c] = hit ? tmin : INFINITY;
+      }
+      int32_t l0 = ch.x, l1 = ch.y, l2 = ch.z, l3 = ch.w;
+      float k0 = k[0], k1 = k[1], k2 = k[2], k3 = k[3];
+      cswap(k0, l0, k1, l1);
+      cswap(k2, l2, k3, l3);
+      cswap(k0, l0, k2, l2);
+      cswap(k1, l1, k3, l3);
+      cswap(k1, l1, k2, l2);
+      if (k0 == INFINITY) {
+        s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+        continue;
+      }
+      const int pushes = (k1 != INFINITY) + (k2 != INFINITY) + (k3 != INFINITY);
+      if (s.sp + pushes > kStackSize) {
+        atomicOr(status, 1u);
+        s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
+        return true;
+      }
+      if (k3 != INFINITY) stack[s.sp++] = l3;
+      if (k2 != INFINITY) stack[s.sp++] = l2;
+      if (k1 != INFINITY) stack[s.sp++] = l1;
+      s.node = l0;
+      continue;
+    }
     if (node >= 0) {
       const BvhNode* nodes = s.cur_inst < 0 ? sc.tlas : sc.blas;
       const float4* np = reinterpret_cast<const float4*>(nodes + node);
@@ -298,7 +425,8 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
       }
       stack[s.sp++] = kToTlas;
       s.cur_inst = static_cast<int32_t>(first);
-      s.node = static_cast<int32_t>(meta.x);  // blas_root
+      // blas_root (binary) or blas4_root (four-wide)
+      s.node = static_cast<int32_t>(kNodes == kNodesBinary ? meta.x : meta.w);
       continue;
     }
     for (uint32_t k = 0; k < count; ++k) {
@@ -320,93 +448,10 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
   return false;
 }
 
-__device__ __forceinline__ void cswap(float& ka, int32_t& la, float& kb, int32_t& lb) {
-  if (kb < ka) {
-    const float tk = ka;
-    ka = kb;
-    kb = tk;
-    const int32_t tl = la;
-    la = lb;
-    lb = tl;
-  }
-}
-
 // The same closest / any hit over Bvh4Node trees: one node visit tests four
 // boxes (six independent 128-bit slab loads), the hit children are ordered
 // by entry distance, the nearest is visited next and the others pushed.
 // Triangle and instance handling is that of traceRay (bit-identical hits).
-// Byte c of w as a float (exact): the byte under the exponent of 2^23, minus 2^23.
-__device__ __forceinline__ float byteToFloat(uint32_t w, uint32_t c) {
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | c)) - 8388608.0f;
-}
-
-// The two four-wide node formats: full-precision child slabs, or 8-bit
-// offsets from the node origin (decoded to world-space bounds that contain
-// the full-precision ones: fmaf rounds q * scale + origin to nearest, and the
-// exact value is already outside the child's box).  fetch() returns, per
-// axis, the near and far bound of each child for a ray whose inverse
-// direction has the given signs (near = lo where the inverse direction is
-// >= 0): the slab distances then need no min/max per axis.  With FMA rounding
-// monotonic in the bound, near <= far along the ray, so the entry and exit
-// distances equal min/max of the two slab planes bit for bit.
-template <bool kQuant>
-struct Wide;
-
-template <>
-struct Wide<false> {
-  using Node = Bvh4Node;
-  static __device__ __forceinline__ const Node* tlas(const SceneView& sc) { return sc.tlas4; }
-  static __device__ __forceinline__ const Node* blas(const SceneView& sc) { return sc.blas4; }
-  static __device__ __forceinline__ int4 fetch(const Node* n, bool negx, bool negy, bool negz,
-                                               float nx[4], float fx[4], float ny[4], float fy[4],
-                                               float nz[4], float fz[4]) {
-    const float4* np = reinterpret_cast<const float4*>(n);
-    // float4 rows: lo.x, hi.x, lo.y, hi.y, lo.z, hi.z
-    const float4 a = __ldg(np + (negx ? 1 : 0)), b = __ldg(np + (negx ? 0 : 1));
-    const float4 c = __ldg(np + (negy ? 3 : 2)), d = __ldg(np + (negy ? 2 : 3));
-    const float4 e = __ldg(np + (negz ? 5 : 4)), f = __ldg(np + (negz ? 4 : 5));
-    nx[0] = a.x; nx[1] = a.y; nx[2] = a.z; nx[3] = a.w;
-    fx[0] = b.x; fx[1] = b.y; fx[2] = b.z; fx[3] = b.w;
-    ny[0] = c.x; ny[1] = c.y; ny[2] = c.z; ny[3] = c.w;
-    fy[0] = d.x; fy[1] = d.y; fy[2] = d.z; fy[3] = d.w;
-    nz[0] = e.x; nz[1] = e.y; nz[2] = e.z; nz[3] = e.w;
-    fz[0] = f.x; fz[1] = f.y; fz[2] = f.z; fz[3] = f.w;
-    return __ldg(reinterpret_cast<const int4*>(np + 6));
-  }
-};
-
-template <>
-struct Wide<true> {
-  using Node = Bvh4QNode;
-  static __device__ __forceinline__ const Node* tlas(const SceneView& sc) { return sc.tlas4q; }
-  static __device__ __forceinline__ const Node* blas(const SceneView& sc) { return sc.blas4q; }
-  static __device__ __forceinline__ int4 fetch(const Node* n, bool negx, bool negy, bool negz,
-                                               float nx[4], float fx[4], float ny[4], float fy[4],
-                                               float nz[4], float fz[4]) {
-    const float4* np = reinterpret_cast<const float4*>(n);
-    const float4 h = __ldg(np);
-    const uint4 qa = __ldg(reinterpret_cast<const uint4*>(np + 1));  // lo.x hi.x lo.y hi.y
-    const uint4 qb = __ldg(reinterpret_cast<const uint4*>(np + 2));  // lo.z hi.z
-    const uint32_t sb = __float_as_uint(h.w);
-    const float sx = __uint_as_float((sb & 0xffu) << 23);
-    const float sy = __uint_as_float(((sb >> 8) & 0xffu) << 23);
-    const float sz = __uint_as_float(((sb >> 16) & 0xffu) << 23);
-    const uint32_t wnx = negx ? qa.y : qa.x, wfx = negx ? qa.x : qa.y;
-    const uint32_t wny = negy ? qa.w : qa.z, wfy = negy ? qa.z : qa.w;
-    const uint32_t wnz = negz ? qb.y : qb.x, wfz = negz ? qb.x : qb.y;
-#pragma unroll
-    for (uint32_t c = 0; c < 4; ++c) {
-      nx[c] = fmaf(byteToFloat(wnx, c), sx, h.x);
-      fx[c] = fmaf(byteToFloat(wfx, c), sx, h.x);
-      ny[c] = fmaf(byteToFloat(wny, c), sy, h.y);
-      fy[c] = fmaf(byteToFloat(wfy, c), sy, h.y);
-      nz[c] = fmaf(byteToFloat(wnz, c), sz, h.z);
-      fz[c] = fmaf(byteToFloat(wfz, c), sz, h.z);
-    }
-    return __ldg(reinterpret_cast<const int4*>(np + 3));
-  }
-};
-
 template <bool kAny, bool kCount, bool kQuant = false>
 __device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, float woy, float woz,
                                             float wdx, float wdy, float wdz, float tmax,

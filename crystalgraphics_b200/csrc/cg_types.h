@@ -38,6 +38,13 @@ static_assert(sizeof(BvhNode) == 64, "BvhNode is 64 bytes");
 // Link of an absent four-wide child (a leaf of zero primitives).
 constexpr int32_t kEmptyLink = -1;
 
+// Node format the traversal walks.
+enum NodeFormat : int {
+  kNodesBinary = 0,  // BvhNode, two children
+  kNodesWide4 = 1,   // Bvh4Node, four children with full-precision boxes
+  kNodesWide4Q = 2,  // Bvh4QNode, four children with 8-bit boxes
+};
+
 // Four-wide node: the slabs of four children, structure-of-arrays so each
 // axis bound is one 128-bit load; links as in BvhNode (leaf count in the low
 // 3 bits of ~link).  An absent child has link kEmptyLink and a point box at

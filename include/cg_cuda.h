@@ -183,8 +183,29 @@ typedef struct cg_scene_info {
   uint32_t blas_node_count, tlas_node_count, light_node_count;
   uint64_t device_bytes;        /* device memory held by the scene           */
   uint64_t tag;                 /* unique per cg_scene_create (Scene::Impl::tag_) */
+  double bvh_build_seconds;     /* time spent building the BVHs              */
+  uint32_t bvh_host_builds;     /* trees built on the host ...               */
+  uint32_t bvh_device_builds;   /* ... and on the GPU                        */
 } cg_scene_info;
 CG_API int cg_scene_get_info(cg_scene_t scene, cg_scene_info* out);
+
+/* Where LoadScene builds its BVHs (binned SAH, 16 bins, with the same split
+ * rule either way): 0 = on the GPU for trees of at least 16384 primitives when
+ * a device is present, else on the host (default); 1 = always on the host;
+ * 2 = always on the GPU (a failed device build fails the load).  No
+ * counterpart in the reference, which builds median-split trees on the host
+ * (src/pathtracing/blas.h:112-194, tlas.h:98-140). */
+#define CG_BVH_BUILD_AUTO 0
+#define CG_BVH_BUILD_HOST 1
+#define CG_BVH_BUILD_DEVICE 2
+CG_API int cg_set_bvh_build(int mode);
+/* Builds one BVH over `count` boxes (6 floats each: lo xyz, hi xyz) on the
+ * host (mode 1) or the GPU (mode 2) and returns its 64-byte BvhNode records
+ * (when node_capacity suffices; *node_count is always set) and the primitive
+ * permutation its leaves index.  For tests of the two builders. */
+CG_API int cg_bvh_build(const float* boxes, uint32_t count, int mode, void* nodes_out,
+                        uint32_t node_capacity, uint32_t* node_count,
+                        uint32_t* order_out);
 
 /* EmissivePrim (src/pathtracing/emissive_buffer.h:27-40), 80 bytes. */
 typedef struct cg_emissive_prim {
@@ -298,16 +319,17 @@ CG_API int cg_batch_render(cg_scene_t scene, const cg_view_desc* views,
                            uint8_t* films_rgba8);
 
 /* Wavefront tuning: rays per level queue (capacity), threads per block of the
- * traversal and shading kernels.  0 = keep.  cg_autotune searches these for a
- * scene and a representative view and keeps the best. */
+ * traversal and shading kernels, and kernel variants.  0 = keep.  cg_autotune
+ * searches these for a scene and a representative view (cg_autotune_views:
+ * several views) and keeps the best. */
 typedef struct cg_tuning {
   uint32_t queue_capacity;
   uint32_t extend_block;
   uint32_t shade_block;
   uint32_t use_graph;   /* 1 = capture the chunk pipeline as a CUDA graph */
   uint32_t bvh_width;   /* 4 (default) or 2: node width the traversal walks */
-  uint32_t persistent;  /* 1 = persistent traversal warps that refill idle lanes
-                           (binary trees), 0 = one ray per thread */
+  uint32_t persistent;  /* 1 (default) = persistent traversal warps that refill
+                           idle lanes, 2 = one ray per thread, 0 = keep */
   uint32_t shade_sort;  /* 1 (default) = group rays by material kind before
                            shading, 2 = do not, 0 = keep */
   uint32_t box_bits;    /* four-wide child boxes: 32 (default) = floats in
@@ -317,6 +339,13 @@ CG_API int cg_set_tuning(const cg_tuning* tuning);
 CG_API int cg_get_tuning(cg_tuning* out);
 CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view,
                        cg_tuning* best);
+/* The same search with the timed batch made of `count` probe views (for
+ * example a sample of a batch to be rendered).  The search is a coordinate
+ * descent from the current tuning: kernel variant (node width and box bits,
+ * persistent traversal, shading sort), then queue capacity, then block sizes;
+ * the fastest tuning is kept. */
+CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views,
+                             uint32_t count, cg_tuning* best);
 
 /* ---- served form -----------------------------------------------------------
  * A request loop over several resident scenes.  Requests are admitted while

@@ -166,6 +166,7 @@ def test_server_cancel_and_timeout(cornell):
 
 @pytest.mark.parametrize("variant", [dict(bvh_width=2, persistent=False),
                                      dict(bvh_width=2, persistent=True),
+                                     dict(bvh_width=4, persistent=True),
                                      dict(bvh_width=4, persistent=False),
                                      dict(bvh_width=4, persistent=False, shade_sort=False),
                                      dict(bvh_width=4, persistent=False, box_bits=8)])
@@ -194,7 +195,16 @@ def test_autotune_returns_a_valid_tuning(cornell):
     s, g = cornell
     t = B.autotune(g, (s.camera.position[:], s.camera.direction[:], 96, 96, 4, 1))
     assert t.queue_capacity >= 4096 and t.extend_block % 32 == 0 and t.shade_block % 32 == 0
-    B.SetTuning(queue_capacity=16 << 20, extend_block=128, shade_block=128, use_graph=1)
+    assert t.bvh_width in (2, 4) and t.box_bits in (8, 32) and t.shade_sort in (1, 2)
+    # a tuning found on probe views renders the batch like the default tuning
+    views = _views(s)
+    ref = B.batch_render(g, views)
+    t2 = B.autotune_views(g, views[::2])
+    assert B.GetTuning().bvh_width == t2.bvh_width
+    for x, y in zip(B.batch_render(g, views), ref):
+        assert _close(x, y) < RTOL
+    B.SetTuning(queue_capacity=16 << 20, extend_block=128, shade_block=128, use_graph=1,
+                bvh_width=4, persistent=False, shade_sort=True, box_bits=32)
 
 
 def test_gltf_scene_renders_like_the_in_memory_scene(tmp_path, cornell):
