@@ -53,7 +53,13 @@ class CgSceneDesc(C.Structure):
         ("instances", C.c_void_p), ("instance_count", u32),
         ("materials", C.c_void_p), ("material_count", u32),
         ("env_rgba32f", C.c_void_p), ("env_width", u32), ("env_height", u32),
+        ("textures", C.c_void_p), ("texture_count", u32),
     ]
+
+
+class CgTexture(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("rgba8", C.c_void_p), ("wrap_s", C.c_int32),
+                ("wrap_t", C.c_int32), ("_pad", u32 * 2)]
 
 
 class CgSceneInfo(C.Structure):
@@ -123,7 +129,8 @@ MATERIAL_DTYPE = np.dtype([
     ("metallic_factor", "<f4"), ("roughness_factor", "<f4"), ("ior", "<f4"),
     ("dispersion", "<f4"), ("transmission_factor", "<f4"), ("thickness_factor", "<f4"),
     ("base_color_texture", "<i4"), ("metallic_roughness_texture", "<i4"),
-    ("emissive_texture", "<i4"), ("transmission_texture", "<i4"), ("_pad", "<u4", 2)])
+    ("emissive_texture", "<i4"), ("transmission_texture", "<i4"), ("texcoord_sets", "<u4"),
+    ("_pad", "<u4")])
 EMISSIVE_DTYPE = np.dtype([("v0", "<f4", 3), ("_p0", "<f4"), ("v1", "<f4", 3), ("_p1", "<f4"),
                            ("v2", "<f4", 3), ("_p2", "<f4"), ("emission", "<f4", 3),
                            ("area", "<f4"), ("weight", "<f4"), ("_pad", "<f4", 3)])

@@ -74,6 +74,7 @@ def _load():
         "cg_autotune": (i, [vp, C.POINTER(_abi.CgViewDesc), C.POINTER(_abi.CgTuning)]),
         "cg_autotune_views": (i, [vp, vp, u32, C.POINTER(_abi.CgTuning)]),
         "cg_set_bvh_build": (i, [i]),
+        "cg_png_decode": (i, [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), vp]),
         "cg_bvh_build": (i, [vp, u32, i, vp, u32, C.POINTER(u32), vp]),
         "cg_server_create": (i, [vp, u32, C.c_uint64, C.POINTER(vp)]),
         "cg_server_destroy": (i, [vp]),
@@ -240,12 +241,19 @@ def parse_gltf(path) -> "scenes.Scene":
                 return np.zeros(0, dtype)
             buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr)
             return np.frombuffer(buf, dtype=dtype, count=n).copy()
+        textures = []
+        if d.texture_count:
+            tex = (_abi.CgTexture * d.texture_count).from_address(d.textures)
+            for t in tex:
+                img = arr(t.rgba8, t.width * t.height * 4, np.uint8).reshape(t.height, t.width, 4)
+                textures.append((img, int(t.wrap_s), int(t.wrap_t)))
         return scenes.Scene(name=os.fspath(path),
                             vertices=arr(d.vertices, d.vertex_count, _abi.VERTEX_DTYPE),
                             indices=arr(d.indices, d.index_count, np.uint32),
                             meshes=arr(d.meshes, d.mesh_count, _abi.MESH_DTYPE),
                             instances=arr(d.instances, d.instance_count, _abi.INSTANCE_DTYPE),
-                            materials=arr(d.materials, d.material_count, _abi.MATERIAL_DTYPE))
+                            materials=arr(d.materials, d.material_count, _abi.MATERIAL_DTYPE),
+                            textures=textures)
     finally:
         lib.cg_gltf_free(st)
 
@@ -315,6 +323,16 @@ def SetBvhBuild(mode: int) -> None:
     """Where LoadScene builds BVHs: _abi.CG_BVH_BUILD_AUTO (GPU for large trees),
     CG_BVH_BUILD_HOST or CG_BVH_BUILD_DEVICE."""
     _check(lib.cg_set_bvh_build(mode))
+
+
+def png_decode(data: bytes) -> np.ndarray:
+    """A PNG file image as an (h, w, 4) uint8 RGBA array."""
+    buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+    w, h = C.c_uint32(), C.c_uint32()
+    _check(lib.cg_png_decode(buf, len(data), C.byref(w), C.byref(h), None))
+    out = np.empty((h.value, w.value, 4), np.uint8)
+    _check(lib.cg_png_decode(buf, len(data), C.byref(w), C.byref(h), out.ctypes.data))
+    return out
 
 
 def bvh_build(boxes: np.ndarray, mode: int):

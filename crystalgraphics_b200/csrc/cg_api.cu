@@ -78,7 +78,9 @@ int uploadScene(const HostScene& h, SceneDev& s) {
       {h.alias.data(), bytesOf(h.alias), 0},     {h.light_bvh.data(), bytesOf(h.light_bvh), 0},
       {h.ltri.data(), bytesOf(h.ltri), 0},       {h.env.data(), bytesOf(h.env), 0},
       {h.tlas4.data(), bytesOf(h.tlas4), 0},     {h.blas4.data(), bytesOf(h.blas4), 0},
-      {h.tlas4q.data(), bytesOf(h.tlas4q), 0},   {h.blas4q.data(), bytesOf(h.blas4q), 0}};
+      {h.tlas4q.data(), bytesOf(h.tlas4q), 0},   {h.blas4q.data(), bytesOf(h.blas4q), 0},
+      {h.mattex.data(), bytesOf(h.mattex), 0},   {h.tex.data(), bytesOf(h.tex), 0},
+      {h.vuv.data(), bytesOf(h.vuv), 0}};
   size_t total = 0;
   for (auto& p : parts) {
     p.off = total;
@@ -106,6 +108,12 @@ int uploadScene(const HostScene& h, SceneDev& s) {
   v.blas4 = reinterpret_cast<const Bvh4Node*>(base + parts[13].off);
   v.tlas4q = reinterpret_cast<const Bvh4QNode*>(base + parts[14].off);
   v.blas4q = reinterpret_cast<const Bvh4QNode*>(base + parts[15].off);
+  v.mattex = reinterpret_cast<const DevMatTex*>(base + parts[16].off);
+  v.tex = reinterpret_cast<const uchar4*>(base + parts[17].off);
+  v.vuv = reinterpret_cast<const float4*>(base + parts[18].off);
+  v.tex_w = h.tex_w;
+  v.tex_h = h.tex_h;
+  v.tex_layers = h.tex_layers;
   v.env_w = h.env_w;
   v.env_h = h.env_h;
   v.emissive_count = static_cast<uint32_t>(h.eprim.size());
@@ -576,6 +584,8 @@ CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
   std::vector<float>().swap(h.tris);
   std::vector<uint32_t>().swap(h.tri_vidx);
   std::vector<float>().swap(h.vnormal);
+  std::vector<uint32_t>().swap(h.tex);
+  std::vector<float>().swap(h.vuv);
   *out = reinterpret_cast<cg_scene_t>(sd.release());
   return CG_OK;
 }

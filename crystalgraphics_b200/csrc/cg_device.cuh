@@ -272,10 +272,13 @@ struct Mat {
   bool volume;
   float emission;
 };
-__device__ __forceinline__ Mat decode(const DevMaterial& m, float w, const SmitsPos& sp) {
-  V3 base{m.base[0], m.base[1], m.base[2]};
+// decode (material.wesl:19-53) from the material values after any texture
+// lookups: base color rgb, metallic, roughness, transmission (clamped) and
+// the emission max(factor * strength, 0).
+__device__ __forceinline__ Mat decodeValues(const DevMaterial& m, V3 base, float metallic,
+                                            float roughness, float transmission, V3 emission,
+                                            float w, const SmitsPos& sp) {
   float reflectance = rgbToReflectance(base, sp);
-  float metallic = m.metallic, transmission = m.transmission;
   float real_ior = m.ior;
   if (metallic == 0.0f && transmission > 0.0f && !(m.dispersion <= 0.0f)) {
     float inv_abbe = m.dispersion / 20.0f;
@@ -285,12 +288,80 @@ __device__ __forceinline__ Mat decode(const DevMaterial& m, float w, const Smits
                           0.0f, 10.0f));
   Mat e;
   e.diffuse_reflectance = (1.0f - metallic) * (1.0f - transmission) * reflectance;
-  e.microfacet_roughness = m.roughness * m.roughness;
+  e.microfacet_roughness = roughness * roughness;
   e.ior = IOR{real_ior, metallic * im};
   e.transmission = transmission;
   e.volume = (m.volume & 1u) != 0u;
-  e.emission = rgbToReflectance(V3{m.emission[0], m.emission[1], m.emission[2]}, sp);
+  e.emission = rgbToReflectance(emission, sp);
   return e;
+}
+
+__device__ __forceinline__ Mat decode(const DevMaterial& m, float w, const SmitsPos& sp) {
+  return decodeValues(m, V3{m.base[0], m.base[1], m.base[2]}, m.metallic, m.roughness,
+                      m.transmission, V3{m.emission[0], m.emission[1], m.emission[2]}, w, sp);
+}
+
+// textureSampleLevel(material_textures, sampler, uv, layer, 0) with the
+// reference's sampler (linear filtering, clamp to edge; src/wgpu/resource.cpp:
+// 133-142) on the RGBA8Unorm array: texel centres at (i + 0.5) / size,
+// bilinear weights in float, rounded per operation as the CPU restatement.
+// x and y are clamped to [-1, size] first (beyond that every tap is the edge
+// texel), which keeps the integer conversion in range.
+__device__ __forceinline__ float4 sampleMaterialTexture(const SceneView& sc, int layer, float u,
+                                                        float v) {
+  const float W = static_cast<float>(sc.tex_w), H = static_cast<float>(sc.tex_h);
+  const float x = fminf(fmaxf(__fsub_rn(__fmul_rn(u, W), 0.5f), -1.0f), W);
+  const float y = fminf(fmaxf(__fsub_rn(__fmul_rn(v, H), 0.5f), -1.0f), H);
+  const float fx = floorf(x), fy = floorf(y);
+  const float ax = __fsub_rn(x, fx), ay = __fsub_rn(y, fy);
+  const int wmax = static_cast<int>(sc.tex_w) - 1, hmax = static_cast<int>(sc.tex_h) - 1;
+  const int x0 = min(max(static_cast<int>(fx), 0), wmax), x1 = min(max(static_cast<int>(fx) + 1, 0), wmax);
+  const int y0 = min(max(static_cast<int>(fy), 0), hmax), y1 = min(max(static_cast<int>(fy) + 1, 0), hmax);
+  const uchar4* L = sc.tex + static_cast<size_t>(layer) * sc.tex_w * sc.tex_h;
+  const uchar4 t00 = __ldg(L + y0 * sc.tex_w + x0), t10 = __ldg(L + y0 * sc.tex_w + x1);
+  const uchar4 t01 = __ldg(L + y1 * sc.tex_w + x0), t11 = __ldg(L + y1 * sc.tex_w + x1);
+  const float bx = __fsub_rn(1.0f, ax), by = __fsub_rn(1.0f, ay);
+  auto ch = [&](unsigned char a, unsigned char b, unsigned char c, unsigned char d) {
+    const float fa = __fdiv_rn(static_cast<float>(a), 255.0f), fb = __fdiv_rn(static_cast<float>(b), 255.0f);
+    const float fc = __fdiv_rn(static_cast<float>(c), 255.0f), fd = __fdiv_rn(static_cast<float>(d), 255.0f);
+    const float top = __fadd_rn(__fmul_rn(fa, bx), __fmul_rn(fb, ax));
+    const float bot = __fadd_rn(__fmul_rn(fc, bx), __fmul_rn(fd, ax));
+    return __fadd_rn(__fmul_rn(top, by), __fmul_rn(bot, ay));
+  };
+  return make_float4(ch(t00.x, t10.x, t01.x, t11.x), ch(t00.y, t10.y, t01.y, t11.y),
+                     ch(t00.z, t10.z, t01.z, t11.z), ch(t00.w, t10.w, t01.w, t11.w));
+}
+
+// decode for a material with textures: each texel multiplies its factor
+// before the clamp (baseColor, roughness, metallic, transmission, emission;
+// material.wesl:181-262).  uv: TEXCOORD_0.xy, TEXCOORD_1.xy at the hit.
+__device__ __forceinline__ Mat decodeTextured(const SceneView& sc, const DevMaterial& m,
+                                              const DevMatTex& t, float4 uv, float w,
+                                              const SmitsPos& sp) {
+  auto texel = [&](int k) {
+    const bool set1 = (t.uv1_bits >> k) & 1u;
+    return sampleMaterialTexture(sc, t.layer[k], set1 ? uv.z : uv.x, set1 ? uv.w : uv.y);
+  };
+  V3 base{m.base[0], m.base[1], m.base[2]};
+  if (t.layer[0] >= 0) {
+    const float4 c = texel(0);
+    base = V3{base.x * c.x, base.y * c.y, base.z * c.z};
+  }
+  float metallic = m.metallic, roughness = m.roughness, transmission = m.transmission;
+  if (t.layer[1] >= 0) {
+    const float4 c = texel(1);
+    roughness = wclamp(t.roughness * c.y, 0.0f, 1.0f);
+    metallic = wclamp(t.metallic * c.z, 0.0f, 1.0f);
+  }
+  if (t.layer[3] >= 0) transmission = wclamp(t.transmission * texel(3).x, 0.0f, 1.0f);
+  V3 emission{m.emission[0], m.emission[1], m.emission[2]};
+  if (t.layer[2] >= 0) {
+    const float4 c = texel(2);
+    const V3 f{t.emissive[0] * c.x, t.emissive[1] * c.y, t.emissive[2] * c.z};
+    emission = V3{fmaxf(f.x * t.emissive_strength, 0.0f), fmaxf(f.y * t.emissive_strength, 0.0f),
+                  fmaxf(f.z * t.emissive_strength, 0.0f)};
+  }
+  return decodeValues(m, base, metallic, roughness, transmission, emission, w, sp);
 }
 
 // ---- shading utilities (shading/util.wesl) ------------------------------------------

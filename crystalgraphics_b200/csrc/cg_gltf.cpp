@@ -31,6 +31,8 @@
 #include "../../include/cg_cuda.h"
 #include "cg_api_internal.h"
 
+#include "cg_png.h"
+
 namespace cg {
 namespace {
 
@@ -269,6 +271,10 @@ struct Loader {
   std::map<std::array<int64_t, 5>, uint32_t> geometry_ids;
   std::vector<cg_instance> instances;
   std::vector<cg_material> materials;
+  // decoded images (RGBA8) and one cg_texture per glTF texture pointing into them
+  std::vector<std::vector<uint8_t>> image_rgba;
+  std::vector<std::array<uint32_t, 2>> image_size;
+  std::vector<cg_texture> textures;
 
   bool fail(const std::string& m) {
     if (err.empty()) err = m;
@@ -351,6 +357,76 @@ struct Loader {
     if (!info) return -1;
     return static_cast<int32_t>(info->integer("index", -1));
   }
+  // bit `slot` of texcoord_sets: textureInfo.texCoord == 1 (textureUv, material.wesl:174-179)
+  static uint32_t texCoordBit(const Json* info, int slot) {
+    return info && info->integer("texCoord", 0) == 1 ? (1u << slot) : 0u;
+  }
+
+  // Bytes of an image: a data URI, a file next to the glTF, or a bufferView.
+  bool imageBytes(const Json& img, std::vector<uint8_t>& out) {
+    if (const Json* uri = img.get("uri")) {
+      const std::string& u = uri->s;
+      if (u.rfind("data:", 0) == 0) {
+        const size_t comma = u.find(',');
+        if (comma == std::string::npos) return fail("bad image data uri");
+        out = base64(u.substr(comma + 1));
+        return true;
+      }
+      std::ifstream f(dir + "/" + u, std::ios::binary);
+      if (!f) return fail("cannot open image " + u);
+      out.assign((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+      return true;
+    }
+    const Json* bvs = doc.get("bufferViews");
+    const int64_t bvi = img.integer("bufferView", -1);
+    if (!bvs || bvi < 0 || size_t(bvi) >= bvs->a.size()) return fail("image without uri or bufferView");
+    const Json& bv = bvs->a[bvi];
+    const int64_t bi = bv.integer("buffer", -1);
+    if (bi < 0 || size_t(bi) >= buffers.size()) return fail("bad buffer index");
+    const size_t off = size_t(bv.integer("byteOffset", 0)), len = size_t(bv.integer("byteLength", 0));
+    if (off + len > buffers[bi].size()) return fail("image bufferView exceeds its buffer");
+    out.assign(buffers[bi].begin() + off, buffers[bi].begin() + off + len);
+    return true;
+  }
+
+  // Every glTF texture: its source image decoded to RGBA8 (the reference's
+  // DecodeImageRgba8 with stb) and its sampler's wrap modes (default repeat).
+  bool loadTextures() {
+    const Json* ts = doc.get("textures");
+    if (!ts) return true;
+    const Json* imgs = doc.get("images");
+    const Json* samplers = doc.get("samplers");
+    const size_t nimg = imgs ? imgs->a.size() : 0;
+    image_rgba.assign(nimg, {});
+    image_size.assign(nimg, {0u, 0u});
+    for (size_t t = 0; t < ts->a.size(); ++t) {
+      const Json& tj = ts->a[t];
+      const int64_t src = tj.integer("source", -1);
+      if (src < 0 || size_t(src) >= nimg)
+        return fail("texture " + std::to_string(t) + " has no image source");
+      if (image_rgba[src].empty()) {
+        std::vector<uint8_t> bytes;
+        if (!imageBytes(imgs->a[src], bytes)) return false;
+        std::string e;
+        uint32_t w = 0, h = 0;
+        if (!decodePng(bytes.data(), bytes.size(), w, h, image_rgba[src], e))
+          return fail("image " + std::to_string(src) + ": " + e);
+        image_size[src] = {w, h};
+      }
+      cg_texture tx{};
+      tx.width = image_size[src][0];
+      tx.height = image_size[src][1];
+      tx.rgba8 = image_rgba[src].data();
+      tx.wrap_s = tx.wrap_t = 10497;
+      const int64_t si = tj.integer("sampler", -1);
+      if (samplers && si >= 0 && size_t(si) < samplers->a.size()) {
+        tx.wrap_s = static_cast<int32_t>(samplers->a[si].integer("wrapS", 10497));
+        tx.wrap_t = static_cast<int32_t>(samplers->a[si].integer("wrapT", 10497));
+      }
+      textures.push_back(tx);
+    }
+    return true;
+  }
 
   void loadMaterials() {
     auto def = [] {
@@ -377,11 +453,14 @@ struct Loader {
         m.roughness_factor = static_cast<float>(pbr->num("roughnessFactor", 1.0));
         m.base_color_texture = textureIndex(pbr->get("baseColorTexture"));
         m.metallic_roughness_texture = textureIndex(pbr->get("metallicRoughnessTexture"));
+        m.texcoord_sets |= texCoordBit(pbr->get("baseColorTexture"), 0) |
+                           texCoordBit(pbr->get("metallicRoughnessTexture"), 1);
       }
       if (const Json* ef = mj.get("emissiveFactor"))
         for (size_t k = 0; k < 3 && k < ef->a.size(); ++k)
           m.emissive_factor[k] = static_cast<float>(ef->a[k].n);
       m.emissive_texture = textureIndex(mj.get("emissiveTexture"));
+      m.texcoord_sets |= texCoordBit(mj.get("emissiveTexture"), 2);
       if (const Json* ext = mj.get("extensions")) {
         if (const Json* e = ext->get("KHR_materials_emissive_strength"))
           m.emissive_strength = static_cast<float>(e->num("emissiveStrength", 1.0));
@@ -392,6 +471,7 @@ struct Loader {
         if (const Json* e = ext->get("KHR_materials_transmission")) {
           m.transmission_factor = static_cast<float>(e->num("transmissionFactor", 0.0));
           m.transmission_texture = textureIndex(e->get("transmissionTexture"));
+          m.texcoord_sets |= texCoordBit(e->get("transmissionTexture"), 3);
         }
         if (const Json* e = ext->get("KHR_materials_volume"))
           m.thickness_factor = static_cast<float>(e->num("thicknessFactor", 0.0));
@@ -535,6 +615,7 @@ struct Loader {
     Parser p{json.data(), json.data() + json.size(), {}};
     if (!p.parse(doc)) return fail("invalid JSON: " + p.err);
     if (!loadBuffers(glb ? &bin : nullptr)) return false;
+    if (!loadTextures()) return false;
     loadMaterials();
     if (!loadMeshes()) return false;
     // root: Rx(+90 deg), glTF y-up -> z-up (scene.cpp:1000)
@@ -576,8 +657,23 @@ extern "C" CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void**
   d.instance_count = static_cast<uint32_t>(L->instances.size());
   d.materials = L->materials.data();
   d.material_count = static_cast<uint32_t>(L->materials.size());
+  d.textures = L->textures.data();
+  d.texture_count = static_cast<uint32_t>(L->textures.size());
   *out = d;
   *storage = L.release();
+  return CG_OK;
+}
+
+extern "C" CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* width,
+                                     uint32_t* height, uint8_t* rgba_out) {
+  if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
+  std::vector<uint8_t> rgba;
+  std::string err;
+  uint32_t w = 0, h = 0;
+  if (!decodePng(data, size, w, h, rgba, err)) return fail(CG_E_INVALID, err);
+  *width = w;
+  *height = h;
+  if (rgba_out) std::memcpy(rgba_out, rgba.data(), rgba.size());
   return CG_OK;
 }
 

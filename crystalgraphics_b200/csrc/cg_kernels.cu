@@ -510,7 +510,17 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
         s.pos = ro + t * rd;
         s.gn = wgn;
         s.sn = dot(wsn, wgn) >= 0.0f ? wsn : -wsn;
-        const Mat m = decode(sc.mat[meta.y], lambda, spos);
+        const DevMaterial& dmat = sc.mat[meta.y];
+        Mat m;
+        if (dmat.volume & kTexturedBit) {
+          // the hit's texture coordinates (bvh.wesl:172-179)
+          const float4 a = __ldg(sc.vuv + vi.x), b = __ldg(sc.vuv + vi.y), cc = __ldg(sc.vuv + vi.z);
+          const float4 uv = make_float4(w0 * a.x + u * b.x + v * cc.x, w0 * a.y + u * b.y + v * cc.y,
+                                        w0 * a.z + u * b.z + v * cc.z, w0 * a.w + u * b.w + v * cc.w);
+          m = decodeTextured(sc, dmat, sc.mattex[meta.y], uv, lambda, spos);
+        } else {
+          m = decode(dmat, lambda, spos);
+        }
         const Counts c = counts(m, sc.has_lights != 0u, depth, caps);
         Rng rng;
         seedRng(rng, key);

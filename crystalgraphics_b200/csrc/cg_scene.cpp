@@ -38,6 +38,58 @@ F3 transformPoint(const float* m, F3 p) {
 
 float luminance(F3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
 
+bool textured(const cg_material& m) {
+  return m.base_color_texture >= 0 || m.metallic_roughness_texture >= 0 || m.emissive_texture >= 0 ||
+         m.transmission_texture >= 0;
+}
+
+// ResizeRgba8Nearest (src/wgpu/resource.cpp:52-75): the source texel of each
+// target texel by integer scaling; texels packed as uint32 (r | g<<8 | b<<16 | a<<24).
+void resizeNearest(const cg_texture& t, uint32_t w, uint32_t h, uint32_t* out) {
+  for (uint32_t y = 0; y < h; ++y) {
+    const uint32_t sy = std::min(t.height - 1, static_cast<uint32_t>((uint64_t(y) * t.height) / h));
+    for (uint32_t x = 0; x < w; ++x) {
+      const uint32_t sx = std::min(t.width - 1, static_cast<uint32_t>((uint64_t(x) * t.width) / w));
+      std::memcpy(out + size_t(y) * w + x, t.rgba8 + (size_t(sy) * t.width + sx) * 4, 4);
+    }
+  }
+}
+
+// WrapCoord (emissive_buffer.h:191-204): glTF clamp to edge (33071), mirrored
+// repeat (33648), else repeat; the result is clamped below 1.
+float wrapCoord(float c, int32_t wrap) {
+  if (wrap == 33071) return std::clamp(c, 0.0f, 0.999999f);
+  if (wrap == 33648) {
+    float wrapped = c - std::floor(c);
+    const auto tile = static_cast<int32_t>(std::floor(c));
+    if (tile % 2 != 0) wrapped = 1.0f - wrapped;
+    return std::clamp(wrapped, 0.0f, 0.999999f);
+  }
+  const float wrapped = c - std::floor(c);
+  return std::clamp(wrapped, 0.0f, 0.999999f);
+}
+
+// EmissiveTextureFactor (emissive_buffer.h:138-189): the emissive texture's
+// texel (nearest, glTF wrap modes, original image) at the triangle's mean UV;
+// (1, 1, 1) without an emissive texture.
+F3 emissiveTextureFactor(const cg_scene_desc* d, const cg_material& m, const cg_vertex& v0,
+                         const cg_vertex& v1, const cg_vertex& v2) {
+  if (m.emissive_texture < 0 || static_cast<uint32_t>(m.emissive_texture) >= d->texture_count)
+    return F3{1.0f, 1.0f, 1.0f};
+  const cg_texture& t = d->textures[m.emissive_texture];
+  const bool set1 = (m.texcoord_sets >> 2) & 1u;
+  const float* a = set1 ? v0.tex_coord1 : v0.tex_coord0;
+  const float* b = set1 ? v1.tex_coord1 : v1.tex_coord0;
+  const float* c = set1 ? v2.tex_coord1 : v2.tex_coord0;
+  const float u = wrapCoord(((a[0] + b[0]) + c[0]) / 3.0f, t.wrap_s);
+  const float v = wrapCoord(((a[1] + b[1]) + c[1]) / 3.0f, t.wrap_t);
+  const uint32_t x = std::min(t.width - 1, static_cast<uint32_t>(u * static_cast<float>(t.width)));
+  const uint32_t y = std::min(t.height - 1, static_cast<uint32_t>(v * static_cast<float>(t.height)));
+  const uint8_t* px = t.rgba8 + (size_t(y) * t.width + x) * 4;
+  return F3{static_cast<float>(px[0]) / 255.0f, static_cast<float>(px[1]) / 255.0f,
+            static_cast<float>(px[2]) / 255.0f};
+}
+
 // A cut of a mesh's BVH2 of at most `target` boxes (the inner node of largest
 // surface area is replaced by its two children first).  Their union contains
 // every triangle, and transformed corner by corner they bound a rotated
@@ -184,13 +236,25 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
         return CG_E_INVALID;
       }
   }
-  for (uint32_t i = 0; i < d->material_count; ++i) {
-    const cg_material& m = d->materials[i];
-    if (m.base_color_texture >= 0 || m.metallic_roughness_texture >= 0 ||
-        m.emissive_texture >= 0 || m.transmission_texture >= 0) {
-      err = "material " + std::to_string(i) + " uses a texture; textured materials are not supported";
+  if (d->texture_count && !d->textures) {
+    err = "scene description has a null texture array with a nonzero count";
+    return CG_E_INVALID;
+  }
+  for (uint32_t t = 0; t < d->texture_count; ++t) {
+    const cg_texture& tx = d->textures[t];
+    if (tx.width == 0 || tx.height == 0 || !tx.rgba8) {
+      err = "texture " + std::to_string(t) + " has no image data";
       return CG_E_INVALID;
     }
+  }
+  for (uint32_t i = 0; i < d->material_count; ++i) {
+    const cg_material& m = d->materials[i];
+    for (int32_t t : {m.base_color_texture, m.metallic_roughness_texture, m.emissive_texture,
+                      m.transmission_texture})
+      if (t < -1 || t >= static_cast<int64_t>(d->texture_count)) {
+        err = "material " + std::to_string(i) + " names a missing texture";
+        return CG_E_INVALID;
+      }
   }
   if (d->env_rgba32f && (d->env_width == 0 || d->env_height == 0)) {
     err = "environment texture has a zero dimension";
@@ -202,6 +266,30 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
   for (uint32_t v = 0; v < d->vertex_count; ++v) {
     for (int k = 0; k < 3; ++k) s.vnormal[size_t(v) * 4 + k] = d->vertices[v].normal[k];
     s.vnormal[size_t(v) * 4 + 3] = 0.0f;
+  }
+  bool any_textured = false;
+  for (uint32_t i = 0; i < d->material_count; ++i) any_textured = any_textured || textured(d->materials[i]);
+  if (any_textured) {
+    s.vuv.resize(size_t(d->vertex_count) * 4);
+    for (uint32_t v = 0; v < d->vertex_count; ++v) {
+      const cg_vertex& vx = d->vertices[v];
+      const float uv[4] = {vx.tex_coord0[0], vx.tex_coord0[1], vx.tex_coord1[0], vx.tex_coord1[1]};
+      std::memcpy(&s.vuv[size_t(v) * 4], uv, sizeof(uv));
+    }
+  }
+  // ---- material texture array (WriteMaterialTextures, src/wgpu/resource.cpp:471-546):
+  // every texture resized (nearest) to the largest width and height, one layer each
+  if (d->texture_count) {
+    s.tex_w = 1;
+    s.tex_h = 1;
+    for (uint32_t t = 0; t < d->texture_count; ++t) {
+      s.tex_w = std::max(s.tex_w, d->textures[t].width);
+      s.tex_h = std::max(s.tex_h, d->textures[t].height);
+    }
+    s.tex_layers = d->texture_count;
+    s.tex.resize(size_t(s.tex_w) * s.tex_h * s.tex_layers);
+    for (uint32_t t = 0; t < d->texture_count; ++t)
+      resizeNearest(d->textures[t], s.tex_w, s.tex_h, s.tex.data() + size_t(t) * s.tex_w * s.tex_h);
   }
 
   // ---- one BLAS per mesh ------------------------------------------------------
@@ -278,17 +366,36 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
     dm.dispersion = m.dispersion;
     dm.transmission = clamp01(m.transmission_factor);
     dm.volume = m.thickness_factor > 0.0f ? 1u : 0u;
+    DevMatTex mt{};
+    mt.layer[0] = m.base_color_texture;
+    mt.layer[1] = m.metallic_roughness_texture;
+    mt.layer[2] = m.emissive_texture;
+    mt.layer[3] = m.transmission_texture;
+    mt.uv1_bits = m.texcoord_sets & 15u;
+    mt.metallic = m.metallic_factor;
+    mt.roughness = m.roughness_factor;
+    mt.transmission = m.transmission_factor;
+    for (int k = 0; k < 3; ++k) mt.emissive[k] = m.emissive_factor[k];
+    mt.emissive_strength = m.emissive_strength;
+    s.mattex.push_back(mt);
+    const bool tx = textured(m);
+    if (tx) dm.volume |= kTexturedBit;
+    // the lobes a hit can sample; a texture can lower metallic, transmission and
+    // roughness below their factors, so textured channels count every lobe
+    const bool mr_tex = m.metallic_roughness_texture >= 0, tr_tex = m.transmission_texture >= 0;
+    const bool diffuse = mr_tex || tr_tex || (1.0f - dm.metallic) * (1.0f - dm.transmission) > 0.0f;
+    const bool transmit = dm.transmission > 1e-6f;
     {
       uint32_t kind = 0;
-      if ((1.0f - dm.metallic) * (1.0f - dm.transmission) > 0.0f) kind |= 1u;
-      kind |= dm.roughness == 0.0f ? 2u : 4u;
-      if (dm.transmission > 1e-6f) kind |= 8u;
+      if (diffuse) kind |= 1u;
+      kind |= mr_tex ? 6u : (dm.roughness == 0.0f ? 2u : 4u);
+      if (transmit) kind |= 8u;
       dm.volume |= kind << kKindShift;
     }
     s.mat.push_back(dm);
     uint32_t lobes = 1;  // a reflection lobe
-    if ((1.0f - dm.metallic) * (1.0f - dm.transmission) > 0.0f) ++lobes;
-    if (dm.transmission > 1e-6f) ++lobes;
+    if (diffuse) ++lobes;
+    if (transmit) ++lobes;
     s.max_lobes = std::max(s.max_lobes, lobes);
   }
 
@@ -368,13 +475,16 @@ int packScene(const cg_scene_desc* d, HostScene& s, std::string& err) {
       F3 c = cross3(sub(p1, p0), sub(p2, p0));
       float area = std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z) * 0.5f;
       if (area <= 0.0f) continue;
-      float w = luminance(base);
+      const F3 f = emissiveTextureFactor(d, d->materials[inst.material], d->vertices[ix[0]],
+                                         d->vertices[ix[1]], d->vertices[ix[2]]);
+      const F3 emission{base.x * f.x, base.y * f.y, base.z * f.z};
+      float w = luminance(emission);
       if (w <= 0.0f) continue;
       DevEmissivePrim e{};
       e.v0[0] = p0.x; e.v0[1] = p0.y; e.v0[2] = p0.z;
       e.v1[0] = p1.x; e.v1[1] = p1.y; e.v1[2] = p1.z;
       e.v2[0] = p2.x; e.v2[1] = p2.y; e.v2[2] = p2.z;
-      e.emission[0] = base.x; e.emission[1] = base.y; e.emission[2] = base.z;
+      e.emission[0] = emission.x; e.emission[1] = emission.y; e.emission[2] = emission.z;
       e.area = area;
       e.weight = area * w;
       s.eprim.push_back(e);

@@ -28,6 +28,10 @@ struct HostScene {
   std::vector<DevAlias> alias;
   std::vector<DevLightTri> ltri;
   std::vector<float> env;           // 4 per texel
+  std::vector<DevMatTex> mattex;    // per material
+  std::vector<uint32_t> tex;        // RGBA8 texels of the texture array (layer-major)
+  std::vector<float> vuv;           // 4 per vertex, when a material is textured
+  uint32_t tex_w = 1, tex_h = 1, tex_layers = 0;
   uint32_t env_w = 0, env_h = 0;
   float total_weight = 0.0f;
   uint32_t mesh_count = 0, triangle_count = 0, blas_depth = 0, tlas_depth = 0;

@@ -99,7 +99,23 @@ struct alignas(16) DevMaterial {
 // (bit 0 diffuse, bit 1 specular, bit 2 rough, bit 3 transmission).  Hits are
 // grouped by kind before shading so a warp runs one path.
 constexpr uint32_t kKindShift = 8u;
+// volume bit 1: the material samples at least one texture (DevMatTex holds them)
+constexpr uint32_t kTexturedBit = 2u;
 static_assert(sizeof(DevMaterial) == 48, "DevMaterial is 48 bytes");
+
+// Texture references of a material (read only when DevMaterial has
+// kTexturedBit): the layer of each texture decode() samples (-1 = none), in
+// the order base color, metallic-roughness, emissive, transmission; bit k of
+// uv1_bits selects TEXCOORD_1 for texture k; and the unclamped factors the
+// texels multiply (material.wesl:181-262).
+struct alignas(16) DevMatTex {
+  int32_t layer[4];
+  uint32_t uv1_bits;
+  float metallic, roughness, transmission;  // factors before the clamp
+  float emissive[3];                        // emissive_factor
+  float emissive_strength;
+};
+static_assert(sizeof(DevMatTex) == 48, "DevMatTex is 48 bytes");
 
 // Emissive triangle for the light-pdf sum (pdf/emission.wesl:120-179):
 // v0, e1, e2, the normalised light normal and max(weight / area, 1e-3).
@@ -150,6 +166,10 @@ struct SceneView {
   const BvhNode* light_bvh;    // over DevLightTri
   const DevLightTri* light_tri;
   const float4* env;           // env_w * env_h texels
+  const DevMatTex* mattex;     // per material (textured materials only read it)
+  const uchar4* tex;           // tex_layers x tex_h x tex_w RGBA8 texels
+  const float4* vuv;           // per vertex: TEXCOORD_0.xy, TEXCOORD_1.xy (textured scenes)
+  uint32_t tex_w, tex_h, tex_layers, _tex_pad;
   uint32_t env_w, env_h;
   uint32_t emissive_count;
   uint32_t instance_count;

@@ -20,6 +20,8 @@ import os
 
 import numpy as np
 
+from . import png
+
 _RX_NEG90 = np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, -1, 0, 0], [0, 0, 0, 1]], np.float64)
 
 
@@ -58,9 +60,33 @@ def write(scene, path: str) -> str:
         nv = add(nrm, 34962)
         accessors.append({"bufferView": nv, "componentType": 5126, "count": vc, "type": "VEC3"})
         na = len(accessors) - 1
+        uv_acc = []
+        for key in ("tex_coord0", "tex_coord1"):
+            uv = np.ascontiguousarray(v[key], np.float32)
+            if vc and np.any(uv != 0):
+                uvv = add(uv, 34962)
+                accessors.append({"bufferView": uvv, "componentType": 5126, "count": vc,
+                                  "type": "VEC2"})
+                uv_acc.append(len(accessors) - 1)
+            else:
+                uv_acc.append(None)
         iv = add(idx.astype(np.uint32), 34963)
         accessors.append({"bufferView": iv, "componentType": 5125, "count": ic, "type": "SCALAR"})
-        mesh_acc.append((pa, na, len(accessors) - 1))
+        mesh_acc.append((pa, na, len(accessors) - 1, uv_acc))
+
+    # textures: one PNG image (in the binary buffer), one sampler per texture
+    images, samplers, textures = [], [], []
+    for img, wrap_s, wrap_t in getattr(scene, "textures", []) or []:
+        bv = add(np.frombuffer(png.encode_rgba8(img), np.uint8))
+        images.append({"bufferView": bv, "mimeType": "image/png"})
+        samplers.append({"wrapS": int(wrap_s), "wrapT": int(wrap_t)})
+        textures.append({"source": len(images) - 1, "sampler": len(samplers) - 1})
+
+    def tex_info(m, field, slot):
+        t = int(m[field])
+        if t < 0:
+            return None
+        return {"index": t, "texCoord": int((int(m["texcoord_sets"]) >> slot) & 1)}
 
     materials = []
     for m in scene.materials:
@@ -69,14 +95,24 @@ def write(scene, path: str) -> str:
             "metallicFactor": float(m["metallic_factor"]),
             "roughnessFactor": float(m["roughness_factor"])},
             "emissiveFactor": [float(x) for x in m["emissive_factor"]]}
+        pbr = mat["pbrMetallicRoughness"]
+        if tex_info(m, "base_color_texture", 0):
+            pbr["baseColorTexture"] = tex_info(m, "base_color_texture", 0)
+        if tex_info(m, "metallic_roughness_texture", 1):
+            pbr["metallicRoughnessTexture"] = tex_info(m, "metallic_roughness_texture", 1)
+        if tex_info(m, "emissive_texture", 2):
+            mat["emissiveTexture"] = tex_info(m, "emissive_texture", 2)
         ext = {}
         if float(m["emissive_strength"]) != 1.0:
             ext["KHR_materials_emissive_strength"] = {"emissiveStrength": float(m["emissive_strength"])}
         ext["KHR_materials_ior"] = {"ior": float(m["ior"])}
         if float(m["dispersion"]):
             ext["KHR_materials_dispersion"] = {"dispersion": float(m["dispersion"])}
-        if float(m["transmission_factor"]):
+        if float(m["transmission_factor"]) or int(m["transmission_texture"]) >= 0:
             ext["KHR_materials_transmission"] = {"transmissionFactor": float(m["transmission_factor"])}
+            if tex_info(m, "transmission_texture", 3):
+                ext["KHR_materials_transmission"]["transmissionTexture"] = \
+                    tex_info(m, "transmission_texture", 3)
         if float(m["thickness_factor"]):
             ext["KHR_materials_volume"] = {"thicknessFactor": float(m["thickness_factor"])}
         mat["extensions"] = ext
@@ -87,8 +123,12 @@ def write(scene, path: str) -> str:
     for inst in scene.instances:
         key = (int(inst["mesh"]), int(inst["material"]))
         if key not in mesh_of:
-            pa, na, ia = mesh_acc[key[0]]
-            gl_meshes.append({"primitives": [{"attributes": {"POSITION": pa, "NORMAL": na},
+            pa, na, ia, uv_acc = mesh_acc[key[0]]
+            attrs = {"POSITION": pa, "NORMAL": na}
+            for k, a in enumerate(uv_acc):
+                if a is not None:
+                    attrs[f"TEXCOORD_{k}"] = a
+            gl_meshes.append({"primitives": [{"attributes": attrs,
                                               "indices": ia, "material": key[1], "mode": 4}]})
             mesh_of[key] = len(gl_meshes) - 1
         W = np.eye(4)
@@ -106,6 +146,8 @@ def write(scene, path: str) -> str:
         "meshes": gl_meshes, "nodes": nodes, "scenes": [{"nodes": list(range(len(nodes)))}],
         "scene": 0,
     }
+    if textures:
+        doc.update(images=images, samplers=samplers, textures=textures)
     with open(bin_path, "wb") as f:
         for b in blobs:
             f.write(b)

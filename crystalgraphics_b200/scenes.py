@@ -52,7 +52,10 @@ class Scene:
     env: np.ndarray | None = None
     camera: object = None
     conf: dict = field(default_factory=dict)
+    # material textures: (rgba8 uint8 array (h, w, 4), wrap_s, wrap_t) per glTF texture
+    textures: list = field(default_factory=list)
     _desc: object = None
+    _tex: object = None
 
     def desc(self) -> _abi.CgSceneDesc:
         """A cg_scene_desc pointing into this object's arrays (keep self alive)."""
@@ -73,6 +76,17 @@ class Scene:
             assert self.env.dtype == np.float32 and self.env.ndim == 3 and self.env.shape[2] == 4
             d.env_rgba32f = self.env.ctypes.data
             d.env_height, d.env_width = self.env.shape[0], self.env.shape[1]
+        if self.textures:
+            arr = (_abi.CgTexture * len(self.textures))()
+            for k, (img, ws, wt) in enumerate(self.textures):
+                assert img.dtype == np.uint8 and img.ndim == 3 and img.shape[2] == 4
+                assert img.flags["C_CONTIGUOUS"]
+                arr[k].height, arr[k].width = img.shape[0], img.shape[1]
+                arr[k].rgba8 = img.ctypes.data
+                arr[k].wrap_s, arr[k].wrap_t = ws, wt
+            d.textures = C.cast(arr, C.c_void_p)
+            d.texture_count = len(self.textures)
+            self._tex = arr
         self._desc = d
         return d
 
@@ -88,16 +102,21 @@ class _Builder:
         self.meshes = []
         self.instances = []
         self.materials = []
+        self.textures = []
         self.nv = 0
         self.ni = 0
 
-    def add_mesh(self, positions, normals, tris) -> int:
+    def add_mesh(self, positions, normals, tris, uv0=None, uv1=None) -> int:
         positions = np.asarray(positions, np.float32)
         normals = np.asarray(normals, np.float32)
         tris = np.asarray(tris, np.uint32).reshape(-1)
         v = np.zeros(len(positions), _abi.VERTEX_DTYPE)
         v["position"] = positions
         v["normal"] = normals
+        if uv0 is not None:
+            v["tex_coord0"] = np.asarray(uv0, np.float32)
+        if uv1 is not None:
+            v["tex_coord1"] = np.asarray(uv1, np.float32)
         self.verts.append(v)
         self.idx.append(tris + np.uint32(self.nv))
         self.meshes.append((self.nv, len(positions), self.ni, len(tris)))
@@ -106,7 +125,10 @@ class _Builder:
         return len(self.meshes) - 1
 
     def add_material(self, base=(1, 1, 1), metallic=0.0, roughness=1.0, ior=1.5, dispersion=0.0,
-                     transmission=0.0, thickness=0.0, emissive=(0, 0, 0), strength=1.0) -> int:
+                     transmission=0.0, thickness=0.0, emissive=(0, 0, 0), strength=1.0,
+                     textures=None, texcoord_sets=0) -> int:
+        """textures: optional dict of base_color / metallic_roughness / emissive /
+        transmission -> texture index; texcoord_sets: bit k selects TEXCOORD_1."""
         m = np.zeros(1, _abi.MATERIAL_DTYPE)
         m["base_color_factor"] = [base[0], base[1], base[2], 1.0]
         m["emissive_factor"] = emissive
@@ -119,7 +141,8 @@ class _Builder:
         m["thickness_factor"] = thickness
         for k in ("base_color_texture", "metallic_roughness_texture", "emissive_texture",
                   "transmission_texture"):
-            m[k] = -1
+            m[k] = (textures or {}).get(k.replace("_texture", ""), -1)
+        m["texcoord_sets"] = texcoord_sets
         self.materials.append(m)
         return len(self.materials) - 1
 
@@ -132,6 +155,11 @@ class _Builder:
         inst["material"] = material
         self.instances.append(inst)
 
+    def add_texture(self, rgba8, wrap_s=10497, wrap_t=10497) -> int:
+        """An RGBA8 image (h, w, 4) as a material texture (glTF wrap modes)."""
+        self.textures.append((np.ascontiguousarray(rgba8, np.uint8), int(wrap_s), int(wrap_t)))
+        return len(self.textures) - 1
+
     def build(self, name, camera, conf, env=None) -> Scene:
         meshes = np.array(self.meshes, np.uint32).reshape(-1, 4).copy().view(_abi.MESH_DTYPE).reshape(-1)
         return Scene(name=name,
@@ -140,7 +168,7 @@ class _Builder:
                      meshes=np.ascontiguousarray(meshes),
                      instances=np.ascontiguousarray(np.concatenate(self.instances)),
                      materials=np.ascontiguousarray(np.concatenate(self.materials)),
-                     env=env, camera=camera, conf=conf)
+                     env=env, camera=camera, conf=conf, textures=list(self.textures))
 
 
 def _quad(p0, p1, p2, p3):
@@ -213,6 +241,70 @@ def cornell(width=256, height=256, spp=1, depth=2) -> Scene:
                    light)
     cam = _abi.make_camera((0.0, -3.4, 1.0), (0.0, 1.0, 0.0), camera_viewport(width, height, 0.42))
     return b.build("cornell", cam, dict(width=width, height=height, spp=spp, depth=depth))
+
+
+def _quad_uv(scale=1.0, offset=0.0):
+    """UVs of _quad's four corners."""
+    return np.array([(0, 0), (1, 0), (1, 1), (0, 1)], np.float32) * scale + offset
+
+
+def _texture(rng, h, w, kind):
+    """Seeded procedural RGBA8 images for the textured scene."""
+    y, x = np.mgrid[0:h, 0:w]
+    img = np.zeros((h, w, 4), np.uint8)
+    img[..., 3] = 255
+    if kind == "checker":
+        c = ((x // 8 + y // 8) % 2).astype(bool)
+        img[..., 0] = np.where(c, 230, 40)
+        img[..., 1] = np.where(c, 200, 90)
+        img[..., 2] = np.where(c, 60, 210)
+    elif kind == "gradient":   # g: roughness, b: metallic (glTF metallicRoughness)
+        img[..., 1] = (255 * x / max(w - 1, 1)).astype(np.uint8)
+        img[..., 2] = (255 * y / max(h - 1, 1)).astype(np.uint8)
+    else:                      # random texels
+        img[..., :3] = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+    return img
+
+
+def textured_cornell(width=96, height=96, spp=2, depth=4) -> Scene:
+    """The Cornell room with material textures of different sizes (resized to
+    the largest into one array): a checkered base color on the floor and back
+    wall with UVs reaching past [0, 1] (clamp to edge when shading, wrap modes
+    in the light buffer), a metallic-roughness gradient on the metal box read
+    through TEXCOORD_1, a random-texel emissive texture on the ceiling light
+    and a transmission texture on a glass box."""
+    rng = np.random.default_rng(7)
+    b = _Builder()
+    checker = b.add_texture(_texture(rng, 64, 64, "checker"))
+    mr = b.add_texture(_texture(rng, 16, 32, "gradient"), 33071, 33071)
+    emis = b.add_texture(_texture(rng, 8, 8, "random"), 33648, 10497)
+    trans = b.add_texture(_texture(rng, 24, 16, "random"))
+    white_tex = b.add_material(base=(0.9, 0.9, 0.9), textures={"base_color": checker})
+    red = b.add_material(base=(0.63, 0.06, 0.05))
+    green = b.add_material(base=(0.14, 0.45, 0.09))
+    metal = b.add_material(base=(0.95, 0.95, 0.95), metallic=1.0, roughness=0.8,
+                           textures={"metallic_roughness": mr}, texcoord_sets=0b10)
+    glass = b.add_material(base=(1, 1, 1), roughness=0.0, ior=1.5, transmission=1.0, thickness=1.0,
+                           textures={"transmission": trans})
+    light = b.add_material(base=(0, 0, 0), emissive=(1, 1, 1), strength=15.0,
+                           textures={"emissive": emis})
+    floor = _quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
+    back = _quad((-1, 1, 0), (1, 1, 0), (1, 1, 2), (-1, 1, 2))
+    b.add_instance(b.add_mesh(*floor, uv0=_quad_uv(1.6, -0.3)), white_tex)
+    b.add_instance(b.add_mesh(*back, uv0=_quad_uv(1.0)), white_tex)
+    b.add_instance(b.add_mesh(*_quad((-1, -1, 2), (-1, 1, 2), (1, 1, 2), (1, -1, 2))), red)
+    b.add_instance(b.add_mesh(*_quad((-1, -1, 0), (-1, 1, 0), (-1, 1, 2), (-1, -1, 2))), red)
+    b.add_instance(b.add_mesh(*_quad((1, -1, 0), (1, -1, 2), (1, 1, 2), (1, 1, 0))), green)
+    P, N, T = _cube()
+    uv = np.tile(_quad_uv(1.0), (6, 1))
+    cube_uv = b.add_mesh(P, N, T, uv0=uv, uv1=uv[:, ::-1].copy())
+    b.add_instance(cube_uv, metal, _trs((0.6, 0.6, 0.6), -0.3, (0.4, -0.3, 0.3)))
+    b.add_instance(cube_uv, glass, _trs((0.5, 0.5, 0.9), 0.4, (-0.4, 0.2, 0.45)))
+    h = 0.3
+    b.add_instance(b.add_mesh(*_quad((-h, -h, 1.999), (-h, h, 1.999), (h, h, 1.999), (h, -h, 1.999)),
+                              uv0=_quad_uv(2.5, -0.7)), light)
+    cam = _abi.make_camera((0.0, -3.4, 1.0), (0.0, 1.0, 0.0), camera_viewport(width, height, 0.42))
+    return b.build("textured_cornell", cam, dict(width=width, height=height, spp=spp, depth=depth))
 
 
 # ---------------------------------------------------------------------------

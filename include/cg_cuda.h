@@ -106,8 +106,10 @@ typedef struct cg_instance {
 
 /* The material fields the path tracer reads out of the reference's
  * PackedMaterial (src/material.h:30-87, shading/material.wesl:19-53).
- * Texture references are glTF texture indices (-1 = none); this backend
- * renders untextured scenes and rejects materials that name a texture. */
+ * Texture references index cg_scene_desc.textures (-1 = none), the four
+ * textures decode() samples (material.wesl:181-262); bit k of texcoord_sets
+ * selects TEXCOORD_1 instead of TEXCOORD_0 for texture k in this order:
+ * base color, metallic-roughness, emissive, transmission. */
 typedef struct cg_material {
   float base_color_factor[4];
   float emissive_factor[3];
@@ -122,8 +124,23 @@ typedef struct cg_material {
   int32_t metallic_roughness_texture;
   int32_t emissive_texture;
   int32_t transmission_texture;
-  uint32_t _pad[2];
+  uint32_t texcoord_sets;
+  uint32_t _pad;
 } cg_material;
+
+/* A decoded material texture (the reference's TextureData after
+ * DecodeImageRgba8, src/image_decode.h:27): RGBA8 rows, top row first.
+ * wrap_s / wrap_t are the glTF sampler wrap modes (33071 clamp to edge,
+ * 33648 mirrored repeat, other = repeat); the reference uses them only for
+ * the emissive-texture factor of its light buffer (emissive_buffer.h:150-200)
+ * and samples every texture with clamp to edge when shading
+ * (src/wgpu/resource.cpp:133-142). */
+typedef struct cg_texture {
+  uint32_t width, height;
+  const uint8_t* rgba8;
+  int32_t wrap_s, wrap_t;
+  uint32_t _pad[2];
+} cg_texture;
 
 /* env_rgba32f == NULL selects the reference's fallback sky: a 512x256
  * vertical gradient (src/pathtracing/scene_data.h:73-98). */
@@ -140,6 +157,8 @@ typedef struct cg_scene_desc {
   uint32_t material_count;
   const float* env_rgba32f;
   uint32_t env_width, env_height;
+  const cg_texture* textures;  /* material textures (may be NULL when count is 0) */
+  uint32_t texture_count;
 } cg_scene_desc;
 
 typedef struct cg_scene_s* cg_scene_t;
@@ -176,6 +195,12 @@ CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out);
  * with arrays owned by *storage, released by cg_gltf_free. */
 CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage);
 CG_API int cg_gltf_free(void* storage);
+/* Decodes a PNG file image to RGBA8 (the reference decodes glTF images with
+ * stb_image, src/image_decode.cpp:12-45; JPEG is not supported here).  With
+ * rgba_out == NULL only *width and *height are set; otherwise rgba_out must
+ * hold width * height * 4 bytes. */
+CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* width, uint32_t* height,
+                         uint8_t* rgba_out);
 
 typedef struct cg_scene_info {
   uint32_t instance_count, mesh_count, triangle_count, material_count;

@@ -60,12 +60,22 @@ struct Material {        // the fields shading/material.wesl:19-53 reads
   V3 base_color;
   V3 emissive;
   float emissive_strength, metallic, roughness, ior, dispersion, transmission, thickness;
+  // MaterialTextureInfo index (-1 none) and tex_coord of the four textures
+  // decode samples: base color, metallic-roughness, emissive, transmission
+  int32_t tex[4];
+  uint32_t tex_coord[4];
 };
 
 }  // namespace
 }  // namespace oracle
 
 struct oracle_scene_s {
+  // the material texture array (WriteMaterialTextures, src/wgpu/resource.cpp:
+  // 471-546): RGBA8 texels, every texture resized to the largest width/height
+  std::vector<uint8_t> tex;
+  uint32_t tex_w = 1, tex_h = 1;
+  std::vector<cg_texture> tex_desc;             // the decoded images as given
+  std::vector<std::vector<uint8_t>> tex_data;   // copies of their texels
   std::vector<cg_vertex> vertices;
   std::vector<uint32_t> indices;
   std::vector<cg_mesh> meshes;
@@ -298,6 +308,41 @@ AABB transAabb(const AABB& a, const float* m) {
 // ---- emissive buffer (src/pathtracing/emissive_buffer.h:44-100) ------------------
 float luminanceRgb(V3 c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
 
+// WrapCoord (emissive_buffer.h:191-204)
+float wrapCoord(float coord, int32_t wrap) {
+  if (wrap == 33071) return std::clamp(coord, 0.0f, 0.999999f);
+  if (wrap == 33648) {
+    float wrapped = coord - std::floor(coord);
+    const auto tile = static_cast<int32_t>(std::floor(coord));
+    if (tile % 2 != 0) wrapped = 1.0f - wrapped;
+    return std::clamp(wrapped, 0.0f, 0.999999f);
+  }
+  float wrapped = coord - std::floor(coord);
+  return std::clamp(wrapped, 0.0f, 0.999999f);
+}
+
+// EmissiveTextureFactor / TriangleUv / SampleTexture (emissive_buffer.h:138-189):
+// nearest texel of the original image at the triangle's mean UV.
+V3 emissiveTextureFactor(const oracle_scene_s& s, const Material& m, const cg_vertex& v0,
+                         const cg_vertex& v1, const cg_vertex& v2) {
+  if (m.tex[2] < 0) return V3{1.0f, 1.0f, 1.0f};
+  const size_t idx = static_cast<size_t>(m.tex[2]);
+  if (idx >= s.tex_desc.size()) return V3{1.0f, 1.0f, 1.0f};
+  const cg_texture& t = s.tex_desc[idx];
+  const bool one = m.tex_coord[2] == 1u;
+  const float* a = one ? v0.tex_coord1 : v0.tex_coord0;
+  const float* b = one ? v1.tex_coord1 : v1.tex_coord0;
+  const float* c = one ? v2.tex_coord1 : v2.tex_coord0;
+  float u = ((a[0] + b[0]) + c[0]) / 3.0f, v = ((a[1] + b[1]) + c[1]) / 3.0f;
+  u = wrapCoord(u, t.wrap_s);
+  v = wrapCoord(v, t.wrap_t);
+  const uint32_t x = std::min(t.width - 1, static_cast<uint32_t>(u * static_cast<float>(t.width)));
+  const uint32_t y = std::min(t.height - 1, static_cast<uint32_t>(v * static_cast<float>(t.height)));
+  const uint8_t* px = s.tex_data[idx].data() + (size_t(y) * t.width + x) * 4;
+  return V3{static_cast<float>(px[0]) / 255.0f, static_cast<float>(px[1]) / 255.0f,
+            static_cast<float>(px[2]) / 255.0f};
+}
+
 void buildEmissive(oracle_scene_s& s) {
   for (size_t p = 0; p < s.inst_desc.size(); ++p) {
     const cg_instance& inst = s.inst_desc[p];
@@ -315,7 +360,11 @@ void buildEmissive(oracle_scene_s& s) {
       V3 c = cross(p1 - p0, p2 - p0);
       float area = std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z) * 0.5f;
       if (area <= 0.0f) continue;
-      V3 emission = base;  // untextured: EmissiveTextureFactor == 1 (emissive_buffer.h:106-109)
+      const cg_vertex& va = s.vertices[s.indices[o]];
+      const cg_vertex& vb = s.vertices[s.indices[o + 1]];
+      const cg_vertex& vc = s.vertices[s.indices[o + 2]];
+      V3 f = emissiveTextureFactor(s, m, va, vb, vc);
+      V3 emission = V3{base.x * f.x, base.y * f.y, base.z * f.z};
       float w = luminanceRgb(emission);
       if (w <= 0.0f) continue;
       cg_emissive_prim e;
@@ -518,6 +567,7 @@ ClosestHit traverse(const oracle_scene_s& s, const Ray& ray, bool prune, Counter
 struct SurfacePos {     // structural/types.wesl:8-14
   V3 pos, shading_norm, geometry_norm;
   uint32_t material_idx;
+  float uv[2][2];        // TEXCOORD_0, TEXCOORD_1 at the hit
 };
 struct HitInfo {
   bool hit;
@@ -548,6 +598,11 @@ HitInfo rayHit(const oracle_scene_s& s, const Ray& ray, bool prune, Counters& cn
   out.sp.shading_norm = dot(wsn, wgn) >= 0.0f ? wsn : -wsn;
   out.sp.geometry_norm = wgn;
   out.sp.material_idx = inst.material_idx;
+  // uv0 = w0 * uv00 + u * uv01 + v * uv02, likewise uv1 (bvh.wesl:172-179)
+  for (int k = 0; k < 2; ++k) {
+    out.sp.uv[0][k] = (w0 * a.tex_coord0[k] + h.u * b.tex_coord0[k]) + h.v * c.tex_coord0[k];
+    out.sp.uv[1][k] = (w0 * a.tex_coord1[k] + h.u * b.tex_coord1[k]) + h.v * c.tex_coord1[k];
+  }
   return out;
 }
 
@@ -562,13 +617,60 @@ struct MatEval {         // Material (material.wesl:60-67)
   float emission;
 };
 
-// decode (material.wesl:19-53) for untextured materials.
-MatEval decode(const Material& m, float w) {
+// textureSampleLevel(material_textures, sampler, uv, layer, 0.0) with linear
+// filtering and clamp to edge (src/wgpu/resource.cpp:133-142) on the RGBA8Unorm
+// array: texel centres at (i + 0.5) / size, bilinear weights in float.  x and
+// y are clamped to [-1, size] first (every tap beyond is the edge texel).  The
+// GPU's texture units quantise the weights (to 1/256 on NVIDIA hardware); this
+// backend and its kernels use float weights (a documented deviation).
+struct Texel {
+  float r, g, b, a;
+};
+Texel sampleTexture(const oracle_scene_s& s, int32_t layer, float u, float v) {
+  const float W = static_cast<float>(s.tex_w), H = static_cast<float>(s.tex_h);
+  const float x = std::fmin(std::fmax(u * W - 0.5f, -1.0f), W);
+  const float y = std::fmin(std::fmax(v * H - 0.5f, -1.0f), H);
+  const float fx = std::floor(x), fy = std::floor(y);
+  const float ax = x - fx, ay = y - fy;
+  const int wmax = static_cast<int>(s.tex_w) - 1, hmax = static_cast<int>(s.tex_h) - 1;
+  const int x0 = std::clamp(static_cast<int>(fx), 0, wmax), x1 = std::clamp(static_cast<int>(fx) + 1, 0, wmax);
+  const int y0 = std::clamp(static_cast<int>(fy), 0, hmax), y1 = std::clamp(static_cast<int>(fy) + 1, 0, hmax);
+  const uint8_t* L = s.tex.data() + size_t(layer) * s.tex_w * s.tex_h * 4;
+  auto at = [&](int x, int y, int c) {
+    return static_cast<float>(L[(size_t(y) * s.tex_w + x) * 4 + c]) / 255.0f;
+  };
+  const float bx = 1.0f - ax, by = 1.0f - ay;
+  float out[4];
+  for (int c = 0; c < 4; ++c) {
+    const float top = at(x0, y0, c) * bx + at(x1, y0, c) * ax;
+    const float bot = at(x0, y1, c) * bx + at(x1, y1, c) * ax;
+    out[c] = top * by + bot * ay;
+  }
+  return Texel{out[0], out[1], out[2], out[3]};
+}
+
+// decode (material.wesl:19-53) with the texture getters (material.wesl:181-262).
+MatEval decode(const oracle_scene_s& s, const Material& m, const float (&uv)[2][2], float w) {
+  auto texel = [&](int k) {
+    const uint32_t set = m.tex_coord[k] == 1u ? 1u : 0u;  // textureUv
+    return sampleTexture(s, m.tex[k], uv[set][0], uv[set][1]);
+  };
   V3 base = m.base_color;
+  if (m.tex[0] >= 0) {
+    const Texel t = texel(0);
+    base = V3{base.x * t.r, base.y * t.g, base.z * t.b};
+  }
   float reflectance = rgbToWavelengthReflectance(base, w);
-  float roughness = wclamp(m.roughness, 0.0f, 1.0f);
-  float metallic = wclamp(m.metallic, 0.0f, 1.0f);
-  float transmission = wclamp(m.transmission, 0.0f, 1.0f);
+  float roughness_f = m.roughness, metallic_f = m.metallic, transmission_f = m.transmission;
+  if (m.tex[1] >= 0) {
+    const Texel t = texel(1);
+    roughness_f = roughness_f * t.g;
+    metallic_f = metallic_f * t.b;
+  }
+  if (m.tex[3] >= 0) transmission_f = transmission_f * texel(3).r;
+  float roughness = wclamp(roughness_f, 0.0f, 1.0f);
+  float metallic = wclamp(metallic_f, 0.0f, 1.0f);
+  float transmission = wclamp(transmission_f, 0.0f, 1.0f);
   float raw_ior = m.ior;
   float real_ior = raw_ior;
   if (metallic == 0.0f && transmission > 0.0f) {
@@ -582,7 +684,12 @@ MatEval decode(const Material& m, float w) {
   float im = std::sqrt(wclamp((4.0f * real_ior) / (1.0f - reflectance) -
                                   std::pow(real_ior + 1.0f, 2.0f),
                               0.0f, 10.0f));
-  V3 raw_emission = vmax(m.emissive * m.emissive_strength, V3{0.0f, 0.0f, 0.0f});
+  V3 strength = m.emissive;
+  if (m.tex[2] >= 0) {
+    const Texel t = texel(2);
+    strength = V3{strength.x * t.r, strength.y * t.g, strength.z * t.b};
+  }
+  V3 raw_emission = vmax(strength * m.emissive_strength, V3{0.0f, 0.0f, 0.0f});
   MatEval e;
   e.diffuse_reflectance = (1.0f - metallic) * (1.0f - transmission) * reflectance;
   e.microfacet_roughness = roughness * roughness;
@@ -1053,7 +1160,7 @@ float trace(TraceCtx& tc, const Ray& ray, float w, int depth, uint32_t key) {
     rng = &node_rng;
   }
   const Material& mat = s.materials[hi.sp.material_idx];
-  MatEval m = decode(mat, w);
+  MatEval m = decode(s, mat, hi.sp.uv, w);
   Counts c = counts(m, !s.alias.empty(), depth, tc.conf);
   Sample smp = sampleModels(s, ray.dir, w, hi.sp, m, c, *rng);
   float emission = m.emission;
@@ -1146,7 +1253,39 @@ oracle_scene_t oracle_scene_create(const cg_scene_desc* d) {
     om.dispersion = m.dispersion;
     om.transmission = m.transmission_factor;
     om.thickness = m.thickness_factor;
+    const int32_t tex[4] = {m.base_color_texture, m.metallic_roughness_texture, m.emissive_texture,
+                            m.transmission_texture};
+    for (int k = 0; k < 4; ++k) {
+      om.tex[k] = tex[k];
+      om.tex_coord[k] = (m.texcoord_sets >> k) & 1u;
+    }
     s->materials.push_back(om);
+  }
+  for (uint32_t t = 0; t < d->texture_count; ++t) {
+    const cg_texture& tx = d->textures[t];
+    s->tex_desc.push_back(tx);
+    s->tex_data.emplace_back(tx.rgba8, tx.rgba8 + size_t(tx.width) * tx.height * 4);
+    s->tex_w = std::max(s->tex_w, tx.width);
+    s->tex_h = std::max(s->tex_h, tx.height);
+  }
+  if (d->texture_count) {
+    // ResizeRgba8Nearest (src/wgpu/resource.cpp:52-75) into one layer per texture
+    const size_t layer = size_t(s->tex_w) * s->tex_h * 4;
+    s->tex.resize(layer * d->texture_count);
+    for (uint32_t t = 0; t < d->texture_count; ++t) {
+      const cg_texture& tx = s->tex_desc[t];
+      const uint8_t* src = s->tex_data[t].data();
+      for (uint32_t y = 0; y < s->tex_h; ++y) {
+        const uint32_t sy = std::min(tx.height - 1,
+                                     static_cast<uint32_t>((uint64_t(y) * tx.height) / s->tex_h));
+        for (uint32_t x = 0; x < s->tex_w; ++x) {
+          const uint32_t sx = std::min(tx.width - 1,
+                                       static_cast<uint32_t>((uint64_t(x) * tx.width) / s->tex_w));
+          std::memcpy(&s->tex[t * layer + (size_t(y) * s->tex_w + x) * 4],
+                      src + (size_t(sy) * tx.width + sx) * 4, 4);
+        }
+      }
+    }
   }
   for (const auto& mesh : s->meshes) blasBuildMesh(*s, mesh);
   // TLAS over instances in scene order (tlas.h:34-77)

@@ -94,3 +94,26 @@ def test_cxx_layer_reports_errors_through_expected(tmp_path):
                        capture_output=True, text=True)
     assert r.returncode == 1
     assert ("EnvInit" in r.stderr) or ("LoadScene" in r.stderr)
+
+
+def test_gltf_textures_round_trip(tmp_path):
+    """Images (PNG in the binary buffer), samplers' wrap modes, textures, the
+    materials' texture references and TEXCOORD_0/1 survive write -> parse; the
+    parsed scene packs the same light buffer in the oracle."""
+    s = scenes.textured_cornell()
+    p = B.parse_gltf(gltf.write(s, str(tmp_path / "t.gltf")))
+    assert len(p.textures) == len(s.textures) == 4
+    for (a, ws, wt), (b, ws2, wt2) in zip(s.textures, p.textures):
+        assert np.array_equal(a, b) and (ws, wt) == (ws2, wt2)
+    for f in ("base_color_texture", "metallic_roughness_texture", "emissive_texture",
+              "transmission_texture", "texcoord_sets"):
+        np.testing.assert_array_equal(p.materials[f][1:], s.materials[f], err_msg=f)
+    for k in range(len(s.instances)):
+        a, b = s.meshes[s.instances[k]["mesh"]], p.meshes[p.instances[k]["mesh"]]
+        va = s.vertices[a["vertex_offset"]:a["vertex_offset"] + a["vertex_count"]]
+        vb = p.vertices[b["vertex_offset"]:b["vertex_offset"] + b["vertex_count"]]
+        assert va["tex_coord0"].tobytes() == vb["tex_coord0"].tobytes()
+        assert va["tex_coord1"].tobytes() == vb["tex_coord1"].tobytes()
+    a, aa, _ = O.OracleScene(s).emissive()
+    b, ba, _ = O.OracleScene(p).emissive()
+    assert a.tobytes() == b.tobytes() and aa.tobytes() == ba.tobytes()

@@ -32,6 +32,7 @@ SCENES = {
     "cornell": lambda: scenes.cornell(),
     "icosphere_s5": lambda: scenes.icosphere_scene(subdiv=5, width=160, height=90),
     "instanced_small": lambda: small_instanced(),
+    "textured": lambda: scenes.textured_cornell(),
 }
 
 
@@ -65,7 +66,7 @@ def test_closest_hits_bit_exact(name, nodes):
     assert hit_frac > 0.2
 
 
-@pytest.mark.parametrize("name", ["icosphere_s5", "instanced_small"])
+@pytest.mark.parametrize("name", ["icosphere_s5", "instanced_small", "textured"])
 def test_emissive_buffer_and_alias_bit_exact(name):
     s = SCENES[name]()
     g = B.LoadScene(s)
@@ -98,6 +99,7 @@ KEYED = [
     ("cornell_d6", lambda: scenes.cornell(), 96, 96, 4, 6, 0.995),
     ("icosphere_d8", lambda: scenes.icosphere_scene(subdiv=4), 96, 54, 4, 8, 0.995),
     ("instanced_d5", lambda: small_instanced(), 96, 64, 2, 5, 0.995),
+    ("textured_d4", lambda: scenes.textured_cornell(), 96, 96, 2, 4, 0.995),
 ]
 
 
