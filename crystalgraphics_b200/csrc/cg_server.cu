@@ -1,12 +1,14 @@
 // cg_server.cu — the served form: render requests over resident scenes.
 //
-// A worker thread owns one Renderer (stream, ray queues).  Requests wait in
-// a FIFO until their film plus their share of path state fits the HBM budget,
-// then join the active set.  Every loop iteration builds one wavefront chunk
-// for one scene out of slices of all its active requests (each gets an equal
-// share of the chunk, the rest is filled first-come first-served), so
-// requests that arrive while others are on the GPU start with the next chunk
-// and share the device with them (continuous batching).  A request finishes
+// A worker thread owns two pipelines ("lanes", each a Renderer with its own
+// stream and ray queues).  Requests wait in a FIFO until their film plus
+// their share of path state fits the HBM budget, then join the active set.
+// Each idle lane gets one wavefront chunk for one scene, made of slices of
+// all that scene's active requests (each gets an equal share of the chunk,
+// the rest is filled first-come first-served), so requests that arrive while
+// others are on the GPU start with the next chunk and share the device with
+// them (continuous batching); with two chunks in flight the host builds and
+// retires chunks while the GPU stays busy.  A request finishes
 // when its last pixel is resolved; its film is copied out and its memory
 // released.  Sample streams are keyed by (request seed, pixel, sample), so a
 // result does not depend on the requests it was batched with.
@@ -48,10 +50,34 @@ struct ServerReq {
 }  // namespace
 }  // namespace cg
 
+// One pipeline of the server: its own stream and ray queues, the view table
+// of the chunk it runs, and the event that marks the chunk's end.  Two lanes
+// keep the device busy while the host retires one chunk and builds the next,
+// and let two chunks (of the same or different scenes) share the GPU.
+struct ServerLane {
+  cg::Renderer rend;
+  cg::ViewDev* table = nullptr;
+  size_t table_cap = 0;
+  std::vector<cg::ViewDev> slices;
+  std::vector<cg::ServerReq*> slice_req;
+  uint32_t used = 0;
+  uint64_t issued = 0;          // dispatch order of the chunk in flight
+  bool busy = false;
+  uint32_t* status_host = nullptr;  // pinned: the chunk's status word
+  cudaEvent_t done = nullptr;
+  ~ServerLane() {
+    if (done) cudaEventDestroy(done);
+    if (status_host) cudaFreeHost(status_host);
+    if (table) cudaFree(table);
+  }
+};
+
 struct cg_server_s {
+  static constexpr int kLanes = 2;
   std::vector<cg::SceneDev*> scenes;
   uint64_t budget = 0;
-  cg::Renderer rend;
+  ServerLane lanes[kLanes];
+  cudaStream_t alloc_stream = nullptr;  // film allocations (synchronised before use)
   cg_conf conf{};
   std::thread worker;
   std::mutex mu;
@@ -63,12 +89,12 @@ struct cg_server_s {
   int fatal = CG_OK;
   std::string fatal_msg;
   uint64_t next_id = 1;
+  uint64_t dispatched = 0;
   cg_server_stats st{};
   uint32_t rr = 0;
-  cg::ViewDev* table = nullptr;
-  size_t table_cap = 0;
-  std::vector<cg::ViewDev> slices;
-  std::vector<cg::ServerReq*> slice_req;
+  ~cg_server_s() {
+    if (alloc_stream) cudaStreamDestroy(alloc_stream);
+  }
 };
 
 namespace cg {
@@ -79,7 +105,8 @@ size_t requestBytes(const cg_server_s& sv, const SceneDev& scene, const cg_reque
   const size_t npx = size_t(r.view.width) * r.view.height;
   const LevelPlan plan = planLevels(capsOf(sv.conf), std::max(1u, scene.max_lobes));
   const size_t per_sample = 12 + plan.max_product * (36 + 20 + 36);
-  const size_t samples = std::min<size_t>(npx * r.view.spp, sv.rend.chunkSamples(scene, capsOf(sv.conf)));
+  const size_t samples =
+      std::min<size_t>(npx * r.view.spp, sv.lanes[0].rend.chunkSamples(scene, capsOf(sv.conf)));
   return npx * 16 + samples * per_sample;
 }
 
@@ -94,8 +121,105 @@ void finishRequest(cg_server_s& sv, ServerReq* r, int status) {
     ++sv.st.cancelled;
 }
 
+// Builds one chunk for one scene (round robin over scenes with work) in
+// `lane`: an equal share of the chunk for each of the scene's active
+// requests, the rest first come first served.  Returns false when no request
+// has pixels left to schedule.
+bool buildChunk(cg_server_s* sv, ServerLane& lane, const Caps& caps, SceneDev*& scene_out,
+                ChunkDesc& ch) {
+  uint32_t scene_idx = UINT32_MAX;
+  for (uint32_t k = 0; k < sv->scenes.size() && scene_idx == UINT32_MAX; ++k) {
+    const uint32_t s = (sv->rr + k) % static_cast<uint32_t>(sv->scenes.size());
+    for (ServerReq* r : sv->active)
+      if (r->req.scene == s && !r->cancelled && r->next_pixel < r->npx) {
+        scene_idx = s;
+        break;
+      }
+  }
+  if (scene_idx == UINT32_MAX) return false;
+  sv->rr = scene_idx + 1;
+  SceneDev& scene = *sv->scenes[scene_idx];
+  const uint32_t cap = lane.rend.chunkSamples(scene, caps);
+  std::vector<ServerReq*> mine;
+  for (ServerReq* r : sv->active)
+    if (r->req.scene == scene_idx && !r->cancelled && r->next_pixel < r->npx) mine.push_back(r);
+  const uint32_t share = std::max<uint32_t>(1u, cap / static_cast<uint32_t>(mine.size()));
+  lane.slices.clear();
+  lane.slice_req.clear();
+  uint32_t used = 0;
+  auto take = [&](ServerReq* r, uint32_t budget_samples) {
+    const uint32_t spp = r->req.view.spp;
+    uint32_t px = std::min<uint32_t>(budget_samples / spp, r->npx - r->next_pixel);
+    px = std::min<uint32_t>(px, (cap - used) / spp);
+    if (px == 0) return;
+    ViewDev v;
+    std::memset(&v, 0, sizeof(v));
+    cameraBasis(r->req.view.camera, v);
+    v.width = r->req.view.width;
+    v.height = r->req.view.height;
+    v.spp = spp;
+    v.seed = r->req.view.seed;
+    v.frame = 0;
+    v.sample_weight = 1.0f;
+    v.pixel_base = r->next_pixel;
+    v.pixel_count = px;
+    v.film = r->film;
+    v.rgba = nullptr;
+    lane.slices.push_back(v);
+    lane.slice_req.push_back(r);
+    r->next_pixel += px;
+    used += px * spp;
+  };
+  for (ServerReq* r : mine) take(r, share);
+  for (ServerReq* r : mine) take(r, cap);
+  layoutViews(lane.slices);
+  ch = ChunkDesc{0, 0, used, 0};
+  for (const ViewDev& v : lane.slices) ch.pixel_count += v.pixel_count;
+  lane.used = used;
+  scene_out = &scene;
+  return true;
+}
+
+// Enqueues the lane's chunk: view table upload, the kernel sequence, the
+// status word read into pinned memory, the completion event.
+int enqueueLane(ServerLane& lane, SceneDev& scene, const ChunkDesc& ch, const Caps& caps) {
+  if (lane.slices.size() > lane.table_cap) {
+    if (lane.table) cudaFree(lane.table);
+    lane.table = nullptr;
+    lane.table_cap = 0;
+    if (cudaMalloc(&lane.table, lane.slices.size() * 2 * sizeof(ViewDev)) != cudaSuccess) {
+      cudaGetLastError();
+      return CG_E_OOM;
+    }
+    lane.table_cap = lane.slices.size() * 2;
+  }
+  cudaStream_t s = lane.rend.stream;
+  if (cudaMemcpyAsync(lane.table, lane.slices.data(), lane.slices.size() * sizeof(ViewDev),
+                      cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return CG_E_CUDA;
+  RenderRecord rec;
+  lane.rend.enqueueChunk(scene, static_cast<uint32_t>(lane.slices.size()), lane.table, ch, caps, s,
+                         rec);
+  if (cudaGetLastError() != cudaSuccess) return CG_E_CUDA;
+  if (cudaMemcpyAsync(lane.status_host, lane.rend.wave.status, 4, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaEventRecord(lane.done, s) != cudaSuccess)
+    return CG_E_CUDA;
+  return CG_OK;
+}
+
+void failAll(cg_server_s* sv, int rc, const char* msg) {
+  sv->fatal = rc;
+  sv->fatal_msg = msg;
+  for (ServerReq* r : sv->active) finishRequest(*sv, r, rc);
+  sv->active.clear();
+  for (ServerReq* r : sv->pending) finishRequest(*sv, r, rc);
+  sv->pending.clear();
+  sv->done_cv.notify_all();
+}
+
 void serverLoop(cg_server_s* sv) {
-  cudaSetDevice(sv->rend.device);
+  cudaSetDevice(sv->lanes[0].rend.device);
   const Caps caps = capsOf(sv->conf);
   std::unique_lock<std::mutex> lk(sv->mu);
   while (true) {
@@ -121,7 +245,8 @@ void serverLoop(cg_server_s* sv) {
       sv->pending.pop_front();
       const size_t fb = size_t(r->npx) * 16;
       void* film = nullptr;
-      if (cudaMallocAsync(&film, fb, sv->rend.stream) != cudaSuccess) {
+      if (cudaMallocAsync(&film, fb, sv->alloc_stream) != cudaSuccess ||
+          cudaStreamSynchronize(sv->alloc_stream) != cudaSuccess) {
         cudaGetLastError();
         r->bytes = 0;
         ++sv->st.rejected;
@@ -137,128 +262,79 @@ void serverLoop(cg_server_s* sv) {
     }
     sv->st.active = static_cast<uint32_t>(sv->active.size());
     sv->st.pending = static_cast<uint32_t>(sv->pending.size());
-    if (sv->active.empty()) {
-      if (sv->stop) break;
-      sv->cv.wait(lk);
-      continue;
-    }
-    // ---- one chunk for one scene, round robin over scenes with work ----
-    uint32_t scene_idx = UINT32_MAX;
-    for (uint32_t k = 0; k < sv->scenes.size() && scene_idx == UINT32_MAX; ++k) {
-      const uint32_t s = (sv->rr + k) % static_cast<uint32_t>(sv->scenes.size());
-      for (ServerReq* r : sv->active)
-        if (r->req.scene == s && !r->cancelled && r->next_pixel < r->npx) {
-          scene_idx = s;
-          break;
-        }
-    }
-    if (scene_idx == UINT32_MAX) {  // only cancelled requests left
-      for (ServerReq* r : sv->active) {
-        cudaFreeAsync(r->film, sv->rend.stream);
-        finishRequest(*sv, r, CG_E_CANCELLED);
+    // ---- dispatch a chunk to every idle lane while there is work ----
+    for (ServerLane& lane : sv->lanes) {
+      if (lane.busy) continue;
+      SceneDev* scene = nullptr;
+      ChunkDesc ch{};
+      if (!buildChunk(sv, lane, caps, scene, ch)) break;
+      const int rc = enqueueLane(lane, *scene, ch, caps);
+      if (rc != CG_OK) {
+        failAll(sv, rc, "CUDA failure in the server loop");
+        return;
       }
-      sv->active.clear();
-      cudaStreamSynchronize(sv->rend.stream);
-      sv->done_cv.notify_all();
+      lane.busy = true;
+      lane.issued = ++sv->dispatched;
+    }
+    ServerLane* oldest = nullptr;
+    for (ServerLane& lane : sv->lanes)
+      if (lane.busy && (!oldest || lane.issued < oldest->issued)) oldest = &lane;
+    if (!oldest) {
+      // nothing in flight: retire requests that were cancelled before they ran
+      bool any = false;
+      for (auto it = sv->active.begin(); it != sv->active.end();) {
+        ServerReq* r = *it;
+        if (r->cancelled && r->resolved == r->next_pixel) {
+          cudaFreeAsync(r->film, sv->alloc_stream);
+          r->film = nullptr;
+          finishRequest(*sv, r, CG_E_CANCELLED);
+          it = sv->active.erase(it);
+          any = true;
+        } else {
+          ++it;
+        }
+      }
+      if (any) {
+        cudaStreamSynchronize(sv->alloc_stream);
+        sv->done_cv.notify_all();
+        continue;
+      }
+      if (sv->stop && sv->active.empty()) break;
+      // idle (or only requests waiting for memory): sleep until a submit,
+      // cancel or shutdown; the timeout re-checks in case a wake-up raced
+      sv->cv.wait_for(lk, std::chrono::milliseconds(50));
       continue;
     }
-    sv->rr = scene_idx + 1;
-    SceneDev& scene = *sv->scenes[scene_idx];
-    const uint32_t cap = sv->rend.chunkSamples(scene, caps);
-    std::vector<ServerReq*> mine;
-    for (ServerReq* r : sv->active)
-      if (r->req.scene == scene_idx && !r->cancelled && r->next_pixel < r->npx) mine.push_back(r);
-    const uint32_t share = std::max<uint32_t>(1u, cap / static_cast<uint32_t>(mine.size()));
-    sv->slices.clear();
-    sv->slice_req.clear();
-    uint32_t used = 0;
-    auto take = [&](ServerReq* r, uint32_t budget_samples) {
-      const uint32_t spp = r->req.view.spp;
-      uint32_t px = std::min<uint32_t>(budget_samples / spp, r->npx - r->next_pixel);
-      px = std::min<uint32_t>(px, (cap - used) / spp);
-      if (px == 0) return;
-      ViewDev v;
-      std::memset(&v, 0, sizeof(v));
-      cameraBasis(r->req.view.camera, v);
-      v.width = r->req.view.width;
-      v.height = r->req.view.height;
-      v.spp = spp;
-      v.seed = r->req.view.seed;
-      v.frame = 0;
-      v.sample_weight = 1.0f;
-      v.pixel_base = r->next_pixel;
-      v.pixel_count = px;
-      v.film = r->film;
-      v.rgba = nullptr;
-      sv->slices.push_back(v);
-      sv->slice_req.push_back(r);
-      r->next_pixel += px;
-      used += px * spp;
-    };
-    for (ServerReq* r : mine) take(r, share);
-    for (ServerReq* r : mine) take(r, cap);
-    layoutViews(sv->slices);
-    ChunkDesc ch{0, 0, used, 0};
-    for (const ViewDev& v : sv->slices) ch.pixel_count += v.pixel_count;
+    // ---- retire the oldest chunk in flight ----
     lk.unlock();
-    // ---- run it ----
-    int rc = CG_OK;
-    if (sv->slices.size() > sv->table_cap) {
-      if (sv->table) cudaFree(sv->table);
-      sv->table = nullptr;
-      sv->table_cap = 0;
-      if (cudaMalloc(&sv->table, sv->slices.size() * 2 * sizeof(ViewDev)) == cudaSuccess)
-        sv->table_cap = sv->slices.size() * 2;
-      else
-        rc = CG_E_OOM;
-    }
-    RenderRecord rec;
-    if (rc == CG_OK &&
-        cudaMemcpyAsync(sv->table, sv->slices.data(), sv->slices.size() * sizeof(ViewDev),
-                        cudaMemcpyHostToDevice, sv->rend.stream) != cudaSuccess)
-      rc = CG_E_CUDA;
-    if (rc == CG_OK) {
-      sv->rend.enqueueChunk(scene, static_cast<uint32_t>(sv->slices.size()), sv->table, ch, caps,
-                            sv->rend.stream, rec);
-      if (cudaGetLastError() != cudaSuccess) rc = CG_E_CUDA;
-    }
-    uint32_t status = 0;
-    if (rc == CG_OK &&
-        (cudaMemcpyAsync(&status, sv->rend.wave.status, 4, cudaMemcpyDeviceToHost, sv->rend.stream) !=
-             cudaSuccess ||
-         cudaStreamSynchronize(sv->rend.stream) != cudaSuccess))
-      rc = CG_E_CUDA;
-    if (rc == CG_OK && status) rc = CG_E_DEVICE;
+    const bool ok = cudaEventSynchronize(oldest->done) == cudaSuccess;
     lk.lock();
-    if (rc != CG_OK) {
-      sv->fatal = rc;
-      sv->fatal_msg = rc == CG_E_DEVICE ? "kernel status word set (stack or queue overflow)"
-                                        : "CUDA failure in the server loop";
-      for (ServerReq* r : sv->active) finishRequest(*sv, r, rc);
-      sv->active.clear();
-      for (ServerReq* r : sv->pending) finishRequest(*sv, r, rc);
-      sv->pending.clear();
-      sv->done_cv.notify_all();
-      break;
+    oldest->busy = false;
+    if (!ok || *oldest->status_host) {
+      cudaGetLastError();
+      failAll(sv, ok ? CG_E_DEVICE : CG_E_CUDA,
+              ok ? "kernel status word set (stack or queue overflow)" : "CUDA failure in the server loop");
+      return;
     }
-    sv->st.samples += used;
-    // ---- completions ----
-    for (size_t k = 0; k < sv->slice_req.size(); ++k) sv->slice_req[k]->resolved += sv->slices[k].pixel_count;
+    sv->st.samples += oldest->used;
+    for (size_t k = 0; k < oldest->slice_req.size(); ++k)
+      oldest->slice_req[k]->resolved += oldest->slices[k].pixel_count;
     bool any = false;
+    cudaStream_t s = oldest->rend.stream;
     for (auto it = sv->active.begin(); it != sv->active.end();) {
       ServerReq* r = *it;
       const bool complete = r->resolved == r->npx;
       if (complete || (r->cancelled && r->resolved == r->next_pixel)) {
         int st = CG_E_CANCELLED;
         if (complete && !r->cancelled) {
-          st = cudaMemcpy2DAsync(r->out, 12, r->film, 16, 12, r->npx, cudaMemcpyDeviceToHost,
-                                 sv->rend.stream) == cudaSuccess
+          st = cudaMemcpy2DAsync(r->out, 12, r->film, 16, 12, r->npx, cudaMemcpyDeviceToHost, s) ==
+                       cudaSuccess
                    ? CG_OK
                    : CG_E_CUDA;
         }
-        cudaFreeAsync(r->film, sv->rend.stream);
+        cudaFreeAsync(r->film, s);
         r->film = nullptr;
-        cudaStreamSynchronize(sv->rend.stream);
+        cudaStreamSynchronize(s);
         finishRequest(*sv, r, st);
         it = sv->active.erase(it);
         any = true;
@@ -297,11 +373,23 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
   for (uint32_t i = 0; i < scene_count; ++i) sv->scenes.push_back(reinterpret_cast<SceneDev*>(scenes[i]));
   sv->budget = hbm_budget_bytes;
   sv->conf = conf;
-  sv->rend.tuning = tuning;
-  int rc = sv->rend.init(device);
-  if (rc != CG_OK) return rc;
-  rc = sv->rend.ensureWave(tuning.queue_capacity);
-  if (rc != CG_OK) return rc;
+  for (ServerLane& lane : sv->lanes) {
+    lane.rend.tuning = tuning;
+    int rc = lane.rend.init(device);
+    if (rc != CG_OK) return rc;
+    rc = lane.rend.ensureWave(tuning.queue_capacity);
+    if (rc != CG_OK) return rc;
+    if (cudaMallocHost(&lane.status_host, sizeof(uint32_t)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CG_E_CUDA, "server lane setup failed");
+    }
+    *lane.status_host = 0u;
+  }
+  if (cudaStreamCreateWithFlags(&sv->alloc_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CG_E_CUDA, "server stream setup failed");
+  }
   sv->worker = std::thread(serverLoop, sv.get());
   *out = sv.release();
   return CG_OK;
@@ -317,7 +405,6 @@ CG_API int cg_server_destroy(cg_server_t server) {
   }
   server->cv.notify_all();
   if (server->worker.joinable()) server->worker.join();
-  if (server->table) cudaFree(server->table);
   delete server;
   return CG_OK;
 }
@@ -329,7 +416,7 @@ CG_API int cg_server_submit(cg_server_t server, const cg_request* request, float
   if (request->scene >= server->scenes.size()) return fail(CG_E_INVALID, "scene index out of range");
   if (v.width == 0 || v.height == 0 || v.spp == 0) return fail(CG_E_INVALID, "zero size or spp");
   SceneDev& scene = *server->scenes[request->scene];
-  if (v.spp > server->rend.chunkSamples(scene, capsOf(server->conf)))
+  if (v.spp > server->lanes[0].rend.chunkSamples(scene, capsOf(server->conf)))
     return fail(CG_E_INVALID, "spp exceeds the wavefront chunk");
   auto r = std::make_unique<ServerReq>();
   r->req = *request;
