@@ -174,9 +174,13 @@ __device__ __forceinline__ float sampleWavelengthTree(const float* __restrict__ 
 }
 
 // ---- Smits RGB -> spectrum (shading/smits.wesl, material.wesl:264-297) ---------------
-__constant__ float kBins[10] = {380.0f, 417.7778f, 455.5556f, 493.3333f, 531.1111f,
-                                568.8889f, 606.6667f, 644.4444f, 682.2222f, 720.0f};
-__constant__ float kSmits[7][10] = {
+// In global memory and read through the read-only data cache: lanes look up
+// different bins (their wavelengths differ), which constant memory would
+// serialise one address at a time; L1 serves a warp's lanes from the same
+// lines in one pass.
+__device__ const float kBins[10] = {380.0f, 417.7778f, 455.5556f, 493.3333f, 531.1111f,
+                                    568.8889f, 606.6667f, 644.4444f, 682.2222f, 720.0f};
+__device__ const float kSmits[7][10] = {
     {1.0f, 1.0f, 0.9999f, 0.9993f, 0.9992f, 0.9998f, 1.0f, 1.0f, 1.0f, 1.0f},                 // white
     {0.1012f, 0.0515f, 0.0f, 0.0f, 0.0f, 0.0f, 0.8325f, 1.0149f, 1.0149f, 1.0149f},           // red
     {0.0f, 0.0f, 0.0273f, 0.7937f, 1.0f, 0.9418f, 0.1719f, 0.0f, 0.0f, 0.0025f},              // green
@@ -205,14 +209,15 @@ __device__ __forceinline__ SmitsPos smitsPos(float w) {
   uint32_t bin = static_cast<uint32_t>(10.0f * (w - 380.0f) / 340.0f);
   p.b0 = bin > 9u ? 9u : bin;
   p.b1 = (bin + 1u) > 9u ? 9u : bin + 1u;  // WGSL robust access clamps index 10 to 9
-  p.mixv = (w - kBins[p.b0]) / (kBins[p.b1] - kBins[p.b0]);
+  const float lo = __ldg(&kBins[p.b0]), hi = __ldg(&kBins[p.b1]);
+  p.mixv = (w - lo) / (hi - lo);
   return p;
 }
 __device__ __forceinline__ float smits(const SmitsPos& p, int curve) {
   const float* X = kSmits[curve];
-  if (p.mode == 0) return X[0];
-  if (p.mode == 1) return X[9];
-  return (1.0f - p.mixv) * X[p.b0] + p.mixv * X[p.b1];
+  if (p.mode == 0) return __ldg(&X[0]);
+  if (p.mode == 1) return __ldg(&X[9]);
+  return (1.0f - p.mixv) * __ldg(&X[p.b0]) + p.mixv * __ldg(&X[p.b1]);
 }
 __device__ __forceinline__ float rgbToSpectrum(V3 rgb, const SmitsPos& sp) {
   float s = 0.0f;
