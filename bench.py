@@ -55,8 +55,10 @@ TRI_B, INST_B, RAY_B = 48, 64, 52
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # DRAM bytes (read + write) per k_extend launch of this workload, mean of the
 # seven launches of one chunk in profiles/dram_traffic_icosphere_1280x720_16spp_d8.md
-# (ncu, cold caches: an upper bound)
+# (ncu, cold caches: an upper bound), captured with 56 closest-hit launches per
+# frame; with another chunking the frame's traffic is spread over its launches
 EXTEND_TRAFFIC_B = 183e6
+EXTEND_TRAFFIC_LAUNCHES = 56
 
 
 def dist_env():
@@ -271,7 +273,7 @@ def _tuning_kwargs(t):
     return dict(queue_capacity=int(t.queue_capacity), extend_block=int(t.extend_block),
                 shade_block=int(t.shade_block), use_graph=int(t.use_graph),
                 bvh_width=int(t.bvh_width), persistent=int(t.persistent) != 2,
-                shade_sort=int(t.shade_sort) != 2)
+                shade_sort={1: "global", 2: "none", 3: "block"}.get(int(t.shade_sort), "global"))
 
 
 def _plain_render(B, g, pos, d, w, h, spp, seed, depth, tuning=None):
@@ -447,11 +449,11 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     samples_per_step = W_ * H_ * SPP_
 
-    if (args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort >= 0 or
+    if (args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort != "default" or
             args.box_bits):
         B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width,
                     persistent=None if args.persistent < 0 else bool(args.persistent),
-                    shade_sort=None if args.shade_sort < 0 else bool(args.shade_sort),
+                    shade_sort=None if args.shade_sort == "default" else args.shade_sort,
                     box_bits=args.box_bits)
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
@@ -506,6 +508,7 @@ def run_ours(args):
     sh_ms, sh_n = prof["shadow"]
     # counting pass totals cover extend + shadow; split the node/tri work by ray count
     per_frame_launch = max(ext_n // max(args.steps, 1), 1)
+    extend_scale = EXTEND_TRAFFIC_LAUNCHES / per_frame_launch
     tun = B.GetTuning()
     width = int(tun.bvh_width) or 4
     node_b = NODE_B["4q"] if width == 4 and int(tun.box_bits) == 8 else NODE_B[width]
@@ -553,9 +556,9 @@ def run_ours(args):
             "roofline": {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": (EXTEND_TRAFFIC_B if (args.case == "full" and width == 4 and
-                                                          node_b == NODE_B[4] and
-                                                          WORKLOAD_NAME == "icosphere")
+                         "traffic": (EXTEND_TRAFFIC_B * extend_scale if (
+                                         args.case == "full" and width == 4 and
+                                         node_b == NODE_B[4] and WORKLOAD_NAME == "icosphere")
                                      else None),
                          "traffic_source": "ncu dram__bytes_read+write per launch, cold "
                                            "caches (profiles/dram_traffic_icosphere_"
@@ -611,8 +614,8 @@ def main():
                     help="four-wide child box precision (0 = library default, 32)")
     ap.add_argument("--forms", default="auto", choices=["auto", "on", "off"],
                     help="batched and served forms vs plain (auto: on at one GPU)")
-    ap.add_argument("--shade-sort", type=int, default=-1, choices=[-1, 0, 1],
-                    help="group rays by material kind before shading (-1 = library default)")
+    ap.add_argument("--shade-sort", default="default", choices=["default", "global", "block", "none"],
+                    help="order of the rays the shading kernel takes (default: the library's, global)")
     args = ap.parse_args()
     global W_, H_, SPP_, DEPTH_, WORKLOAD, WORKLOAD_NAME
     WORKLOAD_NAME = args.workload

@@ -239,6 +239,7 @@ int Renderer::ensureWave(uint32_t capacity) {
                           Q * 16, Q * 4,                                 // hits
                           Q * 16, Q * 16, Q * 4,                         // shadow queue
                           Q * 4,  Q * 4,  Q * 4,                         // sample slots
+                          Q,      Q * 4,                                 // shading key, order
                           256,    256,    256};                          // counts, stats, status
   size_t total = 0;
   for (size_t b : parts) total += align256(b);
@@ -266,6 +267,8 @@ int Renderer::ensureWave(uint32_t capacity) {
   wave.s_L = reinterpret_cast<float*>(take(Q * 4));
   wave.s_lambda = reinterpret_cast<float*>(take(Q * 4));
   wave.s_prob = reinterpret_cast<float*>(take(Q * 4));
+  wave.shade_key = reinterpret_cast<uint8_t*>(take(Q));
+  wave.shade_perm = reinterpret_cast<uint32_t*>(take(Q * 4));
   wave.counts = reinterpret_cast<uint32_t*>(take(256));
   wave.stats = reinterpret_cast<unsigned long long*>(take(256));
   wave.status = reinterpret_cast<uint32_t*>(take(256));
@@ -298,7 +301,9 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.shade_block = tuning.shade_block;
   ls.nodes = nodeFormatOf(tuning);
   ls.persistent = tuning.persistent != 2u;
-  ls.shade_sort = tuning.shade_sort != 2u;
+  ls.shade_sort = tuning.shade_sort == 2u   ? kShadeSortNone
+                  : tuning.shade_sort == 3u ? kShadeSortBlock
+                                            : kShadeSortGlobal;
   profBegin(CG_K_GEN, s);
   launchGen(fc, wave, ch, s);
   profEnd(s);
@@ -309,9 +314,9 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
     launchExtend(scene.view, wave, parity, counting, ls, s);
     profEnd(s);
     profBegin(CG_K_SHADE, s);
-    launchShade(scene.view, fc, wave, static_cast<int>(d), parity, ls, s);
+    const int shade_kernels = launchShade(scene.view, fc, wave, static_cast<int>(d), parity, ls, s);
     profEnd(s);
-    rec.launches += 2;
+    rec.launches += 1 + static_cast<uint32_t>(shade_kernels);
     if (plan.shadow[d]) {
       profBegin(CG_K_SHADOW, s);
       launchShadow(scene.view, wave, counting, ls, s);
@@ -825,7 +830,8 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
   if (t->bvh_width) g_env->tuning.bvh_width = t->bvh_width;
   if (t->persistent) g_env->tuning.persistent = t->persistent == 2u ? 2u : 1u;
-  if (t->shade_sort) g_env->tuning.shade_sort = t->shade_sort == 2u ? 2u : 1u;
+  if (t->shade_sort > 3u) return fail(CG_E_INVALID, "shade_sort must be 0..3");
+  if (t->shade_sort) g_env->tuning.shade_sort = t->shade_sort;
   g_env->tuning.use_graph = t->use_graph;
   g_env->dropAllGraphs();
   return CG_OK;

@@ -86,7 +86,9 @@ struct Renderer {
   float* wl_tree = nullptr;
   float* wl_const = nullptr;
   bool counting = false;
-  cg_tuning tuning{16u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u};
+  // 64M rays per level queue (~9.7 GB of path state): large chunks keep every
+  // level's launch full
+  cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
 

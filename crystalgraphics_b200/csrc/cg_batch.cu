@@ -237,10 +237,10 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32
       winner = t;
     }
   };
-  // kernel variants: (node width, persistent lane refill 1 on / 2 off, shade sort
-  // 1 on / 2 off, bits per child box bound)
+  // kernel variants: (node width, persistent lane refill 1 on / 2 off, shading
+  // order 1 level-wide sort / 3 per-block sort / 2 none, bits per child box bound)
   const uint32_t variants[][4] = {
-      {4u, 1u, 1u, 32u}, {4u, 2u, 1u, 32u}, {4u, 1u, 1u, 8u},
+      {4u, 1u, 1u, 32u}, {4u, 2u, 1u, 32u}, {4u, 1u, 1u, 8u}, {4u, 1u, 3u, 32u},
       {4u, 1u, 2u, 32u}, {2u, 1u, 1u, 32u}, {2u, 2u, 1u, 32u}};
   {
     const cg_tuning base = winner;
@@ -255,7 +255,7 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32
   }
   {
     const cg_tuning base = winner;
-    for (uint32_t q : {8u << 20, 16u << 20, 32u << 20}) {
+    for (uint32_t q : {16u << 20, 64u << 20, 128u << 20}) {
       cg_tuning t = base;
       t.queue_capacity = q;
       consider(t);

@@ -430,10 +430,75 @@ __device__ __forceinline__ int shadeKey(const SceneView& sc, const WaveBuffers& 
   return 2 + static_cast<int>((sc.mat[meta.y].volume >> kKindShift) & 15u);
 }
 
-// kSort: before shading, every block sorts its slice of the queue by shading
-// key in shared memory (counting sort), so a warp shades misses, cut hits or
-// one material kind rather than a mix of code paths.
-template <bool kSort>
+// ---- the global shading order: a counting sort of the level by shading key ----
+constexpr int kTicket = 6, kKeyCount = 8, kKeyCursor = 32;
+
+// Shading key of every queued ray and the number of rays per key (one atomic
+// per distinct key per warp).  The block that finishes last turns the counts
+// into the scatter cursors (exclusive prefix sums) and zeroes the counts and
+// the ticket for the next level; no block waits for another.
+__global__ void __launch_bounds__(256) k_shade_keys(SceneView sc, FrameConst fc, WaveBuffers wb,
+                                                    int depth, int parity) {
+  const uint32_t n = min(wb.counts[parity], wb.capacity);
+  const uint32_t cut_depth = max(1u, min(fc.caps.trace_depth, 64u)) - 1u;
+  const bool cut = static_cast<uint32_t>(depth) >= cut_depth;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = warp_global * 32u; base < n; base += warps * 32u) {
+    const uint32_t i = base + lane;
+    const int key = i < n ? shadeKey(sc, wb, i, cut) : kNumKeys - 1;
+    if (i < n) wb.shade_key[i] = static_cast<uint8_t>(key);
+    const unsigned peers = __match_any_sync(kFull, key);
+    if (key != kNumKeys - 1 && lane == static_cast<uint32_t>(__ffs(peers) - 1))
+      atomicAdd(&wb.counts[kKeyCount + key], static_cast<uint32_t>(__popc(peers)));
+  }
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&wb.counts[kTicket], 1u) == gridDim.x - 1u;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    uint32_t off = 0;
+    for (int k = 0; k < kNumKeys; ++k) {
+      const uint32_t c = atomicExch(&wb.counts[kKeyCount + k], 0u);
+      wb.counts[kKeyCursor + k] = off;
+      off += c;
+    }
+    wb.counts[kTicket] = 0u;
+  }
+}
+
+// Places every ray at its key's cursor: shade_perm lists the level's rays
+// grouped by key.
+__global__ void __launch_bounds__(256) k_shade_scatter(WaveBuffers wb, int parity) {
+  const uint32_t n = min(wb.counts[parity], wb.capacity);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = warp_global * 32u; base < n; base += warps * 32u) {
+    const uint32_t i = base + lane;
+    const int key = i < n ? wb.shade_key[i] : kNumKeys - 1;
+    const unsigned peers = __match_any_sync(kFull, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (key != kNumKeys - 1 && static_cast<int>(lane) == leader)
+      pos = atomicAdd(&wb.counts[kKeyCursor + key], static_cast<uint32_t>(__popc(peers)));
+    pos = __shfl_sync(peers, pos, leader);
+    const uint32_t at = pos + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
+    if (key != kNumKeys - 1 && at < wb.capacity) wb.shade_perm[at] = i;
+  }
+}
+
+// kSort (ShadeSort): kShadeSortBlock — before shading, every block sorts its
+// slice of the queue by shading key in shared memory (counting sort);
+// kShadeSortGlobal — the level was sorted by k_shade_keys / k_shade_scatter
+// and the kernel takes rays in that order.  Either way a warp shades misses,
+// cut hits or one material kind rather than a mix of code paths.
+template <int kSort>
 __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                int depth, int parity) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
@@ -448,7 +513,8 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
   if (blockIdx.x == 0 && threadIdx.x == 0) wb.counts[3] = 0u;  // next extend's work counter
   for (uint32_t bbase = blockIdx.x * blockDim.x; bbase < n; bbase += gridDim.x * blockDim.x) {
     uint32_t i = bbase + threadIdx.x;
-    if (kSort) {
+    if (kSort == kShadeSortGlobal && i < n) i = wb.shade_perm[i];
+    if (kSort == kShadeSortBlock) {
       const int key = i < n ? shadeKey(sc, wb, i, static_cast<uint32_t>(depth) >= cut_depth)
                             : kNumKeys - 1;
       if (threadIdx.x < kNumKeys) s_cnt[threadIdx.x] = 0;
@@ -765,14 +831,22 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
   }
 }
 
-void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
-                 int parity, const LaunchShape& ls, cudaStream_t s) {
+int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
+                int parity, const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
-  if (ls.shade_sort)
-    k_shade<true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+  if (ls.shade_sort == kShadeSortGlobal) {
+    const uint32_t g = gridFor(8u);  // 8 blocks of 256 per SM
+    k_shade_keys<<<g, 256, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade_scatter<<<g, 256, 0, s>>>(wb, parity);
+    k_shade<kShadeSortGlobal><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    return 3;
+  }
+  if (ls.shade_sort == kShadeSortBlock)
+    k_shade<kShadeSortBlock><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
   else
-    k_shade<false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade<kShadeSortNone><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+  return 1;
 }
 
 void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,

@@ -51,7 +51,11 @@ struct WaveBuffers {
   float* s_L;            // per sample slot: accumulated radiance
   float* s_lambda;
   float* s_prob;
-  uint32_t* counts;      // [0], [1] ray queues, [2] shadow queue
+  uint8_t* shade_key;    // per queued ray: its shading key (the global shading sort)
+  uint32_t* shade_perm;  // queued rays in shading-key order
+  uint32_t* counts;      // [0], [1] ray queues, [2] shadow queue, [3], [4] traversal work
+                         // counters, [6] block ticket, [8..26] rays per shading key,
+                         // [32..50] scatter cursors
   unsigned long long* stats;  // [0] extend rays [1] shadow rays [2] nodes [3] tris [4] insts
   uint32_t* status;      // bit 0: traversal stack overflow, bit 1: queue overflow
   uint32_t capacity;     // rays per queue (and shadow rays)
@@ -73,6 +77,11 @@ struct ChunkDesc {
   uint32_t pixel_count;
 };
 
+// How the shading kernel orders a level's rays: as queued, by a counting
+// sort of each block's slice, or by a counting sort of the whole level
+// (two small kernels build a permutation; no barriers in the shading kernel).
+enum ShadeSort : int { kShadeSortNone = 0, kShadeSortBlock = 1, kShadeSortGlobal = 2 };
+
 struct LaunchShape {
   uint32_t extend_block = 128;
   uint32_t shade_block = 128;
@@ -80,15 +89,16 @@ struct LaunchShape {
   uint32_t grid_shade = 0;
   int nodes = kNodesWide4;   // NodeFormat of the traversal
   bool persistent = true;    // persistent warps with lane refill
-  bool shade_sort = true;    // group a block's rays by shading key before shading
+  int shade_sort = kShadeSortGlobal;  // ShadeSort: order of the rays the shading kernel takes
 };
 
 void launchWavelengthTree(float* tree, float* consts, cudaStream_t s);
 void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch, cudaStream_t s);
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
                   const LaunchShape& ls, cudaStream_t s);
-void launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
-                 int parity, const LaunchShape& ls, cudaStream_t s);
+// Returns the number of kernels launched (one, or three with the global sort).
+int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
+                int parity, const LaunchShape& ls, cudaStream_t s);
 void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s);
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,

@@ -41,7 +41,9 @@ constexpr size_t kOffShSlot = kOffShD + Q * 16;
 constexpr size_t kOffSL = kOffShSlot + Q * 4;
 constexpr size_t kOffSLambda = kOffSL + Q * 4;
 constexpr size_t kOffSProb = kOffSLambda + Q * 4;
-constexpr size_t kOffCounts = kOffSProb + Q * 4;   // 256 B: queue counts
+constexpr size_t kOffKey = kOffSProb + Q * 4;      // shading keys (1 B per ray)
+constexpr size_t kOffPerm = kOffKey + Q;           // shading order
+constexpr size_t kOffCounts = kOffPerm + Q * 4;    // 256 B: queue counts
 constexpr size_t kOffStats = kOffCounts + 256;     // 256 B: ray statistics
 constexpr size_t kOffStatus = kOffStats + 256;     // 256 B: kernel status word
 constexpr size_t kOffView = kOffStatus + 256;      // 256 B: the ViewDev table
@@ -51,7 +53,7 @@ constexpr size_t kScratchBytes = kOffWlConst + 256;
 static_assert(sizeof(ViewDev) <= 256, "the view table slot holds one ViewDev");
 static_assert(kOffCounts % 256 == 0 && kOffWlTree % 256 == 0, "256-byte aligned parts");
 
-// ~18.6 MB per device; file scope so that only this file's host code asks for
+// ~19.3 MB per device; file scope so that only this file's host code asks for
 // its address.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -104,6 +106,8 @@ WaveBuffers scratchBuffers(unsigned char* b) {
   w.s_L = reinterpret_cast<float*>(b + kOffSL);
   w.s_lambda = reinterpret_cast<float*>(b + kOffSLambda);
   w.s_prob = reinterpret_cast<float*>(b + kOffSProb);
+  w.shade_key = b + kOffKey;
+  w.shade_perm = reinterpret_cast<uint32_t*>(b + kOffPerm);
   w.counts = reinterpret_cast<uint32_t*>(b + kOffCounts);
   w.stats = reinterpret_cast<unsigned long long*>(b + kOffStats);
   w.status = reinterpret_cast<uint32_t*>(b + kOffStatus);

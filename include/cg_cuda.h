@@ -355,8 +355,10 @@ typedef struct cg_tuning {
   uint32_t bvh_width;   /* 4 (default) or 2: node width the traversal walks */
   uint32_t persistent;  /* 1 (default) = persistent traversal warps that refill
                            idle lanes, 2 = one ray per thread, 0 = keep */
-  uint32_t shade_sort;  /* 1 (default) = group rays by material kind before
-                           shading, 2 = do not, 0 = keep */
+  uint32_t shade_sort;  /* order of the rays the shading kernel takes: 1 (default)
+                           = grouped by material kind with a level-wide counting
+                           sort, 3 = sorted within each block's slice, 2 = as
+                           queued, 0 = keep */
   uint32_t box_bits;    /* four-wide child boxes: 32 (default) = floats in
                            128-byte nodes, 8 = 8-bit offsets in 64-byte nodes */
 } cg_tuning;
@@ -419,7 +421,7 @@ CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out);
  * per pixel, `film_rgba8` (may be NULL) uchar4 sRGB — on `stream` (NULL = the
  * default stream) of the current device, and returns when it is done.
  * It calls no cudaMalloc or cudaFree: the ray queues and tables live in a
- * library-owned device array of about 18.6 MB (131072 queued rays) that every
+ * library-owned device array of about 19.3 MB (131072 queued rays) that every
  * GPU loading the library holds until the process exits.  A view whose spp
  * cannot fit that array in one chunk is rejected with CG_E_INVALID.  The first
  * call on a device sets the array up (finds its device address, fills the

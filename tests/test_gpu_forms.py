@@ -81,7 +81,7 @@ def test_batch_uneven_views_in_many_chunks(cornell):
     B.SetTuning(queue_capacity=8192)
     small = B.batch_render(g, views)
     assert B.LastStats().chunks > 3
-    B.SetTuning(queue_capacity=16 << 20)
+    B.SetTuning(queue_capacity=64 << 20)
     for x, y in zip(ref, small):
         assert _close(x, y) < RTOL
 
@@ -169,6 +169,7 @@ def test_server_cancel_and_timeout(cornell):
                                      dict(bvh_width=4, persistent=True),
                                      dict(bvh_width=4, persistent=False),
                                      dict(bvh_width=4, persistent=False, shade_sort=False),
+                                     dict(bvh_width=4, persistent=True, shade_sort="block"),
                                      dict(bvh_width=4, persistent=False, box_bits=8)])
 def test_traversal_variants_render_the_same_samples(variant):
     """Binary or four-wide trees, one ray per thread or persistent warps, rays
@@ -195,7 +196,7 @@ def test_autotune_returns_a_valid_tuning(cornell):
     s, g = cornell
     t = B.autotune(g, (s.camera.position[:], s.camera.direction[:], 96, 96, 4, 1))
     assert t.queue_capacity >= 4096 and t.extend_block % 32 == 0 and t.shade_block % 32 == 0
-    assert t.bvh_width in (2, 4) and t.box_bits in (8, 32) and t.shade_sort in (1, 2)
+    assert t.bvh_width in (2, 4) and t.box_bits in (8, 32) and t.shade_sort in (1, 2, 3)
     # a tuning found on probe views renders the batch like the default tuning
     views = _views(s)
     ref = B.batch_render(g, views)
@@ -203,7 +204,7 @@ def test_autotune_returns_a_valid_tuning(cornell):
     assert B.GetTuning().bvh_width == t2.bvh_width
     for x, y in zip(B.batch_render(g, views), ref):
         assert _close(x, y) < RTOL
-    B.SetTuning(queue_capacity=16 << 20, extend_block=128, shade_block=128, use_graph=1,
+    B.SetTuning(queue_capacity=64 << 20, extend_block=128, shade_block=128, use_graph=1,
                 bvh_width=4, persistent=False, shade_sort=True, box_bits=32)
 
 
