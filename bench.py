@@ -602,9 +602,9 @@ def main():
                     help="plain-path configuration (default: the icosphere frame)")
     ap.add_argument("--case", default="full", choices=["full", "medium", "small"],
                     help="small: the same scene at 320x180, 4 spp, with a 2M-ray queue; "
-                         "medium: 640x360, 16 spp with the default queue (two chunks per "
-                         "frame of the same size as the full frame's eight): the cases "
-                         "ncu --set full captures")
+                         "medium: 640x360, 16 spp with a 16M-ray queue (two chunks of "
+                         "1.84M samples, ~2.5 GB on the device): the cases ncu --set full "
+                         "captures")
     ap.add_argument("--queue", type=int, default=0, help="ray queue capacity (0 = default)")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4],
                     help="node width of the traversal (0 = library default, 4)")
@@ -629,6 +629,7 @@ def main():
     elif args.case == "medium":
         W_, H_ = 640, 360
         WORKLOAD = WORKLOAD.replace("1280x720", "640x360")
+        args.queue = args.queue or (16 << 20)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -301,6 +301,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.shade_block = tuning.shade_block;
   ls.nodes = nodeFormatOf(tuning);
   ls.persistent = tuning.persistent != 2u;
+  const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
   ls.shade_sort = tuning.shade_sort == 2u   ? kShadeSortNone
                   : tuning.shade_sort == 3u ? kShadeSortBlock
                                             : kShadeSortGlobal;
@@ -311,7 +312,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   for (uint32_t d = 0; d < plan.levels; ++d) {
     const int parity = static_cast<int>(d & 1u);
     profBegin(CG_K_EXTEND, s);
-    launchExtend(scene.view, wave, parity, counting, ls, s);
+    launchExtend(scene.view, wave, parity, counting, ls, d >= cut_depth, s);
     profEnd(s);
     profBegin(CG_K_SHADE, s);
     const int shade_kernels = launchShade(scene.view, fc, wave, static_cast<int>(d), parity, ls, s);

@@ -121,6 +121,55 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   wb.ray_slot[0][i] = i;
 }
 
+// ---- shading keys (the level-wide shading order) ---------------------------------
+// Key of a hit: 0 miss, 1 hit beyond the depth cut (no work), 2 + material
+// kind; kNumKeys - 1 marks an empty slot.  The closest-hit kernel writes each
+// ray's key and counts rays per key (counts[kKeyCount + k]); the block that
+// finishes last turns the counts into the scatter cursors (counts[kKeyCursor
+// + k], exclusive prefix sums) and zeroes the counts and the ticket
+// (counts[kTicket]) for the next level.  No block waits for another.
+constexpr int kNumKeys = 19;
+constexpr int kTicket = 6, kKeyCount = 8, kKeyCursor = 32;
+
+__device__ __forceinline__ int shadeKeyOf(const SceneView& sc, int32_t inst, bool cut) {
+  if (inst < 0) return 0;
+  if (cut) return 1;
+  const uint4 meta = __ldg(reinterpret_cast<const uint4*>(sc.inst + inst) + 3);
+  return 2 + static_cast<int>((sc.mat[meta.y].volume >> kKindShift) & 15u);
+}
+
+// keys: 0 none, 1 keys for a level shaded before the depth cut, 2 after it.
+// Called by the lanes that finished a ray (one atomic per distinct key among them).
+__device__ __forceinline__ void writeShadeKey(const SceneView& sc, const WaveBuffers& wb, uint32_t i,
+                                              int32_t inst, int keys) {
+  const int key = shadeKeyOf(sc, inst, keys == 2);
+  wb.shade_key[i] = static_cast<uint8_t>(key);
+  const unsigned peers = __match_any_sync(__activemask(), key);
+  if ((threadIdx.x & 31u) == static_cast<uint32_t>(__ffs(peers) - 1))
+    atomicAdd(&wb.counts[kKeyCount + key], static_cast<uint32_t>(__popc(peers)));
+}
+
+// At the end of a keyed closest-hit launch (every thread of the block).
+__device__ __forceinline__ void finishShadeKeys(const WaveBuffers& wb) {
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&wb.counts[kTicket], 1u) == gridDim.x - 1u;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    uint32_t off = 0;
+    for (int k = 0; k < kNumKeys; ++k) {
+      const uint32_t c = atomicExch(&wb.counts[kKeyCount + k], 0u);
+      wb.counts[kKeyCursor + k] = off;
+      off += c;
+    }
+    wb.counts[kTicket] = 0u;
+  }
+}
+
 // ---- extend: closest hit --------------------------------------------------------
 // Any hit / closest hit over the trees of node format kNodes (NodeFormat).
 template <bool kAny, bool kCount, int kNodes>
@@ -134,8 +183,10 @@ __device__ __forceinline__ HitRec trace(const SceneView& sc, float4 o, float4 d,
 }
 
 // At most 64 registers per thread (4 blocks of 256 or 8 of 128 per SM).
+// keys (writeShadeKey): also the level's shading keys and their counts.
 template <bool kCount, int kNodes>
-__global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb, int parity) {
+__global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb, int parity,
+                                                   int keys) {
   // counts can exceed the capacity after an overflow (the appends are then
   // dropped and the status word set); never read past the queue
   const uint32_t n = min(wb.counts[parity], wb.capacity);
@@ -154,7 +205,9 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
     HitRec h = trace<false, kCount, kNodes>(sc, o, d, MAXD, cnt, wb.status);
     wb.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
     wb.hit_inst[i] = h.inst;
+    if (keys) writeShadeKey(sc, wb, i, h.inst, keys);
   }
+  if (keys) finishShadeKeys(wb);
   if (kCount) {
     unsigned long long a = cnt.nodes, b = cnt.tris, c = cnt.insts;
     for (int o = 16; o > 0; o >>= 1) {
@@ -181,7 +234,7 @@ constexpr int kRefill = 8;
 
 template <bool kAny, bool kCount, int kNodes>
 __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuffers& wb, uint32_t n,
-                                                   uint32_t* work, int parity) {
+                                                   uint32_t* work, int parity, int keys) {
   const uint32_t lane = threadIdx.x & 31u;
   TravCounters cnt{0u, 0u, 0u};
   int32_t stack[kStackSize];
@@ -218,6 +271,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
       } else {
         wb.hit[ray] = make_float4(st.best.t, st.best.u, st.best.v, __uint_as_float(st.best.tri));
         wb.hit_inst[ray] = st.best.inst;
+        if (keys) writeShadeKey(sc, wb, static_cast<uint32_t>(ray), st.best.inst, keys);
       }
       ray = -1;
     }
@@ -242,7 +296,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
 // k_shade for the next extend, k_extend for the shadow launch after it).
 template <bool kCount, int kNodes>
 __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, WaveBuffers wb,
-                                                              int parity) {
+                                                              int parity, int keys) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     wb.counts[parity ^ 1] = 0u;
@@ -250,14 +304,15 @@ __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, Wave
     wb.counts[4] = 0u;
     atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
   }
-  persistentTraverse<false, kCount, kNodes>(sc, wb, n, &wb.counts[3], parity);
+  persistentTraverse<false, kCount, kNodes>(sc, wb, n, &wb.counts[3], parity, keys);
+  if (keys) finishShadeKeys(wb);
 }
 
 template <bool kCount, int kNodes>
 __global__ void __launch_bounds__(256, 4) k_shadow_persistent(SceneView sc, WaveBuffers wb) {
   const uint32_t n = min(wb.counts[2], wb.capacity);
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&wb.stats[1], static_cast<unsigned long long>(n));
-  persistentTraverse<true, kCount, kNodes>(sc, wb, n, &wb.counts[4], 0);
+  persistentTraverse<true, kCount, kNodes>(sc, wb, n, &wb.counts[4], 0, 0);
 }
 
 // ---- shadow: t-bounded any hit (solveEmission, trace.wesl:91-113) ----------------
@@ -417,61 +472,6 @@ struct Child {
 };
 
 // ---- shade: one tree node per ray ------------------------------------------------
-// Shading keys: 0 miss, 1 hit beyond the depth cut (no work), 2 + material
-// kind; kNumKeys - 1 marks an empty slot.
-constexpr int kNumKeys = 19;
-
-__device__ __forceinline__ int shadeKey(const SceneView& sc, const WaveBuffers& wb, uint32_t i,
-                                        bool cut) {
-  const int32_t inst = wb.hit_inst[i];
-  if (inst < 0) return 0;
-  if (cut) return 1;
-  const uint4 meta = __ldg(reinterpret_cast<const uint4*>(sc.inst + inst) + 3);
-  return 2 + static_cast<int>((sc.mat[meta.y].volume >> kKindShift) & 15u);
-}
-
-// ---- the global shading order: a counting sort of the level by shading key ----
-constexpr int kTicket = 6, kKeyCount = 8, kKeyCursor = 32;
-
-// Shading key of every queued ray and the number of rays per key (one atomic
-// per distinct key per warp).  The block that finishes last turns the counts
-// into the scatter cursors (exclusive prefix sums) and zeroes the counts and
-// the ticket for the next level; no block waits for another.
-__global__ void __launch_bounds__(256) k_shade_keys(SceneView sc, FrameConst fc, WaveBuffers wb,
-                                                    int depth, int parity) {
-  const uint32_t n = min(wb.counts[parity], wb.capacity);
-  const uint32_t cut_depth = max(1u, min(fc.caps.trace_depth, 64u)) - 1u;
-  const bool cut = static_cast<uint32_t>(depth) >= cut_depth;
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t base = warp_global * 32u; base < n; base += warps * 32u) {
-    const uint32_t i = base + lane;
-    const int key = i < n ? shadeKey(sc, wb, i, cut) : kNumKeys - 1;
-    if (i < n) wb.shade_key[i] = static_cast<uint8_t>(key);
-    const unsigned peers = __match_any_sync(kFull, key);
-    if (key != kNumKeys - 1 && lane == static_cast<uint32_t>(__ffs(peers) - 1))
-      atomicAdd(&wb.counts[kKeyCount + key], static_cast<uint32_t>(__popc(peers)));
-  }
-  __shared__ bool s_last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = atomicAdd(&wb.counts[kTicket], 1u) == gridDim.x - 1u;
-  }
-  __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    uint32_t off = 0;
-    for (int k = 0; k < kNumKeys; ++k) {
-      const uint32_t c = atomicExch(&wb.counts[kKeyCount + k], 0u);
-      wb.counts[kKeyCursor + k] = off;
-      off += c;
-    }
-    wb.counts[kTicket] = 0u;
-  }
-}
-
 // Places every ray at its key's cursor: shade_perm lists the level's rays
 // grouped by key.
 __global__ void __launch_bounds__(256) k_shade_scatter(WaveBuffers wb, int parity) {
@@ -495,8 +495,8 @@ __global__ void __launch_bounds__(256) k_shade_scatter(WaveBuffers wb, int parit
 
 // kSort (ShadeSort): kShadeSortBlock — before shading, every block sorts its
 // slice of the queue by shading key in shared memory (counting sort);
-// kShadeSortGlobal — the level was sorted by k_shade_keys / k_shade_scatter
-// and the kernel takes rays in that order.  Either way a warp shades misses,
+// kShadeSortGlobal — the level was sorted (keys from the closest-hit kernel,
+// permutation from k_shade_scatter) and the kernel takes rays in that order.  Either way a warp shades misses,
 // cut hits or one material kind rather than a mix of code paths.
 template <int kSort>
 __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
     uint32_t i = bbase + threadIdx.x;
     if (kSort == kShadeSortGlobal && i < n) i = wb.shade_perm[i];
     if (kSort == kShadeSortBlock) {
-      const int key = i < n ? shadeKey(sc, wb, i, static_cast<uint32_t>(depth) >= cut_depth)
+      const int key = i < n ? shadeKeyOf(sc, wb.hit_inst[i], static_cast<uint32_t>(depth) >= cut_depth)
                             : kNumKeys - 1;
       if (threadIdx.x < kNumKeys) s_cnt[threadIdx.x] = 0;
       __syncthreads();
@@ -806,28 +806,29 @@ void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
 }
 
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
-                  const LaunchShape& ls, cudaStream_t s) {
+                  const LaunchShape& ls, bool cut, cudaStream_t s) {
+  const int keys = ls.shade_sort == kShadeSortGlobal ? (cut ? 2 : 1) : 0;
   const uint32_t block = ls.extend_block;
   if (ls.persistent) {  // one resident grid: 64 registers -> 65536 / (64 * block) blocks per SM
     const uint32_t g = gridFor(1024u / block);
     switch (ls.nodes * 2 + (counting ? 1 : 0)) {
-      case kNodesBinary * 2: k_extend_persistent<false, kNodesBinary><<<g, block, 0, s>>>(sc, wb, parity); break;
-      case kNodesBinary * 2 + 1: k_extend_persistent<true, kNodesBinary><<<g, block, 0, s>>>(sc, wb, parity); break;
-      case kNodesWide4 * 2: k_extend_persistent<false, kNodesWide4><<<g, block, 0, s>>>(sc, wb, parity); break;
-      case kNodesWide4 * 2 + 1: k_extend_persistent<true, kNodesWide4><<<g, block, 0, s>>>(sc, wb, parity); break;
-      case kNodesWide4Q * 2 + 1: k_extend_persistent<true, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb, parity); break;
-      default: k_extend_persistent<false, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb, parity); break;
+      case kNodesBinary * 2: k_extend_persistent<false, kNodesBinary><<<g, block, 0, s>>>(sc, wb, parity, keys); break;
+      case kNodesBinary * 2 + 1: k_extend_persistent<true, kNodesBinary><<<g, block, 0, s>>>(sc, wb, parity, keys); break;
+      case kNodesWide4 * 2: k_extend_persistent<false, kNodesWide4><<<g, block, 0, s>>>(sc, wb, parity, keys); break;
+      case kNodesWide4 * 2 + 1: k_extend_persistent<true, kNodesWide4><<<g, block, 0, s>>>(sc, wb, parity, keys); break;
+      case kNodesWide4Q * 2 + 1: k_extend_persistent<true, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb, parity, keys); break;
+      default: k_extend_persistent<false, kNodesWide4Q><<<g, block, 0, s>>>(sc, wb, parity, keys); break;
     }
     return;
   }
   const uint32_t grid = ls.grid_extend ? ls.grid_extend : gridFor(2048u / block);
   switch (ls.nodes * 2 + (counting ? 1 : 0)) {
-    case kNodesBinary * 2: k_extend<false, kNodesBinary><<<grid, block, 0, s>>>(sc, wb, parity); break;
-    case kNodesBinary * 2 + 1: k_extend<true, kNodesBinary><<<grid, block, 0, s>>>(sc, wb, parity); break;
-    case kNodesWide4 * 2: k_extend<false, kNodesWide4><<<grid, block, 0, s>>>(sc, wb, parity); break;
-    case kNodesWide4 * 2 + 1: k_extend<true, kNodesWide4><<<grid, block, 0, s>>>(sc, wb, parity); break;
-    case kNodesWide4Q * 2 + 1: k_extend<true, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb, parity); break;
-    default: k_extend<false, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb, parity); break;
+    case kNodesBinary * 2: k_extend<false, kNodesBinary><<<grid, block, 0, s>>>(sc, wb, parity, keys); break;
+    case kNodesBinary * 2 + 1: k_extend<true, kNodesBinary><<<grid, block, 0, s>>>(sc, wb, parity, keys); break;
+    case kNodesWide4 * 2: k_extend<false, kNodesWide4><<<grid, block, 0, s>>>(sc, wb, parity, keys); break;
+    case kNodesWide4 * 2 + 1: k_extend<true, kNodesWide4><<<grid, block, 0, s>>>(sc, wb, parity, keys); break;
+    case kNodesWide4Q * 2 + 1: k_extend<true, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb, parity, keys); break;
+    default: k_extend<false, kNodesWide4Q><<<grid, block, 0, s>>>(sc, wb, parity, keys); break;
   }
 }
 
@@ -835,12 +836,10 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
                 int parity, const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
-  if (ls.shade_sort == kShadeSortGlobal) {
-    const uint32_t g = gridFor(8u);  // 8 blocks of 256 per SM
-    k_shade_keys<<<g, 256, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade_scatter<<<g, 256, 0, s>>>(wb, parity);
+  if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
+    k_shade_scatter<<<gridFor(8u), 256, 0, s>>>(wb, parity);
     k_shade<kShadeSortGlobal><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    return 3;
+    return 2;
   }
   if (ls.shade_sort == kShadeSortBlock)
     k_shade<kShadeSortBlock><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);

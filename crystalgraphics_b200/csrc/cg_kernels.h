@@ -78,8 +78,9 @@ struct ChunkDesc {
 };
 
 // How the shading kernel orders a level's rays: as queued, by a counting
-// sort of each block's slice, or by a counting sort of the whole level
-// (two small kernels build a permutation; no barriers in the shading kernel).
+// sort of each block's slice, or by a counting sort of the whole level (the
+// closest-hit kernel counts keys, a scatter kernel builds the permutation; no
+// barriers in the shading kernel).
 enum ShadeSort : int { kShadeSortNone = 0, kShadeSortBlock = 1, kShadeSortGlobal = 2 };
 
 struct LaunchShape {
@@ -94,9 +95,12 @@ struct LaunchShape {
 
 void launchWavelengthTree(float* tree, float* consts, cudaStream_t s);
 void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch, cudaStream_t s);
+// With the level-wide shading order (ls.shade_sort == kShadeSortGlobal) the
+// launch also writes the level's shading keys; `cut`: the level is shaded at
+// or beyond the depth cut.
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
-                  const LaunchShape& ls, cudaStream_t s);
-// Returns the number of kernels launched (one, or three with the global sort).
+                  const LaunchShape& ls, bool cut, cudaStream_t s);
+// Returns the number of kernels launched (one, or two with the global sort).
 int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
                 int parity, const LaunchShape& ls, cudaStream_t s);
 void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,

@@ -175,6 +175,7 @@ extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
   fc.wl_tree = reinterpret_cast<const float*>(base + kOffWlTree);
   fc.wl_const = reinterpret_cast<const float*>(base + kOffWlConst);
   LaunchShape ls;  // default block sizes
+  const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
   uint64_t pix = 0, smp = 0;
   const uint64_t npx = v.pixel_count;
   while (pix < npx) {  // the chunk sequence of Renderer::enqueueChunk
@@ -187,7 +188,7 @@ extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
     launchGen(fc, wb, ch, s);
     for (uint32_t d = 0; d < plan.levels; ++d) {
       const int parity = static_cast<int>(d & 1u);
-      launchExtend(sd.view, wb, parity, false, ls, s);
+      launchExtend(sd.view, wb, parity, false, ls, d >= cut_depth, s);
       launchShade(sd.view, fc, wb, static_cast<int>(d), parity, ls, s);
       if (plan.shadow[d]) launchShadow(sd.view, wb, false, ls, s);
     }
