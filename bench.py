@@ -53,12 +53,13 @@ NODE_B = {4: 128, "4q": 64, 2: 64}
 TRI_B, INST_B, RAY_B = 48, 64, 52
 # non-tensor FP32 peak (nominal; no measured figure exists for it)
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
-# DRAM bytes (read + write) per k_extend launch of this workload, mean of the
+# DRAM bytes (read + write) per closest-hit launch of this workload, mean of the
 # seven launches of one chunk in profiles/dram_traffic_icosphere_1280x720_16spp_d8.md
-# (ncu, cold caches: an upper bound), captured with 56 closest-hit launches per
-# frame; with another chunking the frame's traffic is spread over its launches
-EXTEND_TRAFFIC_B = 183e6
-EXTEND_TRAFFIC_LAUNCHES = 56
+# (ncu, cold caches: an upper bound), captured with 14 closest-hit launches per
+# frame (64M-ray queues); with another chunking the frame's traffic is spread
+# over its launches
+EXTEND_TRAFFIC_B = 792e6
+EXTEND_TRAFFIC_LAUNCHES = 14
 
 
 def dist_env():
