@@ -213,17 +213,26 @@ int Renderer::init(int dev) {
 
 void Renderer::adoptBuffers(Renderer& prev) {
   if (prev.stream) cudaStreamSynchronize(prev.stream);
+  if (prev.stream2) cudaStreamSynchronize(prev.stream2);
   std::swap(wl_tree, prev.wl_tree);
   std::swap(wl_const, prev.wl_const);
   std::swap(wave_arena.base, prev.wave_arena.base);
   std::swap(wave_arena.size, prev.wave_arena.size);
   std::swap(wave, prev.wave);
+  std::swap(wave2_arena.base, prev.wave2_arena.base);
+  std::swap(wave2_arena.size, prev.wave2_arena.size);
+  std::swap(wave2, prev.wave2);
 }
 
 Renderer::~Renderer() {
   if (stream) cudaStreamSynchronize(stream);
+  if (stream2) cudaStreamSynchronize(stream2);
   for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
   wave_arena.release();
+  wave2_arena.release();
+  if (fork_ev) cudaEventDestroy(fork_ev);
+  if (join_ev) cudaEventDestroy(join_ev);
+  if (stream2) cudaStreamDestroy(stream2);
   if (wl_tree) cudaFree(wl_tree);
   if (wl_const) cudaFree(wl_const);
   if (ev0) cudaEventDestroy(ev0);
@@ -231,9 +240,10 @@ Renderer::~Renderer() {
   if (stream) cudaStreamDestroy(stream);
 }
 
-int Renderer::ensureWave(uint32_t capacity) {
-  if (wave_arena.base && wave.capacity == capacity) return CG_OK;
-  if (stream) CG_CUDA(cudaStreamSynchronize(stream));
+namespace {
+// Carves one set of ray queues, sample slots and counters of `capacity` rays
+// out of a fresh allocation.
+int allocWave(DeviceArena& arena, WaveBuffers& w, uint32_t capacity) {
   const size_t Q = capacity;
   const size_t parts[] = {Q * 16, Q * 16, Q * 16, Q * 16, Q * 4, Q * 4,  // ray queues
                           Q * 16, Q * 4,                                 // hits
@@ -243,41 +253,61 @@ int Renderer::ensureWave(uint32_t capacity) {
                           256,    256,    256};                          // counts, stats, status
   size_t total = 0;
   for (size_t b : parts) total += align256(b);
-  wave = WaveBuffers{};
-  int rc = wave_arena.alloc(total);
+  w = WaveBuffers{};
+  int rc = arena.alloc(total);
   if (rc != CG_OK) return rc;
-  char* p = static_cast<char*>(wave_arena.base);
+  char* p = static_cast<char*>(arena.base);
   size_t off = 0;
   auto take = [&](size_t b) {
     char* r = p + off;
     off += align256(b);
     return r;
   };
-  wave.ray_o[0] = reinterpret_cast<float4*>(take(Q * 16));
-  wave.ray_o[1] = reinterpret_cast<float4*>(take(Q * 16));
-  wave.ray_d[0] = reinterpret_cast<float4*>(take(Q * 16));
-  wave.ray_d[1] = reinterpret_cast<float4*>(take(Q * 16));
-  wave.ray_slot[0] = reinterpret_cast<uint32_t*>(take(Q * 4));
-  wave.ray_slot[1] = reinterpret_cast<uint32_t*>(take(Q * 4));
-  wave.hit = reinterpret_cast<float4*>(take(Q * 16));
-  wave.hit_inst = reinterpret_cast<int32_t*>(take(Q * 4));
-  wave.sh_o = reinterpret_cast<float4*>(take(Q * 16));
-  wave.sh_d = reinterpret_cast<float4*>(take(Q * 16));
-  wave.sh_slot = reinterpret_cast<uint32_t*>(take(Q * 4));
-  wave.s_L = reinterpret_cast<float*>(take(Q * 4));
-  wave.s_lambda = reinterpret_cast<float*>(take(Q * 4));
-  wave.s_prob = reinterpret_cast<float*>(take(Q * 4));
-  wave.shade_key = reinterpret_cast<uint8_t*>(take(Q));
-  wave.shade_perm = reinterpret_cast<uint32_t*>(take(Q * 4));
-  wave.counts = reinterpret_cast<uint32_t*>(take(256));
-  wave.stats = reinterpret_cast<unsigned long long*>(take(256));
-  wave.status = reinterpret_cast<uint32_t*>(take(256));
-  wave.capacity = capacity;
-  wave.sample_capacity = capacity;
-  CG_CUDA(cudaMemset(wave.counts, 0, 256));
-  CG_CUDA(cudaMemset(wave.stats, 0, 256));
-  CG_CUDA(cudaMemset(wave.status, 0, 256));
+  w.ray_o[0] = reinterpret_cast<float4*>(take(Q * 16));
+  w.ray_o[1] = reinterpret_cast<float4*>(take(Q * 16));
+  w.ray_d[0] = reinterpret_cast<float4*>(take(Q * 16));
+  w.ray_d[1] = reinterpret_cast<float4*>(take(Q * 16));
+  w.ray_slot[0] = reinterpret_cast<uint32_t*>(take(Q * 4));
+  w.ray_slot[1] = reinterpret_cast<uint32_t*>(take(Q * 4));
+  w.hit = reinterpret_cast<float4*>(take(Q * 16));
+  w.hit_inst = reinterpret_cast<int32_t*>(take(Q * 4));
+  w.sh_o = reinterpret_cast<float4*>(take(Q * 16));
+  w.sh_d = reinterpret_cast<float4*>(take(Q * 16));
+  w.sh_slot = reinterpret_cast<uint32_t*>(take(Q * 4));
+  w.s_L = reinterpret_cast<float*>(take(Q * 4));
+  w.s_lambda = reinterpret_cast<float*>(take(Q * 4));
+  w.s_prob = reinterpret_cast<float*>(take(Q * 4));
+  w.shade_key = reinterpret_cast<uint8_t*>(take(Q));
+  w.shade_perm = reinterpret_cast<uint32_t*>(take(Q * 4));
+  w.counts = reinterpret_cast<uint32_t*>(take(256));
+  w.stats = reinterpret_cast<unsigned long long*>(take(256));
+  w.status = reinterpret_cast<uint32_t*>(take(256));
+  w.capacity = capacity;
+  w.sample_capacity = capacity;
+  CG_CUDA(cudaMemset(w.counts, 0, 256));
+  CG_CUDA(cudaMemset(w.stats, 0, 256));
+  CG_CUDA(cudaMemset(w.status, 0, 256));
   return CG_OK;
+}
+}  // namespace
+
+int Renderer::ensureWave(uint32_t capacity) {
+  if (wave_arena.base && wave.capacity == capacity) return CG_OK;
+  if (stream) CG_CUDA(cudaStreamSynchronize(stream));
+  if (stream2) CG_CUDA(cudaStreamSynchronize(stream2));
+  wave2_arena.release();  // the second set follows the first one's capacity
+  wave2 = WaveBuffers{};
+  return allocWave(wave_arena, wave, capacity);
+}
+
+int Renderer::ensureSecondPipeline() {
+  if (!stream2) {
+    CG_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+    CG_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+    CG_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+  }
+  if (wave2_arena.base && wave2.capacity == wave.capacity) return CG_OK;
+  return allocWave(wave2_arena, wave2, wave.capacity);
 }
 
 uint32_t Renderer::chunkSamples(const SceneDev& scene, const Caps& caps) const {
@@ -288,7 +318,8 @@ uint32_t Renderer::chunkSamples(const SceneDev& scene, const Caps& caps) const {
 
 void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const ViewDev* table,
                             const ChunkDesc& ch, const Caps& caps, cudaStream_t s,
-                            RenderRecord& rec) {
+                            RenderRecord& rec, const WaveBuffers* wbp) {
+  const WaveBuffers& wb = wbp ? *wbp : wave;
   const LevelPlan plan = planLevels(caps, std::max(1u, scene.max_lobes));
   FrameConst fc;
   fc.views = table;
@@ -306,27 +337,27 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
                   : tuning.shade_sort == 3u ? kShadeSortBlock
                                             : kShadeSortGlobal;
   profBegin(CG_K_GEN, s);
-  launchGen(fc, wave, ch, s);
+  launchGen(fc, wb, ch, s);
   profEnd(s);
   ++rec.launches;
   for (uint32_t d = 0; d < plan.levels; ++d) {
     const int parity = static_cast<int>(d & 1u);
     profBegin(CG_K_EXTEND, s);
-    launchExtend(scene.view, wave, parity, counting, ls, d >= cut_depth, s);
+    launchExtend(scene.view, wb, parity, counting, ls, d >= cut_depth, s);
     profEnd(s);
     profBegin(CG_K_SHADE, s);
-    const int shade_kernels = launchShade(scene.view, fc, wave, static_cast<int>(d), parity, ls, s);
+    const int shade_kernels = launchShade(scene.view, fc, wb, static_cast<int>(d), parity, ls, s);
     profEnd(s);
     rec.launches += 1 + static_cast<uint32_t>(shade_kernels);
     if (plan.shadow[d]) {
       profBegin(CG_K_SHADOW, s);
-      launchShadow(scene.view, wave, counting, ls, s);
+      launchShadow(scene.view, wb, counting, ls, s);
       profEnd(s);
       ++rec.launches;
     }
   }
   profBegin(CG_K_RESOLVE, s);
-  launchResolve(fc, wave, ch, s);
+  launchResolve(fc, wb, ch, s);
   profEnd(s);
   ++rec.launches;
   ++rec.chunks;
@@ -345,6 +376,7 @@ int Renderer::enqueueViews(const SceneDev& scene, const std::vector<ViewDev>& vi
       return fail(CG_E_INVALID, "spp " + std::to_string(v.spp) + " exceeds the wavefront chunk of " +
                                     std::to_string(sample_cap) + " samples");
   // chunks of whole pixels, each filled up to sample_cap samples
+  std::vector<ChunkDesc> chunks;
   size_t vi = 0;
   uint64_t pix_in_view = 0, gpix = 0, gsmp = 0;
   while (vi < views.size()) {
@@ -370,7 +402,27 @@ int Renderer::enqueueViews(const SceneDev& scene, const std::vector<ViewDev>& vi
     if (ch.pixel_count == 0) break;
     gpix += ch.pixel_count;
     gsmp += ch.sample_count;
-    enqueueChunk(scene, static_cast<uint32_t>(views.size()), table, ch, caps, s, rec);
+    chunks.push_back(ch);
+  }
+  // Two pipelines: even chunks on `s` with `wave`, odd ones on stream2 with
+  // wave2, forked from and joined back into `s` by events (also inside a
+  // stream capture), so one chunk's sparse deep levels overlap the other's.
+  // Per-kernel timing keeps one pipeline.
+  const bool two = tuning.pipelines != 1u && chunks.size() > 1 && !profiling;
+  if (two) {
+    rc = ensureSecondPipeline();
+    if (rc != CG_OK) return rc;
+    CG_CUDA(cudaEventRecord(fork_ev, s));
+    CG_CUDA(cudaStreamWaitEvent(stream2, fork_ev, 0));
+  }
+  for (size_t k = 0; k < chunks.size(); ++k) {
+    const bool odd = two && (k & 1u);
+    enqueueChunk(scene, static_cast<uint32_t>(views.size()), table, chunks[k], caps,
+                 odd ? stream2 : s, rec, odd ? &wave2 : &wave);
+  }
+  if (two) {
+    CG_CUDA(cudaEventRecord(join_ev, stream2));
+    CG_CUDA(cudaStreamWaitEvent(s, join_ev, 0));
   }
   return CG_OK;
 }
@@ -410,15 +462,25 @@ void Renderer::profCollect() {
 int Renderer::beginStats(cudaStream_t s) {
   CG_CUDA(cudaMemsetAsync(wave.stats, 0, 256, s));
   CG_CUDA(cudaMemsetAsync(wave.status, 0, 256, s));
+  if (wave2_arena.base) {  // ordered before the fork that the second pipeline waits on
+    CG_CUDA(cudaMemsetAsync(wave2.stats, 0, 256, s));
+    CG_CUDA(cudaMemsetAsync(wave2.status, 0, 256, s));
+  }
   return CG_OK;
 }
 
 int Renderer::readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_stats& out) {
-  unsigned long long st[8] = {0};
-  uint32_t status = 0;
+  unsigned long long st[8] = {0}, st2[8] = {0};
+  uint32_t status = 0, status2 = 0;
   CG_CUDA(cudaMemcpyAsync(st, wave.stats, sizeof(st), cudaMemcpyDeviceToHost, s));
   CG_CUDA(cudaMemcpyAsync(&status, wave.status, sizeof(status), cudaMemcpyDeviceToHost, s));
+  if (wave2_arena.base) {  // zeroed by beginStats; after the join, in stream order on s
+    CG_CUDA(cudaMemcpyAsync(st2, wave2.stats, sizeof(st2), cudaMemcpyDeviceToHost, s));
+    CG_CUDA(cudaMemcpyAsync(&status2, wave2.status, sizeof(status2), cudaMemcpyDeviceToHost, s));
+  }
   CG_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < 8; ++k) st[k] += st2[k];
+  status |= status2;
   profCollect();
   out.samples = rec.samples;
   out.extend_rays = st[0];
@@ -827,6 +889,8 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (t->box_bits && t->box_bits != 8 && t->box_bits != 32)
     return fail(CG_E_INVALID, "box_bits must be 8 or 32");
   if (t->box_bits) g_env->tuning.box_bits = t->box_bits;
+  if (t->pipelines > 2) return fail(CG_E_INVALID, "pipelines must be 1 or 2");
+  if (t->pipelines) g_env->tuning.pipelines = t->pipelines;
   if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
   if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
   if (t->bvh_width) g_env->tuning.bvh_width = t->bvh_width;

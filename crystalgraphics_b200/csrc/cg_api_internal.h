@@ -88,9 +88,17 @@ struct Renderer {
   bool counting = false;
   // 64M rays per level queue (~9.7 GB of path state): large chunks keep every
   // level's launch full
-  cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u};
+  cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u, 2u, 0u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
+  // the second chunk pipeline (enqueueViews): its ray queues, stream and the
+  // fork / join events; allocated on first use
+  DeviceArena wave2_arena;
+  WaveBuffers wave2{};
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // allocates them (never inside a stream capture: cudaMalloc is not allowed there)
+  int ensureSecondPipeline();
 
   int init(int dev);
   // Takes over prev's wavelength tables and ray queues (after its stream has
@@ -105,9 +113,11 @@ struct Renderer {
   // and no synchronisation: the sequence can be captured into a CUDA graph.
   int enqueueViews(const SceneDev& scene, const std::vector<ViewDev>& views, const ViewDev* table,
                    const Caps& caps, cudaStream_t s, RenderRecord& rec);
-  // Enqueues one chunk covering all of `views` (their samples must fit).
+  // Enqueues one chunk covering all of `views` (their samples must fit), on
+  // the ray queues `wbp` (default: `wave`).
   void enqueueChunk(const SceneDev& scene, uint32_t view_count, const ViewDev* table,
-                    const ChunkDesc& ch, const Caps& caps, cudaStream_t s, RenderRecord& rec);
+                    const ChunkDesc& ch, const Caps& caps, cudaStream_t s, RenderRecord& rec,
+                    const WaveBuffers* wbp = nullptr);
   int beginStats(cudaStream_t s);
   int readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_stats& out);
 

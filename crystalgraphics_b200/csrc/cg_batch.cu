@@ -83,6 +83,10 @@ static int runBatch(Env& env, const SceneDev& scene, const cg_view_desc* views, 
   const Caps caps = capsOf(env.conf);
   int rc = env.ensureWave(env.tuning.queue_capacity);
   if (rc != CG_OK) return rc;
+  if (env.tuning.pipelines != 1u) {  // before any capture
+    rc = env.ensureSecondPipeline();
+    if (rc != CG_OK) return rc;
+  }
   gp = nullptr;
   const bool use_graph = env.tuning.use_graph && !env.profiling;
   if (use_graph) {
@@ -250,6 +254,14 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32
       t.persistent = var[1];
       t.shade_sort = var[2];
       t.box_bits = var[3];
+      consider(t);
+    }
+  }
+  {
+    const cg_tuning base = winner;
+    for (uint32_t pl : {1u, 2u}) {
+      cg_tuning t = base;
+      t.pipelines = pl;
       consider(t);
     }
   }

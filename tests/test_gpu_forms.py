@@ -86,6 +86,30 @@ def test_batch_uneven_views_in_many_chunks(cornell):
         assert _close(x, y) < RTOL
 
 
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_two_chunk_pipelines_render_the_same_films(cornell, use_graph):
+    """Chunks alternating between two streams with their own ray queues give
+    the same films (and ray counts) as one pipeline, in View() and in a
+    captured batch."""
+    s, g = cornell
+    views = _views(s)
+    conf = B.PathTraceConf(render_width=96, render_height=80, sample_count=4, trace_depth=4)
+    out = {}
+    for pl in (1, 2):
+        B.EnvInit(conf)
+        B.SetTuning(queue_capacity=8192, pipelines=pl, use_graph=use_graph)
+        B.View(g, B.Camera.from_c(s.camera))
+        st = B.LastStats()
+        assert st.chunks > 3
+        out[pl] = (B.ReadFilm(), st.extend_rays, st.shadow_rays, B.batch_render(g, views))
+    a, b = out[1], out[2]
+    assert _close(b[0], a[0]) < RTOL
+    assert (a[1], a[2]) == (b[1], b[2])
+    for x, y in zip(a[3], b[3]):
+        assert _close(y, x) < RTOL
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
+
+
 def test_server_results_same_alone_and_in_the_mix(cornell):
     s, g = cornell
     s2 = small_instanced()
