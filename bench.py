@@ -12,8 +12,8 @@ Metric: Msamples/s (one sample = one render() iteration of one pixel).
           library's stream), scene and film resident in HBM, L2 flushed
           between steps.
   e2e     the same metric through the C ABI with host buffers: per step
-          cg_view(scene, &camera) plus cg_film_read of the XYZ film into host
-          memory, host wall clock around synchronised steps.
+          cg_view(scene, &camera) plus cg_film_read of the XYZ film into
+          pinned host memory, host wall clock around synchronised steps.
   roofline the dominant kernel's algorithmic bytes per launch (from a
           counting pass of the same kernels) over its CUDA-event time.
   cpu_baseline the oracle (the reference's estimator restated in C++,
@@ -485,7 +485,8 @@ def run_ours(args):
     shadow = st.shadow_rays
 
     # ---- e2e through the C ABI with host buffers ----
-    host = np.empty((H_, W_, 3), np.float32)
+    # the film lands in pinned host memory (one DMA per step)
+    host = torch.empty((H_, W_, 3), dtype=torch.float32, pin_memory=True).numpy()
     d.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -621,7 +622,7 @@ def main():
                     help="node width of the traversal (0 = library default, 4)")
     ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
                     help="persistent lane-refill traversal (-1 = library default)")
-    ap.add_argument("--pipelines", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--pipelines", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="chunk pipelines of View() (0 = library default, 2)")
     ap.add_argument("--box-bits", type=int, default=0, choices=[0, 8, 32],
                     help="four-wide child box precision (0 = library default, 32)")

@@ -213,26 +213,32 @@ int Renderer::init(int dev) {
 
 void Renderer::adoptBuffers(Renderer& prev) {
   if (prev.stream) cudaStreamSynchronize(prev.stream);
-  if (prev.stream2) cudaStreamSynchronize(prev.stream2);
+  for (cudaStream_t x : prev.xstream)
+    if (x) cudaStreamSynchronize(x);
   std::swap(wl_tree, prev.wl_tree);
   std::swap(wl_const, prev.wl_const);
   std::swap(wave_arena.base, prev.wave_arena.base);
   std::swap(wave_arena.size, prev.wave_arena.size);
   std::swap(wave, prev.wave);
-  std::swap(wave2_arena.base, prev.wave2_arena.base);
-  std::swap(wave2_arena.size, prev.wave2_arena.size);
-  std::swap(wave2, prev.wave2);
+  for (int k = 0; k < kMaxPipelines - 1; ++k) {
+    std::swap(xwave_arena[k].base, prev.xwave_arena[k].base);
+    std::swap(xwave_arena[k].size, prev.xwave_arena[k].size);
+    std::swap(xwave[k], prev.xwave[k]);
+  }
 }
 
 Renderer::~Renderer() {
   if (stream) cudaStreamSynchronize(stream);
-  if (stream2) cudaStreamSynchronize(stream2);
+  for (cudaStream_t x : xstream)
+    if (x) cudaStreamSynchronize(x);
   for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
   wave_arena.release();
-  wave2_arena.release();
+  for (int k = 0; k < kMaxPipelines - 1; ++k) {
+    xwave_arena[k].release();
+    if (xjoin_ev[k]) cudaEventDestroy(xjoin_ev[k]);
+    if (xstream[k]) cudaStreamDestroy(xstream[k]);
+  }
   if (fork_ev) cudaEventDestroy(fork_ev);
-  if (join_ev) cudaEventDestroy(join_ev);
-  if (stream2) cudaStreamDestroy(stream2);
   if (wl_tree) cudaFree(wl_tree);
   if (wl_const) cudaFree(wl_const);
   if (ev0) cudaEventDestroy(ev0);
@@ -294,20 +300,27 @@ int allocWave(DeviceArena& arena, WaveBuffers& w, uint32_t capacity) {
 int Renderer::ensureWave(uint32_t capacity) {
   if (wave_arena.base && wave.capacity == capacity) return CG_OK;
   if (stream) CG_CUDA(cudaStreamSynchronize(stream));
-  if (stream2) CG_CUDA(cudaStreamSynchronize(stream2));
-  wave2_arena.release();  // the second set follows the first one's capacity
-  wave2 = WaveBuffers{};
+  for (int k = 0; k < kMaxPipelines - 1; ++k) {  // the extra sets follow the first one's capacity
+    if (xstream[k]) CG_CUDA(cudaStreamSynchronize(xstream[k]));
+    xwave_arena[k].release();
+    xwave[k] = WaveBuffers{};
+  }
   return allocWave(wave_arena, wave, capacity);
 }
 
-int Renderer::ensureSecondPipeline() {
-  if (!stream2) {
-    CG_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
-    CG_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
-    CG_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+int Renderer::ensurePipelines(int count) {
+  if (!fork_ev) CG_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+  for (int k = 0; k + 1 < count && k < kMaxPipelines - 1; ++k) {
+    if (!xstream[k]) {
+      CG_CUDA(cudaStreamCreateWithFlags(&xstream[k], cudaStreamNonBlocking));
+      CG_CUDA(cudaEventCreateWithFlags(&xjoin_ev[k], cudaEventDisableTiming));
+    }
+    if (!(xwave_arena[k].base && xwave[k].capacity == wave.capacity)) {
+      const int rc = allocWave(xwave_arena[k], xwave[k], wave.capacity);
+      if (rc != CG_OK) return rc;
+    }
   }
-  if (wave2_arena.base && wave2.capacity == wave.capacity) return CG_OK;
-  return allocWave(wave2_arena, wave2, wave.capacity);
+  return CG_OK;
 }
 
 uint32_t Renderer::chunkSamples(const SceneDev& scene, const Caps& caps) const {
@@ -404,25 +417,27 @@ int Renderer::enqueueViews(const SceneDev& scene, const std::vector<ViewDev>& vi
     gsmp += ch.sample_count;
     chunks.push_back(ch);
   }
-  // Two pipelines: even chunks on `s` with `wave`, odd ones on stream2 with
-  // wave2, forked from and joined back into `s` by events (also inside a
-  // stream capture), so one chunk's sparse deep levels overlap the other's.
-  // Per-kernel timing keeps one pipeline.
-  const bool two = tuning.pipelines != 1u && chunks.size() > 1 && !profiling;
-  if (two) {
-    rc = ensureSecondPipeline();
+  // P pipelines: chunk k runs on pipeline k mod P; pipeline 0 is `s` with
+  // `wave`, the others are extra streams with their own ray queues, forked
+  // from and joined back into `s` by events (also inside a stream capture), so
+  // one chunk's sparse deep levels overlap another's launches.  Per-kernel
+  // timing keeps one pipeline.
+  int P = profiling ? 1 : static_cast<int>(std::clamp(tuning.pipelines, 1u, uint32_t(kMaxPipelines)));
+  P = std::min<int>(P, static_cast<int>(chunks.size()));
+  if (P > 1) {
+    rc = ensurePipelines(P);
     if (rc != CG_OK) return rc;
     CG_CUDA(cudaEventRecord(fork_ev, s));
-    CG_CUDA(cudaStreamWaitEvent(stream2, fork_ev, 0));
+    for (int k = 0; k + 1 < P; ++k) CG_CUDA(cudaStreamWaitEvent(xstream[k], fork_ev, 0));
   }
   for (size_t k = 0; k < chunks.size(); ++k) {
-    const bool odd = two && (k & 1u);
+    const int p = static_cast<int>(k % static_cast<size_t>(P));
     enqueueChunk(scene, static_cast<uint32_t>(views.size()), table, chunks[k], caps,
-                 odd ? stream2 : s, rec, odd ? &wave2 : &wave);
+                 p ? xstream[p - 1] : s, rec, p ? &xwave[p - 1] : &wave);
   }
-  if (two) {
-    CG_CUDA(cudaEventRecord(join_ev, stream2));
-    CG_CUDA(cudaStreamWaitEvent(s, join_ev, 0));
+  for (int k = 0; k + 1 < P; ++k) {
+    CG_CUDA(cudaEventRecord(xjoin_ev[k], xstream[k]));
+    CG_CUDA(cudaStreamWaitEvent(s, xjoin_ev[k], 0));
   }
   return CG_OK;
 }
@@ -462,37 +477,41 @@ void Renderer::profCollect() {
 int Renderer::beginStats(cudaStream_t s) {
   CG_CUDA(cudaMemsetAsync(wave.stats, 0, 256, s));
   CG_CUDA(cudaMemsetAsync(wave.status, 0, 256, s));
-  if (wave2_arena.base) {  // ordered before the fork that the second pipeline waits on
-    CG_CUDA(cudaMemsetAsync(wave2.stats, 0, 256, s));
-    CG_CUDA(cudaMemsetAsync(wave2.status, 0, 256, s));
-  }
+  for (int k = 0; k < kMaxPipelines - 1; ++k)
+    if (xwave_arena[k].base) {  // ordered before the fork the extra pipelines wait on
+      CG_CUDA(cudaMemsetAsync(xwave[k].stats, 0, 256, s));
+      CG_CUDA(cudaMemsetAsync(xwave[k].status, 0, 256, s));
+    }
   return CG_OK;
 }
 
 int Renderer::readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_stats& out) {
-  unsigned long long st[8] = {0}, st2[8] = {0};
-  uint32_t status = 0, status2 = 0;
-  CG_CUDA(cudaMemcpyAsync(st, wave.stats, sizeof(st), cudaMemcpyDeviceToHost, s));
-  CG_CUDA(cudaMemcpyAsync(&status, wave.status, sizeof(status), cudaMemcpyDeviceToHost, s));
-  if (wave2_arena.base) {  // zeroed by beginStats; after the join, in stream order on s
-    CG_CUDA(cudaMemcpyAsync(st2, wave2.stats, sizeof(st2), cudaMemcpyDeviceToHost, s));
-    CG_CUDA(cudaMemcpyAsync(&status2, wave2.status, sizeof(status2), cudaMemcpyDeviceToHost, s));
-  }
+  unsigned long long st[kMaxPipelines][8] = {};
+  uint32_t status[kMaxPipelines] = {};
+  CG_CUDA(cudaMemcpyAsync(st[0], wave.stats, sizeof(st[0]), cudaMemcpyDeviceToHost, s));
+  CG_CUDA(cudaMemcpyAsync(&status[0], wave.status, 4, cudaMemcpyDeviceToHost, s));
+  for (int k = 0; k < kMaxPipelines - 1; ++k)
+    if (xwave_arena[k].base) {  // zeroed by beginStats; after the join, in stream order on s
+      CG_CUDA(cudaMemcpyAsync(st[k + 1], xwave[k].stats, sizeof(st[0]), cudaMemcpyDeviceToHost, s));
+      CG_CUDA(cudaMemcpyAsync(&status[k + 1], xwave[k].status, 4, cudaMemcpyDeviceToHost, s));
+    }
   CG_CUDA(cudaStreamSynchronize(s));
-  for (int k = 0; k < 8; ++k) st[k] += st2[k];
-  status |= status2;
+  for (int p = 1; p < kMaxPipelines; ++p) {
+    for (int k = 0; k < 8; ++k) st[0][k] += st[p][k];
+    status[0] |= status[p];
+  }
   profCollect();
   out.samples = rec.samples;
-  out.extend_rays = st[0];
-  out.shadow_rays = st[1];
-  out.node_visits = st[2];
-  out.tri_tests = st[3];
-  out.inst_visits = st[4];
+  out.extend_rays = st[0][0];
+  out.shadow_rays = st[0][1];
+  out.node_visits = st[0][2];
+  out.tri_tests = st[0][3];
+  out.inst_visits = st[0][4];
   out.chunks = rec.chunks;
   out.kernel_launches = rec.launches;
   out.device_ms = ms;
-  if (status & 1u) return fail(CG_E_DEVICE, "traversal stack overflow in a kernel");
-  if (status & 2u) return fail(CG_E_DEVICE, "ray queue overflow in a kernel");
+  if (status[0] & 1u) return fail(CG_E_DEVICE, "traversal stack overflow in a kernel");
+  if (status[0] & 2u) return fail(CG_E_DEVICE, "ray queue overflow in a kernel");
   return CG_OK;
 }
 
@@ -519,6 +538,7 @@ Env::~Env() {
   if (views_dev) cudaFree(views_dev);
   if (film) cudaFree(film);
   if (rgba) cudaFree(rgba);
+  if (film_pack) cudaFree(film_pack);
 }
 
 // `prev` (may be null) is the environment being replaced: on the same device
@@ -548,6 +568,7 @@ static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& o
   const size_t npx = size_t(env->conf.render_width) * env->conf.render_height;
   CG_CUDA(cudaMalloc(&env->film, npx * sizeof(float4)));
   CG_CUDA(cudaMalloc(&env->rgba, npx * sizeof(uchar4)));
+  CG_CUDA(cudaMalloc(&env->film_pack, npx * 3 * sizeof(float)));
   CG_CUDA(cudaMemset(env->film, 0, npx * sizeof(float4)));
   CG_CUDA(cudaMemset(env->rgba, 0, npx * sizeof(uchar4)));
   out = std::move(env);
@@ -811,18 +832,13 @@ CG_API int cg_film_read(void* host, size_t bytes, int format) {
   if (format != CG_FILM_XYZ32F && format != CG_FILM_RGB32F)
     return fail(CG_E_INVALID, "unknown film format");
   if (bytes < npx * 12) return fail(CG_E_INVALID, "buffer too small for 3 floats per pixel");
-  // strided copy: 12 of every 16 bytes per pixel
-  CG_CUDA(cudaMemcpy2DAsync(host, 12, env.film, 16, 12, npx, cudaMemcpyDeviceToHost, env.stream));
+  // packed (and for RGB converted) on the device, then one contiguous copy
+  // (a direct DMA when `host` is pinned)
+  launchFilmPack(static_cast<const float4*>(env.film), env.film_pack, npx,
+                 format == CG_FILM_RGB32F, env.stream);
+  CG_CUDA(cudaGetLastError());
+  CG_CUDA(cudaMemcpyAsync(host, env.film_pack, npx * 12, cudaMemcpyDeviceToHost, env.stream));
   CG_CUDA(cudaStreamSynchronize(env.stream));
-  if (format == CG_FILM_RGB32F) {
-    float* o = static_cast<float*>(host);
-    for (size_t i = 0; i < npx; ++i) {  // xyz_to_srgb of physics/srgb.wesl:6-10
-      const float X = o[3 * i], Y = o[3 * i + 1], Z = o[3 * i + 2];
-      o[3 * i] = (2.36461385f * X + -0.89654057f * Y) + -0.46807328f * Z;
-      o[3 * i + 1] = (-0.51516621f * X + 1.4264081f * Y) + 0.0887581f * Z;
-      o[3 * i + 2] = (0.0052037f * X + -0.01440816f * Y) + 1.00920446f * Z;
-    }
-  }
   return CG_OK;
 }
 
@@ -889,7 +905,8 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (t->box_bits && t->box_bits != 8 && t->box_bits != 32)
     return fail(CG_E_INVALID, "box_bits must be 8 or 32");
   if (t->box_bits) g_env->tuning.box_bits = t->box_bits;
-  if (t->pipelines > 2) return fail(CG_E_INVALID, "pipelines must be 1 or 2");
+  if (t->pipelines > static_cast<uint32_t>(Renderer::kMaxPipelines))
+    return fail(CG_E_INVALID, "pipelines must be 1 to 4");
   if (t->pipelines) g_env->tuning.pipelines = t->pipelines;
   if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
   if (t->shade_block) g_env->tuning.shade_block = t->shade_block;

@@ -91,14 +91,17 @@ struct Renderer {
   cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u, 2u, 0u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
-  // the second chunk pipeline (enqueueViews): its ray queues, stream and the
-  // fork / join events; allocated on first use
-  DeviceArena wave2_arena;
-  WaveBuffers wave2{};
-  cudaStream_t stream2 = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
-  // allocates them (never inside a stream capture: cudaMalloc is not allowed there)
-  int ensureSecondPipeline();
+  // the extra chunk pipelines of enqueueViews (pipeline 0 is `stream` with
+  // `wave`): their ray queues, streams and join events, and the fork event;
+  // allocated on first use
+  static constexpr int kMaxPipelines = 4;
+  DeviceArena xwave_arena[kMaxPipelines - 1];
+  WaveBuffers xwave[kMaxPipelines - 1]{};
+  cudaStream_t xstream[kMaxPipelines - 1] = {};
+  cudaEvent_t fork_ev = nullptr, xjoin_ev[kMaxPipelines - 1] = {};
+  // allocates pipelines 1 .. count - 1 (never inside a stream capture:
+  // cudaMalloc is not allowed there)
+  int ensurePipelines(int count);
 
   int init(int dev);
   // Takes over prev's wavelength tables and ray queues (after its stream has
@@ -154,6 +157,7 @@ struct Env : Renderer {
   cg_conf conf{};
   void* film = nullptr;   // float4 per pixel
   void* rgba = nullptr;   // uchar4 per pixel
+  float* film_pack = nullptr;  // three floats per pixel: the XYZ / RGB readback
   // FrameHistory (src/wgpu/frame_history.h)
   bool has_prev = false;
   uint64_t prev_tag = 0;

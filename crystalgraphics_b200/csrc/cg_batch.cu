@@ -83,8 +83,8 @@ static int runBatch(Env& env, const SceneDev& scene, const cg_view_desc* views, 
   const Caps caps = capsOf(env.conf);
   int rc = env.ensureWave(env.tuning.queue_capacity);
   if (rc != CG_OK) return rc;
-  if (env.tuning.pipelines != 1u) {  // before any capture
-    rc = env.ensureSecondPipeline();
+  if (env.tuning.pipelines > 1u) {  // before any capture
+    rc = env.ensurePipelines(static_cast<int>(env.tuning.pipelines));
     if (rc != CG_OK) return rc;
   }
   gp = nullptr;
@@ -259,7 +259,7 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32
   }
   {
     const cg_tuning base = winner;
-    for (uint32_t pl : {1u, 2u}) {
+    for (uint32_t pl : {1u, 2u, 3u, 4u}) {
       cg_tuning t = base;
       t.pipelines = pl;
       consider(t);

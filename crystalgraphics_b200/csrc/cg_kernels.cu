@@ -880,6 +880,34 @@ void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc&
   k_resolve<<<(n + 127) / 128, 128, 0, s>>>(fc, wb, ch);
 }
 
+// Film readback: the float4 film packed to three floats per pixel, as XYZ or
+// converted to linear sRGB (xyz_to_srgb of physics/srgb.wesl:6-10, rounded
+// after every product and sum like the host loop it replaces, so no fused
+// multiply-adds).
+__global__ void k_film_pack(const float4* __restrict__ film, float* __restrict__ out, size_t npx,
+                            int rgb) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= npx) return;
+  const float4 f = film[i];
+  float a = f.x, b = f.y, c = f.z;
+  if (rgb) {
+    a = __fadd_rn(__fadd_rn(__fmul_rn(2.36461385f, f.x), __fmul_rn(-0.89654057f, f.y)),
+                  __fmul_rn(-0.46807328f, f.z));
+    b = __fadd_rn(__fadd_rn(__fmul_rn(-0.51516621f, f.x), __fmul_rn(1.4264081f, f.y)),
+                  __fmul_rn(0.0887581f, f.z));
+    c = __fadd_rn(__fadd_rn(__fmul_rn(0.0052037f, f.x), __fmul_rn(-0.01440816f, f.y)),
+                  __fmul_rn(1.00920446f, f.z));
+  }
+  out[3 * i] = a;
+  out[3 * i + 1] = b;
+  out[3 * i + 2] = c;
+}
+
+void launchFilmPack(const float4* film, float* out, size_t npx, bool rgb, cudaStream_t s) {
+  if (npx == 0) return;
+  k_film_pack<<<static_cast<unsigned>((npx + 255) / 256), 256, 0, s>>>(film, out, npx, rgb ? 1 : 0);
+}
+
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
                         int4* out_ids, uint32_t* status, int nodes, cudaStream_t s) {
   if (n == 0) return;

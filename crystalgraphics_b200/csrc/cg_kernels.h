@@ -107,6 +107,8 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s);
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
                    cudaStream_t s);
+// Packs a float4 film to three floats per pixel (XYZ, or linear sRGB).
+void launchFilmPack(const float4* film, float* out, size_t npx, bool rgb, cudaStream_t s);
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
                         int4* out_ids, uint32_t* status, int nodes, cudaStream_t s);
 

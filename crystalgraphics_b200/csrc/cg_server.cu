@@ -100,14 +100,15 @@ struct cg_server_s {
 namespace cg {
 namespace {
 
-// Film bytes plus the path state the request can occupy in one chunk.
+// Film bytes (the float4 film and its packed three-float readback) plus the
+// path state the request can occupy in one chunk.
 size_t requestBytes(const cg_server_s& sv, const SceneDev& scene, const cg_request& r) {
   const size_t npx = size_t(r.view.width) * r.view.height;
   const LevelPlan plan = planLevels(capsOf(sv.conf), std::max(1u, scene.max_lobes));
   const size_t per_sample = 12 + plan.max_product * (36 + 20 + 36);
   const size_t samples =
       std::min<size_t>(npx * r.view.spp, sv.lanes[0].rend.chunkSamples(scene, capsOf(sv.conf)));
-  return npx * 16 + samples * per_sample;
+  return npx * (16 + 12) + samples * per_sample;
 }
 
 void finishRequest(cg_server_s& sv, ServerReq* r, int status) {
@@ -243,7 +244,7 @@ void serverLoop(cg_server_s* sv) {
         continue;
       }
       sv->pending.pop_front();
-      const size_t fb = size_t(r->npx) * 16;
+      const size_t fb = size_t(r->npx) * (16 + 12);  // film, then its packed readback
       void* film = nullptr;
       if (cudaMallocAsync(&film, fb, sv->alloc_stream) != cudaSuccess ||
           cudaStreamSynchronize(sv->alloc_stream) != cudaSuccess) {
@@ -327,8 +328,12 @@ void serverLoop(cg_server_s* sv) {
       if (complete || (r->cancelled && r->resolved == r->next_pixel)) {
         int st = CG_E_CANCELLED;
         if (complete && !r->cancelled) {
-          st = cudaMemcpy2DAsync(r->out, 12, r->film, 16, 12, r->npx, cudaMemcpyDeviceToHost, s) ==
-                       cudaSuccess
+          // packed on the device behind the film, then one contiguous copy
+          float* packed = reinterpret_cast<float*>(r->film + r->npx);
+          launchFilmPack(r->film, packed, r->npx, false, s);
+          st = cudaGetLastError() == cudaSuccess &&
+                       cudaMemcpyAsync(r->out, packed, size_t(r->npx) * 12,
+                                       cudaMemcpyDeviceToHost, s) == cudaSuccess
                    ? CG_OK
                    : CG_E_CUDA;
         }

@@ -361,9 +361,9 @@ typedef struct cg_tuning {
                            queued, 0 = keep */
   uint32_t box_bits;    /* four-wide child boxes: 32 (default) = floats in
                            128-byte nodes, 8 = 8-bit offsets in 64-byte nodes */
-  uint32_t pipelines;   /* chunk pipelines of View() and cg_batch_render: 2
-                           (default) = alternate chunks between two streams with
-                           their own ray queues, 1 = one; 0 = keep */
+  uint32_t pipelines;   /* chunk pipelines of View() and cg_batch_render, 1 to
+                           4: chunk k runs on stream k mod pipelines with that
+                           stream's own ray queues (2 = default); 0 = keep */
   uint32_t _pad;
 } cg_tuning;
 CG_API int cg_set_tuning(const cg_tuning* tuning);

@@ -57,6 +57,33 @@ def test_batch_matches_single_views(cornell):
     B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
 
 
+def test_film_read_formats(cornell):
+    """XYZ, linear sRGB (the xyz_to_srgb matrix, each product and sum rounded
+    to float32 in the same order) and rgba8 readbacks of one film, into
+    pageable and pinned host buffers."""
+    import torch
+
+    s, g = cornell
+    B.EnvInit(B.PathTraceConf(render_width=61, render_height=37, sample_count=2, trace_depth=3))
+    B.View(g, B.Camera.from_c(s.camera))
+    xyz = B.ReadFilm(_abi.CG_FILM_XYZ32F)
+    rgb = B.ReadFilm(_abi.CG_FILM_RGB32F)
+    pinned = torch.empty((37, 61, 3), dtype=torch.float32, pin_memory=True).numpy()
+    B.ReadFilm(_abi.CG_FILM_XYZ32F, out=pinned)
+    assert np.array_equal(pinned, xyz)
+    assert float(np.abs(xyz).max()) > 0
+    f = np.float32
+    X, Y, Z = xyz[..., 0], xyz[..., 1], xyz[..., 2]
+    m = [(2.36461385, -0.89654057, -0.46807328), (-0.51516621, 1.4264081, 0.0887581),
+         (0.0052037, -0.01440816, 1.00920446)]
+    for c, (a, b, d) in enumerate(m):
+        want = (f(a) * X + f(b) * Y) + f(d) * Z
+        assert np.array_equal(rgb[..., c], want), c
+    rgba = B.ReadFilm(_abi.CG_FILM_RGBA8)
+    assert rgba.shape == (37, 61, 4) and int(rgba[..., 3].min()) == 255
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
+
+
 def test_batch_graph_replay_is_stable(cornell):
     s, g = cornell
     B.SetTuning(use_graph=1)
@@ -87,26 +114,28 @@ def test_batch_uneven_views_in_many_chunks(cornell):
 
 
 @pytest.mark.parametrize("use_graph", [0, 1])
-def test_two_chunk_pipelines_render_the_same_films(cornell, use_graph):
-    """Chunks alternating between two streams with their own ray queues give
+def test_chunk_pipelines_render_the_same_films(cornell, use_graph):
+    """Chunks spread over two or three streams with their own ray queues give
     the same films (and ray counts) as one pipeline, in View() and in a
     captured batch."""
     s, g = cornell
     views = _views(s)
     conf = B.PathTraceConf(render_width=96, render_height=80, sample_count=4, trace_depth=4)
     out = {}
-    for pl in (1, 2):
+    for pl in (1, 2, 3):
         B.EnvInit(conf)
         B.SetTuning(queue_capacity=8192, pipelines=pl, use_graph=use_graph)
         B.View(g, B.Camera.from_c(s.camera))
         st = B.LastStats()
         assert st.chunks > 3
         out[pl] = (B.ReadFilm(), st.extend_rays, st.shadow_rays, B.batch_render(g, views))
-    a, b = out[1], out[2]
-    assert _close(b[0], a[0]) < RTOL
-    assert (a[1], a[2]) == (b[1], b[2])
-    for x, y in zip(a[3], b[3]):
-        assert _close(y, x) < RTOL
+    a = out[1]
+    for pl in (2, 3):
+        b = out[pl]
+        assert _close(b[0], a[0]) < RTOL
+        assert (a[1], a[2]) == (b[1], b[2])
+        for x, y in zip(a[3], b[3]):
+            assert _close(y, x) < RTOL
     B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
 
 
