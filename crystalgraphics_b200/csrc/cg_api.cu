@@ -894,26 +894,30 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
   if (!t) return fail(CG_E_INVALID, "null argument");
   std::lock_guard<std::mutex> lk(g_env_mu);
   if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  // every field is checked before any is applied
   auto okBlock = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 1024 && b % 32 == 0); };
   if (!okBlock(t->extend_block) || !okBlock(t->shade_block))
     return fail(CG_E_INVALID, "block sizes must be multiples of 32 in [32, 1024]");
+  if (t->extend_block > 256u)  // the traversal kernels' launch bounds
+    return fail(CG_E_INVALID, "extend_block must be at most 256");
   if (t->queue_capacity && (t->queue_capacity < 4096 || t->queue_capacity > (1u << 28)))
     return fail(CG_E_INVALID, "queue capacity must be in [4096, 2^28]");
-  if (t->queue_capacity) g_env->tuning.queue_capacity = t->queue_capacity;
   if (t->bvh_width && t->bvh_width != 2 && t->bvh_width != 4)
     return fail(CG_E_INVALID, "bvh_width must be 2 or 4");
   if (t->box_bits && t->box_bits != 8 && t->box_bits != 32)
     return fail(CG_E_INVALID, "box_bits must be 8 or 32");
-  if (t->box_bits) g_env->tuning.box_bits = t->box_bits;
   if (t->pipelines > static_cast<uint32_t>(Renderer::kMaxPipelines))
     return fail(CG_E_INVALID, "pipelines must be 1 to 4");
-  if (t->pipelines) g_env->tuning.pipelines = t->pipelines;
-  if (t->extend_block) g_env->tuning.extend_block = t->extend_block;
-  if (t->shade_block) g_env->tuning.shade_block = t->shade_block;
-  if (t->bvh_width) g_env->tuning.bvh_width = t->bvh_width;
-  if (t->persistent) g_env->tuning.persistent = t->persistent == 2u ? 2u : 1u;
   if (t->shade_sort > 3u) return fail(CG_E_INVALID, "shade_sort must be 0..3");
-  if (t->shade_sort) g_env->tuning.shade_sort = t->shade_sort;
+  cg_tuning& g = g_env->tuning;
+  if (t->queue_capacity) g.queue_capacity = t->queue_capacity;
+  if (t->box_bits) g.box_bits = t->box_bits;
+  if (t->pipelines) g.pipelines = t->pipelines;
+  if (t->extend_block) g.extend_block = t->extend_block;
+  if (t->shade_block) g.shade_block = t->shade_block;
+  if (t->bvh_width) g.bvh_width = t->bvh_width;
+  if (t->persistent) g.persistent = t->persistent == 2u ? 2u : 1u;
+  if (t->shade_sort) g.shade_sort = t->shade_sort;
   g_env->tuning.use_graph = t->use_graph;
   g_env->dropAllGraphs();
   return CG_OK;

@@ -300,11 +300,39 @@ __device__ __forceinline__ void travInit(TravState& s, float4 o, float4 d, float
   s.best = HitRec{tmax, 0.0f, 0.0f, -1, 0u};
 }
 
+// Traversal stacks of the resumable walk.  LocalStack: all entries in local
+// memory.  ShortStack: the first kShort entries live in
+// shared memory, one column per thread (entry i of thread t at i * stride + t,
+// so a warp's accesses hit 32 different banks at any depths), the rest in
+// local memory.  Most walks stay within the shared part, so pushes and pops do
+// not compete with node fetches for L1 and L2.
+struct LocalStack {
+  int32_t e[kStackSize];
+  __device__ __forceinline__ int32_t get(int i) const { return e[i]; }
+  __device__ __forceinline__ void set(int i, int32_t v) { e[i] = v; }
+};
+
+template <int kShort>
+struct ShortStack {
+  int32_t* col;      // this thread's column of the block's shared stack
+  uint32_t stride;   // threads per block
+  int32_t spill[kStackSize - kShort];
+  __device__ __forceinline__ int32_t get(int i) const {
+    return i < kShort ? col[i * stride] : spill[i - kShort];
+  }
+  __device__ __forceinline__ void set(int i, int32_t v) {
+    if (i < kShort)
+      col[i * stride] = v;
+    else
+      spill[i - kShort] = v;
+  }
+};
+
 // Runs at most `budget` steps (a node visit, a leaf, or a return to the
 // TLAS); returns true when the ray is finished (s.best holds its hit; with
 // kAny the first hit below s.best.t finishes it).
-template <bool kAny, bool kCount, int kNodes = kNodesBinary>
-__device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int32_t* stack,
+template <bool kAny, bool kCount, int kNodes, class Stack>
+__device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, Stack& stack,
                                           int budget, TravCounters& cnt, uint32_t* status) {
   for (int step = 0; step < budget; ++step) {
     const int32_t node = s.node;
@@ -336,7 +364,7 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
       cswap(k1, l1, k3, l3);
       cswap(k1, l1, k2, l2);
       if (k0 == INFINITY) {
-        s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+        s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
         continue;
       }
       const int pushes = (k1 != INFINITY) + (k2 != INFINITY) + (k3 != INFINITY);
@@ -345,9 +373,9 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
         s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
         return true;
       }
-      if (k3 != INFINITY) stack[s.sp++] = l3;
-      if (k2 != INFINITY) stack[s.sp++] = l2;
-      if (k1 != INFINITY) stack[s.sp++] = l1;
+      if (k3 != INFINITY) stack.set(s.sp++, l3);
+      if (k2 != INFINITY) stack.set(s.sp++, l2);
+      if (k1 != INFINITY) stack.set(s.sp++, l1);
       s.node = l0;
       continue;
     }
@@ -382,14 +410,14 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
           s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
           return true;
         }
-        stack[s.sp++] = far;
+        stack.set(s.sp++, far);
         s.node = near;
       } else if (h0) {
         s.node = n3.x;
       } else if (h1) {
         s.node = n3.y;
       } else {
-        s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+        s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
       }
       continue;
     }
@@ -400,14 +428,14 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
       s.dx = s.wdx; s.dy = s.wdy; s.dz = s.wdz;
       s.idx = safeInv(s.dx); s.idy = safeInv(s.dy); s.idz = safeInv(s.dz);
       s.oix = s.ox * s.idx; s.oiy = s.oy * s.idy; s.oiz = s.oz * s.idz;
-      s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+      s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
       continue;
     }
     const uint32_t first = static_cast<uint32_t>(~node) >> 3;
     const uint32_t count = static_cast<uint32_t>(~node) & 7u;
     if (s.cur_inst < 0) {
       if (count == 0u) {
-        s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+        s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
         continue;
       }
       const float4* ipf = reinterpret_cast<const float4*>(sc.inst + first);
@@ -423,7 +451,7 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
         s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
         return true;
       }
-      stack[s.sp++] = kToTlas;
+      stack.set(s.sp++, kToTlas);
       s.cur_inst = static_cast<int32_t>(first);
       // blas_root (binary) or blas4_root (four-wide)
       s.node = static_cast<int32_t>(kNodes == kNodesBinary ? meta.x : meta.w);
@@ -443,7 +471,7 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, int
         if (kAny) return true;
       }
     }
-    s.node = s.sp > 0 ? stack[--s.sp] : kDone;
+    s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
   }
   return false;
 }

@@ -258,7 +258,20 @@ def test_autotune_returns_a_valid_tuning(cornell):
     for x, y in zip(B.batch_render(g, views), ref):
         assert _close(x, y) < RTOL
     B.SetTuning(queue_capacity=64 << 20, extend_block=128, shade_block=128, use_graph=1,
-                bvh_width=4, persistent=False, shade_sort=True, box_bits=32)
+                bvh_width=4, persistent=True, shade_sort=True, box_bits=32, pipelines=2)
+
+
+def test_tuning_rejects_out_of_range_values(cornell):
+    before = B.GetTuning()
+    for bad in (dict(extend_block=512), dict(extend_block=48), dict(shade_block=2048),
+                dict(queue_capacity=1024), dict(pipelines=5), dict(bvh_width=3),
+                dict(box_bits=16)):
+        with pytest.raises(B.Error) as e:
+            B.SetTuning(**bad)
+        assert e.value.code == _abi.CG_E_INVALID, bad
+    after = B.GetTuning()
+    assert (after.extend_block, after.queue_capacity, after.pipelines) == \
+        (before.extend_block, before.queue_capacity, before.pipelines)
 
 
 def test_gltf_scene_renders_like_the_in_memory_scene(tmp_path, cornell):
