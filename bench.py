@@ -264,6 +264,7 @@ BATCH_DEPTH = 12     # the instanced scene's trace depth
 SERVE_DEPTH = 12     # one conf serves all four resident scenes
 SERVE_RATES = (50, 200, 2000)
 SERVE_REQUESTS = 48
+SERVE_REPEATS = 3
 
 
 def _rel_diff(a, b):
@@ -361,7 +362,10 @@ def served_form(B, torch):
     """Poisson request streams over four resident scenes (the icosphere and
     three instanced scenes with 4096, 2048 and 8192 instances) through the
     continuous-batching server; the plain baseline serves the same requests one
-    at a time through EnvInit/View/ReadFilm in arrival order."""
+    at a time through EnvInit/View/ReadFilm in arrival order.  Host-side work
+    (admission, film copy-out into fresh caller buffers) varies on a shared
+    host, so every rate runs SERVE_REPEATS times and the run with the median
+    throughput is reported; plain service times are per-request medians."""
     from crystalgraphics_b200 import scenes
     resident = [scenes.icosphere_scene(), scenes.instanced_scene(),
                 scenes.instanced_scene(instances=2048, seed=5),
@@ -374,12 +378,14 @@ def served_form(B, torch):
     total = sum(req_samples)
     out = {"workload": "4 resident scenes, requests of {256^2, 512^2, 1280x720, 1920x1080} x "
                        "spp {1,4,16}, random poses, Poisson arrivals, depth 12",
-           "requests_per_rate": SERVE_REQUESTS, "samples_per_rate": total, "rates": []}
+           "requests_per_rate": SERVE_REQUESTS, "samples_per_rate": total,
+           "repeats": SERVE_REPEATS, "rates": []}
     # warm the server path once
     with B.Server(gs, 32 << 30) as sv:
         _, si, p, d, w, h, spp, seed = base[0]
         sv.wait(sv.submit(si, p, d, w, h, spp, seed))
-    for rate in SERVE_RATES:
+
+    def serve_once(rate):
         with B.Server(gs, 32 << 30) as sv:
             ids = []
             t_start = time.perf_counter()
@@ -389,18 +395,28 @@ def served_form(B, torch):
                     time.sleep(delay)
                 ids.append(sv.submit(si, p, d, w, h, spp, seed))
             res = [sv.wait(i)[1] for i in ids]
-            peak = sv.stats().peak_bytes
+            st = sv.stats()
         lat = np.array([r.finish_s - r.submit_s for r in res]) * 1e3
         span = max(r.finish_s for r in res) - min(r.submit_s for r in res)
-        out["rates"].append({"rate_hz": rate, "msamples_per_s": total / span / 1e6,
-                             "p50_ms": float(np.percentile(lat, 50)),
-                             "p99_ms": float(np.percentile(lat, 99)),
-                             "peak_admitted_bytes": int(peak)})
-    # plain: per-request service time measured, FIFO over the same arrivals
-    service = []
-    for (_, si, p, d, w, h, spp, seed) in base:
-        _, wall, _ = _plain_render(B, gs[si], p, d, w, h, spp, seed, SERVE_DEPTH)
-        service.append(wall)
+        return {"rate_hz": rate, "msamples_per_s": total / span / 1e6,
+                "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)),
+                "peak_admitted_bytes": int(st.peak_bytes), "chunks": int(st.chunks),
+                "busy_s": st.busy_s, "span_s": span, "copy_out_s": st.copy_out_s}
+
+    for rate in SERVE_RATES:
+        runs = sorted((serve_once(rate) for _ in range(SERVE_REPEATS)),
+                      key=lambda e: e["msamples_per_s"])
+        entry = runs[len(runs) // 2]
+        entry["msamples_per_s_runs"] = [e["msamples_per_s"] for e in runs]
+        out["rates"].append(entry)
+    # plain: per-request service time (median of SERVE_REPEATS), FIFO over the same arrivals
+    walls = [[] for _ in base]
+    for _ in range(SERVE_REPEATS):
+        for k, (_, si, p, d, w, h, spp, seed) in enumerate(base):
+            _, wall, _ = _plain_render(B, gs[si], p, d, w, h, spp, seed, SERVE_DEPTH)
+            walls[k].append(wall)
+    service = [float(np.median(x)) for x in walls]
     for entry, rate in zip(out["rates"], SERVE_RATES):
         free_at, lat, first = 0.0, [], base[0][0] / rate
         for (t_arr, *_), sv_s in zip(base, service):
@@ -410,8 +426,9 @@ def served_form(B, torch):
         entry["plain_p50_ms"] = float(np.percentile(lat, 50))
         entry["plain_p99_ms"] = float(np.percentile(lat, 99))
         entry["plain_msamples_per_s"] = total / (free_at - first) / 1e6
-    out["plain"] = ("one request at a time through EnvInit/View/ReadFilm: service times "
-                    "measured, latencies from the same arrival times in FIFO order")
+    out["plain"] = ("one request at a time through EnvInit/View/ReadFilm: per-request service "
+                    "times measured (median of repeats), latencies from the same arrival times "
+                    "in FIFO order")
     for g in gs:
         g.close()
     B.EnvTerm()

@@ -114,7 +114,8 @@ class CgServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64),
                 ("cancelled", C.c_uint64), ("rejected", C.c_uint64),
                 ("samples", C.c_uint64), ("active", u32), ("pending", u32),
-                ("bytes_in_use", C.c_uint64), ("peak_bytes", C.c_uint64)]
+                ("bytes_in_use", C.c_uint64), ("peak_bytes", C.c_uint64),
+                ("chunks", C.c_uint64), ("busy_s", C.c_double), ("copy_out_s", C.c_double)]
 
 
 # numpy record layouts of the scene arrays (must match include/cg_cuda.h)

@@ -9,9 +9,12 @@
 // others are on the GPU start with the next chunk and share the device with
 // them (continuous batching); with two chunks in flight the host builds and
 // retires chunks while the GPU stays busy.  A request finishes
-// when its last pixel is resolved; its film is copied out and its memory
-// released.  Sample streams are keyed by (request seed, pixel, sample), so a
-// result does not depend on the requests it was batched with.
+// when its last pixel is resolved: the worker enqueues the film's packing and
+// its copy into a pinned staging buffer and goes on dispatching; a copy-out
+// thread waits for that copy, writes the caller's buffer (whose first-touch
+// page faults would otherwise stall dispatch) and completes the request.
+// Sample streams are keyed by (request seed, pixel, sample), so a result does
+// not depend on the requests it was batched with.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,6 +75,20 @@ struct ServerLane {
   }
 };
 
+// A finished film on its way to the caller: pinned staging slot, the event
+// after its device-to-host copy.
+struct CopyJob {
+  cg::ServerReq* r = nullptr;
+  size_t slot = 0;
+  cudaEvent_t ev = nullptr;
+};
+
+struct StagingBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool busy = false;
+};
+
 struct cg_server_s {
   static constexpr int kLanes = 2;
   std::vector<cg::SceneDev*> scenes;
@@ -91,8 +108,20 @@ struct cg_server_s {
   uint64_t next_id = 1;
   uint64_t dispatched = 0;
   cg_server_stats st{};
-  uint32_t rr = 0;
+  uint32_t cur_scene = 0;  // scene of the current run of chunks
+  uint32_t run = 0;        // chunks dispatched in that run
+  // copy-out thread and its queue; staging buffers and events are reused
+  std::thread copier;
+  std::mutex copy_mu;
+  std::condition_variable copy_cv;
+  std::deque<CopyJob> copy_q;
+  bool copy_stop = false;
+  std::vector<StagingBuf> staging;   // guarded by copy_mu
+  std::vector<cudaEvent_t> free_events;  // guarded by copy_mu
   ~cg_server_s() {
+    for (StagingBuf& b : staging)
+      if (b.p) cudaFreeHost(b.p);
+    for (cudaEvent_t e : free_events) cudaEventDestroy(e);
     if (alloc_stream) cudaStreamDestroy(alloc_stream);
   }
 };
@@ -122,23 +151,37 @@ void finishRequest(cg_server_s& sv, ServerReq* r, int status) {
     ++sv.st.cancelled;
 }
 
-// Builds one chunk for one scene (round robin over scenes with work) in
-// `lane`: an equal share of the chunk for each of the scene's active
-// requests, the rest first come first served.  Returns false when no request
-// has pixels left to schedule.
+// Chunks of one scene dispatched in a row before the server moves on to the
+// next scene with work.  Both lanes then mostly run chunks of the same scene,
+// whose trees share the L2 (two scenes' trees at once overflow it).
+constexpr uint32_t kSceneRun = 4;
+
+// Builds one chunk for one scene in `lane`: the current scene while its run
+// lasts and it has work, else the next scene with work (round robin); an
+// equal share of the chunk for each of the scene's active requests, the rest
+// first come first served.  Returns false when no request has pixels left to
+// schedule.
 bool buildChunk(cg_server_s* sv, ServerLane& lane, const Caps& caps, SceneDev*& scene_out,
                 ChunkDesc& ch) {
-  uint32_t scene_idx = UINT32_MAX;
-  for (uint32_t k = 0; k < sv->scenes.size() && scene_idx == UINT32_MAX; ++k) {
-    const uint32_t s = (sv->rr + k) % static_cast<uint32_t>(sv->scenes.size());
+  const uint32_t nscenes = static_cast<uint32_t>(sv->scenes.size());
+  auto hasWork = [&](uint32_t s) {
     for (ServerReq* r : sv->active)
-      if (r->req.scene == s && !r->cancelled && r->next_pixel < r->npx) {
-        scene_idx = s;
-        break;
-      }
+      if (r->req.scene == s && !r->cancelled && r->next_pixel < r->npx) return true;
+    return false;
+  };
+  uint32_t scene_idx = UINT32_MAX;
+  if (sv->run < kSceneRun && hasWork(sv->cur_scene)) {
+    scene_idx = sv->cur_scene;
+  } else {
+    for (uint32_t k = 1; k <= nscenes && scene_idx == UINT32_MAX; ++k) {
+      const uint32_t s = (sv->cur_scene + k) % nscenes;
+      if (hasWork(s)) scene_idx = s;
+    }
+    if (scene_idx == UINT32_MAX) return false;
+    sv->cur_scene = scene_idx;
+    sv->run = 0;
   }
-  if (scene_idx == UINT32_MAX) return false;
-  sv->rr = scene_idx + 1;
+  ++sv->run;
   SceneDev& scene = *sv->scenes[scene_idx];
   const uint32_t cap = lane.rend.chunkSamples(scene, caps);
   std::vector<ServerReq*> mine;
@@ -209,6 +252,76 @@ int enqueueLane(ServerLane& lane, SceneDev& scene, const ChunkDesc& ch, const Ca
   return CG_OK;
 }
 
+// A free pinned staging buffer of at least `bytes` (allocated if none is)
+// and an event; false if pinned memory or the event cannot be had.
+bool takeStaging(cg_server_s* sv, size_t bytes, size_t& slot, cudaEvent_t& ev) {
+  std::lock_guard<std::mutex> lk(sv->copy_mu);
+  if (sv->free_events.empty()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    sv->free_events.push_back(e);
+  }
+  size_t best = SIZE_MAX;
+  for (size_t k = 0; k < sv->staging.size(); ++k)
+    if (!sv->staging[k].busy && sv->staging[k].bytes >= bytes &&
+        (best == SIZE_MAX || sv->staging[k].bytes < sv->staging[best].bytes))
+      best = k;
+  if (best == SIZE_MAX) {
+    StagingBuf b;
+    if (cudaMallocHost(&b.p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    b.bytes = bytes;
+    sv->staging.push_back(b);
+    best = sv->staging.size() - 1;
+  }
+  sv->staging[best].busy = true;
+  slot = best;
+  ev = sv->free_events.back();
+  sv->free_events.pop_back();
+  return true;
+}
+
+void copyLoop(cg_server_s* sv, int device) {
+  cudaSetDevice(device);
+  while (true) {
+    CopyJob job;
+    const void* src = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(sv->copy_mu);
+      sv->copy_cv.wait(lk, [&] { return sv->copy_stop || !sv->copy_q.empty(); });
+      if (sv->copy_q.empty()) break;
+      job = sv->copy_q.front();
+      sv->copy_q.pop_front();
+      src = sv->staging[job.slot].p;
+    }
+    const double t0 = nowSeconds();
+    int st = CG_OK;
+    if (cudaEventSynchronize(job.ev) != cudaSuccess) {
+      cudaGetLastError();
+      st = CG_E_CUDA;
+    } else {
+      std::memcpy(job.r->out, src, size_t(job.r->npx) * 12);
+    }
+    {
+      std::lock_guard<std::mutex> lk(sv->copy_mu);
+      sv->staging[job.slot].busy = false;
+      sv->free_events.push_back(job.ev);
+    }
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->st.copy_out_s += nowSeconds() - t0;
+      finishRequest(*sv, job.r, st);
+    }
+    sv->done_cv.notify_all();
+    sv->cv.notify_all();  // its memory may let the worker admit a waiting request
+  }
+}
+
 void failAll(cg_server_s* sv, int rc, const char* msg) {
   sv->fatal = rc;
   sv->fatal_msg = msg;
@@ -222,6 +335,7 @@ void failAll(cg_server_s* sv, int rc, const char* msg) {
 void serverLoop(cg_server_s* sv) {
   cudaSetDevice(sv->lanes[0].rend.device);
   const Caps caps = capsOf(sv->conf);
+  double busy_since = 0.0;  // start of the current stretch with a chunk in flight
   std::unique_lock<std::mutex> lk(sv->mu);
   while (true) {
     // ---- admission (FIFO under the HBM budget) ----
@@ -235,8 +349,9 @@ void serverLoop(cg_server_s* sv) {
         continue;
       }
       if (sv->st.bytes_in_use + r->bytes > sv->budget) {
-        if (!sv->active.empty()) break;  // wait for memory to free up
-        sv->pending.pop_front();         // can never fit
+        // wait for memory held by active requests or films being copied out
+        if (r->bytes <= sv->budget && sv->st.bytes_in_use > 0) break;
+        sv->pending.pop_front();  // can never fit
         r->bytes = 0;
         ++sv->st.rejected;
         finishRequest(*sv, r, CG_E_OOM);
@@ -264,6 +379,8 @@ void serverLoop(cg_server_s* sv) {
     sv->st.active = static_cast<uint32_t>(sv->active.size());
     sv->st.pending = static_cast<uint32_t>(sv->pending.size());
     // ---- dispatch a chunk to every idle lane while there is work ----
+    const bool was_busy = std::any_of(std::begin(sv->lanes), std::end(sv->lanes),
+                                      [](const ServerLane& l) { return l.busy; });
     for (ServerLane& lane : sv->lanes) {
       if (lane.busy) continue;
       SceneDev* scene = nullptr;
@@ -276,6 +393,8 @@ void serverLoop(cg_server_s* sv) {
       }
       lane.busy = true;
       lane.issued = ++sv->dispatched;
+      ++sv->st.chunks;
+      if (!was_busy && busy_since == 0.0) busy_since = nowSeconds();
     }
     ServerLane* oldest = nullptr;
     for (ServerLane& lane : sv->lanes)
@@ -311,6 +430,11 @@ void serverLoop(cg_server_s* sv) {
     const bool ok = cudaEventSynchronize(oldest->done) == cudaSuccess;
     lk.lock();
     oldest->busy = false;
+    if (std::none_of(std::begin(sv->lanes), std::end(sv->lanes),
+                     [](const ServerLane& l) { return l.busy; })) {
+      sv->st.busy_s += nowSeconds() - busy_since;
+      busy_since = 0.0;
+    }
     if (!ok || *oldest->status_host) {
       cudaGetLastError();
       failAll(sv, ok ? CG_E_DEVICE : CG_E_CUDA,
@@ -328,19 +452,40 @@ void serverLoop(cg_server_s* sv) {
       if (complete || (r->cancelled && r->resolved == r->next_pixel)) {
         int st = CG_E_CANCELLED;
         if (complete && !r->cancelled) {
-          // packed on the device behind the film, then one contiguous copy
-          float* packed = reinterpret_cast<float*>(r->film + r->npx);
-          launchFilmPack(r->film, packed, r->npx, false, s);
-          st = cudaGetLastError() == cudaSuccess &&
-                       cudaMemcpyAsync(r->out, packed, size_t(r->npx) * 12,
-                                       cudaMemcpyDeviceToHost, s) == cudaSuccess
-                   ? CG_OK
-                   : CG_E_CUDA;
+          // packed on the device behind the film, one contiguous copy into
+          // pinned staging; the copy-out thread completes the request
+          size_t slot = 0;
+          cudaEvent_t ev = nullptr;
+          const size_t bytes = size_t(r->npx) * 12;
+          st = CG_E_OOM;
+          if (takeStaging(sv, bytes, slot, ev)) {
+            float* packed = reinterpret_cast<float*>(r->film + r->npx);
+            launchFilmPack(r->film, packed, r->npx, false, s);
+            void* dst = nullptr;
+            {
+              std::lock_guard<std::mutex> clk(sv->copy_mu);
+              dst = sv->staging[slot].p;
+            }
+            const bool queued =
+                cudaGetLastError() == cudaSuccess &&
+                cudaMemcpyAsync(dst, packed, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                cudaEventRecord(ev, s) == cudaSuccess;
+            std::lock_guard<std::mutex> clk(sv->copy_mu);
+            if (queued) {
+              sv->copy_q.push_back(CopyJob{r, slot, ev});
+              sv->copy_cv.notify_one();
+              st = CG_OK;
+            } else {
+              cudaGetLastError();
+              sv->staging[slot].busy = false;
+              sv->free_events.push_back(ev);
+              st = CG_E_CUDA;
+            }
+          }
         }
-        cudaFreeAsync(r->film, s);
+        cudaFreeAsync(r->film, s);  // after the copy in stream order
         r->film = nullptr;
-        cudaStreamSynchronize(s);
-        finishRequest(*sv, r, st);
+        if (st != CG_OK) finishRequest(*sv, r, st);  // else the copy-out thread does
         it = sv->active.erase(it);
         any = true;
       } else {
@@ -396,6 +541,7 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
     return fail(CG_E_CUDA, "server stream setup failed");
   }
   sv->worker = std::thread(serverLoop, sv.get());
+  sv->copier = std::thread(copyLoop, sv.get(), device);
   *out = sv.release();
   return CG_OK;
 }
@@ -410,6 +556,12 @@ CG_API int cg_server_destroy(cg_server_t server) {
   }
   server->cv.notify_all();
   if (server->worker.joinable()) server->worker.join();
+  {
+    std::lock_guard<std::mutex> lk(server->copy_mu);
+    server->copy_stop = true;  // the copier drains its queue first
+  }
+  server->copy_cv.notify_all();
+  if (server->copier.joinable()) server->copier.join();
   delete server;
   return CG_OK;
 }

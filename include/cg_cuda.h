@@ -375,8 +375,8 @@ CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view,
 /* The same search with the timed batch made of `count` probe views (for
  * example a sample of a batch to be rendered).  The search is a coordinate
  * descent from the current tuning: kernel variant (node width and box bits,
- * persistent traversal, shading sort), then queue capacity, then block sizes;
- * the fastest tuning is kept. */
+ * persistent traversal, shading sort), then chunk pipelines (1-4), then queue
+ * capacity, then block sizes; the fastest tuning is kept. */
 CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views,
                              uint32_t count, cg_tuning* best);
 
@@ -384,7 +384,10 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views,
  * A request loop over several resident scenes.  Requests are admitted while
  * their film plus path-state bytes fit the HBM budget, batched with the work
  * already on the GPU at chunk granularity (continuous batching), and
- * completed independently.  Per-request sample streams are keyed by
+ * completed independently: a copy-out thread writes each finished film into
+ * the caller's buffer while the GPU goes on with other requests.  Chunks of
+ * one scene run in short runs (both lanes on the same scene's trees) before
+ * the next scene with work gets its turn.  Per-request sample streams are keyed by
  * (request seed, pixel, sample), so a request's result does not depend on
  * what it was batched with. */
 typedef struct cg_server_s* cg_server_t;
@@ -413,6 +416,12 @@ typedef struct cg_server_stats {
   uint64_t samples;
   uint32_t active, pending;
   uint64_t bytes_in_use, peak_bytes;
+  uint64_t chunks;     /* wavefront chunks dispatched */
+  double busy_s;       /* seconds with at least one chunk in flight (host clock,
+                          dispatch to retirement) */
+  double copy_out_s;   /* seconds the copy-out thread spent waiting for finished
+                          films' device-to-host copies and writing them into
+                          the callers' buffers (overlaps the rendering) */
 } cg_server_stats;
 CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out);
 
