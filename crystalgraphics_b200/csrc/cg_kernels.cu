@@ -139,20 +139,42 @@ __device__ __forceinline__ int shadeKeyOf(const SceneView& sc, int32_t inst, boo
   return 2 + static_cast<int>((sc.mat[meta.y].volume >> kKindShift) & 15u);
 }
 
+// The block's key counts of a keyed closest-hit launch (one shared array per
+// block), flushed to the level's counts once at the end of the block.
+__device__ __forceinline__ uint32_t* blockKeyCounts() {
+  __shared__ uint32_t s_keycnt[kNumKeys];
+  return s_keycnt;
+}
+
+// At the start of a keyed closest-hit launch (every thread of the block).
+__device__ __forceinline__ void beginShadeKeys() {
+  if (threadIdx.x < kNumKeys) blockKeyCounts()[threadIdx.x] = 0u;
+  __syncthreads();
+}
+
 // keys: 0 none, 1 keys for a level shaded before the depth cut, 2 after it.
-// Called by the lanes that finished a ray (one atomic per distinct key among them).
+// Called by the lanes that finished a ray (one shared-memory atomic per
+// distinct key among them).
 __device__ __forceinline__ void writeShadeKey(const SceneView& sc, const WaveBuffers& wb, uint32_t i,
                                               int32_t inst, int keys) {
   const int key = shadeKeyOf(sc, inst, keys == 2);
   wb.shade_key[i] = static_cast<uint8_t>(key);
   const unsigned peers = __match_any_sync(__activemask(), key);
   if ((threadIdx.x & 31u) == static_cast<uint32_t>(__ffs(peers) - 1))
-    atomicAdd(&wb.counts[kKeyCount + key], static_cast<uint32_t>(__popc(peers)));
+    atomicAdd(&blockKeyCounts()[key], static_cast<uint32_t>(__popc(peers)));
 }
 
-// At the end of a keyed closest-hit launch (every thread of the block).
+// At the end of a keyed closest-hit launch (every thread of the block): adds
+// the block's counts to the level's, and the last block to finish turns the
+// level's counts into the scatter cursors (exclusive scan).
 __device__ __forceinline__ void finishShadeKeys(const WaveBuffers& wb) {
   __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x < kNumKeys) {
+    const uint32_t c = blockKeyCounts()[threadIdx.x];
+    if (c) atomicAdd(&wb.counts[kKeyCount + threadIdx.x], c);
+    __threadfence();  // ordered before this block's ticket
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -198,6 +220,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
     wb.counts[4] = 0u;
     atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
   }
+  if (keys) beginShadeKeys();
   TravCounters cnt{0u, 0u, 0u};
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = tid; i < n; i += stride) {
@@ -317,6 +340,7 @@ __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, Wave
     wb.counts[4] = 0u;
     atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
   }
+  if (keys) beginShadeKeys();
   persistentTraverse<false, kCount, kNodes>(sc, wb, n, &wb.counts[3], parity, keys);
   if (keys) finishShadeKeys(wb);
 }
@@ -486,23 +510,61 @@ struct Child {
 
 // ---- shade: one tree node per ray ------------------------------------------------
 // Places every ray at its key's cursor: shade_perm lists the level's rays
-// grouped by key.
-__global__ void __launch_bounds__(256) k_shade_scatter(WaveBuffers wb, int parity) {
+// grouped by key.  A block takes tiles of kScatterTile rays: each warp ranks
+// its 512 rays per key in shared memory (one match per 32 rays), the block
+// claims its range of every key with one global atomic per key and tile, and
+// the rays are written from registers.  (One global atomic per key and warp
+// serialised on the 19 cursors and took ~400 us per 8M-ray level.)
+constexpr int kScatterBlock = 256, kScatterItems = 16;
+constexpr int kScatterWarps = kScatterBlock / 32;
+constexpr uint32_t kScatterTile = kScatterBlock * kScatterItems;
+
+__global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb, int parity) {
+  __shared__ uint32_t s_cnt[kScatterWarps][kNumKeys];
+  __shared__ uint32_t s_off[kScatterWarps][kNumKeys];
   const uint32_t n = min(wb.counts[parity], wb.capacity);
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t base = warp_global * 32u; base < n; base += warps * 32u) {
-    const uint32_t i = base + lane;
-    const int key = i < n ? wb.shade_key[i] : kNumKeys - 1;
-    const unsigned peers = __match_any_sync(kFull, key);
-    const int leader = __ffs(peers) - 1;
-    uint32_t pos = 0;
-    if (key != kNumKeys - 1 && static_cast<int>(lane) == leader)
-      pos = atomicAdd(&wb.counts[kKeyCursor + key], static_cast<uint32_t>(__popc(peers)));
-    pos = __shfl_sync(peers, pos, leader);
-    const uint32_t at = pos + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
-    if (key != kNumKeys - 1 && at < wb.capacity) wb.shade_perm[at] = i;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned lower = (1u << lane) - 1u;
+  for (uint32_t base = blockIdx.x * kScatterTile; base < n; base += gridDim.x * kScatterTile) {
+    for (uint32_t k = threadIdx.x; k < kScatterWarps * kNumKeys; k += kScatterBlock)
+      (&s_cnt[0][0])[k] = 0u;
+    __syncthreads();
+    const uint32_t first = base + warp * (32u * kScatterItems) + lane;
+    uint32_t key[kScatterItems], rank[kScatterItems];
+#pragma unroll
+    for (int r = 0; r < kScatterItems; ++r) {
+      const uint32_t i = first + 32u * r;
+      const int k = i < n ? wb.shade_key[i] : kNumKeys - 1;  // kNumKeys - 1: no ray
+      const unsigned peers = __match_any_sync(kFull, k);
+      const int leader = __ffs(peers) - 1;
+      uint32_t before = 0;
+      if (static_cast<int>(lane) == leader) {
+        before = s_cnt[warp][k];
+        s_cnt[warp][k] = before + static_cast<uint32_t>(__popc(peers));
+      }
+      before = __shfl_sync(kFull, before, leader);
+      key[r] = static_cast<uint32_t>(k);
+      rank[r] = before + static_cast<uint32_t>(__popc(peers & lower));
+    }
+    __syncthreads();
+    if (threadIdx.x < kNumKeys - 1) {
+      const uint32_t k = threadIdx.x;
+      uint32_t total = 0;
+      for (int w = 0; w < kScatterWarps; ++w) {
+        s_off[w][k] = total;
+        total += s_cnt[w][k];
+      }
+      const uint32_t at = total ? atomicAdd(&wb.counts[kKeyCursor + k], total) : 0u;
+      for (int w = 0; w < kScatterWarps; ++w) s_off[w][k] += at;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kScatterItems; ++r) {
+      if (key[r] == kNumKeys - 1) continue;
+      const uint32_t at = s_off[warp][key[r]] + rank[r];
+      if (at < wb.capacity) wb.shade_perm[at] = first + 32u * r;
+    }
+    __syncthreads();  // s_cnt / s_off are rewritten by the next tile
   }
 }
 
@@ -851,7 +913,7 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
   if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
-    k_shade_scatter<<<gridFor(8u), 256, 0, s>>>(wb, parity);
+    k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
     k_shade<kShadeSortGlobal><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
     return 2;
   }
