@@ -476,17 +476,27 @@ enum { M_NONE = 0, M_DIFFUSE = 1, M_SREFL = 2, M_RREFL = 3, M_STRANS = 4, M_RTRA
 
 // balancePdfDenominator (sample.wesl:505-554).  A lobe (or the light) with a
 // zero sample count contributes 0 * pdf = 0; its pdf is not evaluated.
+// Lobe groups of a shading kernel (kLobes): lobes outside the mask have zero
+// sample counts for every ray the kernel takes, so their code is left out.
+constexpr int kLobeHit = 1, kLobeDiffuse = 2, kLobeReflect = 4, kLobeTransmit = 8;
+constexpr int kLobesAll = kLobeHit | kLobeDiffuse | kLobeReflect | kLobeTransmit;
+
+template <int kLobes = kLobesAll>
 __device__ __forceinline__ float balanceDenom(const SceneView& sc, V3 curr, V3 next, const Surf& s,
                                               const Mat& m, const Counts& c, int model,
                                               float model_pdf, float light_pdf_in,
                                               uint32_t* status) {
   float pd = 0.0f, psr = 0.0f, prr = 0.0f, pst = 0.0f, prt = 0.0f, pl = 0.0f;
-  if (c.diffuse) pd = model == M_DIFFUSE ? model_pdf : diffusePdf(curr, next, s);
-  if (c.specular_reflect) psr = model == M_SREFL ? model_pdf : specularReflectPdf(curr, next, s);
-  if (c.rough_reflect) prr = model == M_RREFL ? model_pdf : roughReflectPdf(curr, next, s, m);
-  if (c.specular_transmit)
+  if ((kLobes & kLobeDiffuse) && c.diffuse)
+    pd = model == M_DIFFUSE ? model_pdf : diffusePdf(curr, next, s);
+  if ((kLobes & kLobeReflect) && c.specular_reflect)
+    psr = model == M_SREFL ? model_pdf : specularReflectPdf(curr, next, s);
+  if ((kLobes & kLobeReflect) && c.rough_reflect)
+    prr = model == M_RREFL ? model_pdf : roughReflectPdf(curr, next, s, m);
+  if ((kLobes & kLobeTransmit) && c.specular_transmit)
     pst = model == M_STRANS ? model_pdf : specularTransmitPdf(curr, next, s, m);
-  if (c.rough_transmit) prt = model == M_RTRANS ? model_pdf : roughTransmitPdf(curr, next, s, m);
+  if ((kLobes & kLobeTransmit) && c.rough_transmit)
+    prt = model == M_RTRANS ? model_pdf : roughTransmitPdf(curr, next, s, m);
   if (c.light) pl = light_pdf_in >= 0.0f ? light_pdf_in : lightPdf(sc, s.pos, next, status);
   return fmaxf(static_cast<float>(c.diffuse) * pd + static_cast<float>(c.specular_reflect) * psr +
                    static_cast<float>(c.rough_reflect) * prr +
@@ -568,15 +578,29 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
   }
 }
 
+// kLobes: the lobe group (kLobesAll unless the level is in global shading
+// order, where one launch per group takes its keys' contiguous range of the
+// permutation: keys [0, 2) misses and hits beyond the depth cut, [2, 10) opaque
+// kinds, [10, 18) kinds with transmission; see shadeKeyOf).
 // kSort (ShadeSort): kShadeSortBlock — before shading, every block sorts its
 // slice of the queue by shading key in shared memory (counting sort);
 // kShadeSortGlobal — the level was sorted (keys from the closest-hit kernel,
 // permutation from k_shade_scatter) and the kernel takes rays in that order.  Either way a warp shades misses,
 // cut hits or one material kind rather than a mix of code paths.
-template <int kSort>
+template <int kSort, int kLobes = kLobesAll>
 __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                int depth, int parity) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
+  // [lo, hi): the queue slice (or, in global order, the permutation range of
+  // this launch's keys) the launch takes
+  uint32_t lo = 0, hi = n;
+  if (kSort == kShadeSortGlobal) {
+    // after k_shade_scatter every cursor is the end of its key's range
+    constexpr int k0 = kLobes == 0 ? 0 : (kLobes & kLobeTransmit) ? 10 : 2;
+    constexpr int k1 = kLobes == 0 ? 2 : (kLobes & kLobeTransmit) ? kNumKeys - 1 : 10;
+    lo = k0 == 0 ? 0u : min(wb.counts[kKeyCursor + k0 - 1], n);
+    hi = min(wb.counts[kKeyCursor + k1 - 1], n);
+  }
   const uint32_t lane = threadIdx.x & 31u;
   const int out = parity ^ 1;
   __shared__ int s_cnt[kNumKeys];
@@ -585,10 +609,12 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
   const uint32_t cut_depth = max(1u, min(fc.caps.trace_depth, 64u)) - 1u;
   const SampleCaps caps{fc.caps.trace_depth, fc.caps.transport_cap, fc.caps.emission_cap,
                         fc.caps.diffuse_cap, fc.caps.rough_cap};
-  if (blockIdx.x == 0 && threadIdx.x == 0) wb.counts[3] = 0u;  // next extend's work counter
-  for (uint32_t bbase = blockIdx.x * blockDim.x; bbase < n; bbase += gridDim.x * blockDim.x) {
+  // the next extend's work counter, zeroed by the level's first shading launch
+  if ((kSort != kShadeSortGlobal || kLobes == 0) && blockIdx.x == 0 && threadIdx.x == 0)
+    wb.counts[3] = 0u;
+  for (uint32_t bbase = lo + blockIdx.x * blockDim.x; bbase < hi; bbase += gridDim.x * blockDim.x) {
     uint32_t i = bbase + threadIdx.x;
-    if (kSort == kShadeSortGlobal && i < n) i = wb.shade_perm[i];
+    if (kSort == kShadeSortGlobal) i = i < hi ? wb.shade_perm[i] : n;  // n: no ray
     if (kSort == kShadeSortBlock) {
       const int key = i < n ? shadeKeyOf(sc, wb.hit_inst[i], static_cast<uint32_t>(depth) >= cut_depth)
                             : kNumKeys - 1;
@@ -628,7 +654,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
       float addL = 0.0f;
       if (hinst < 0) {
         addL = W * envRadiance(sc, rd, spos);
-      } else if (static_cast<uint32_t>(depth) < cut_depth) {
+      } else if ((kLobes & kLobeHit) && static_cast<uint32_t>(depth) < cut_depth) {
         // surface frame of the closest hit (bvh.wesl:102-129, 167-179)
         const uint32_t tri = __float_as_uint(h4.w);
         const float t = h4.x, u = h4.y, v = h4.z;
@@ -669,13 +695,14 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
         const V3 curr = rd;
         uint32_t ti = 0;  // transport sample index (child key)
         auto push = [&](V3 next, int model, float prob, float dist) {
-          const float coeff = dist / balanceDenom(sc, curr, next, s, m, c, model, prob, -1.0f, wb.status);
+          const float coeff =
+              dist / balanceDenom<kLobes>(sc, curr, next, s, m, c, model, prob, -1.0f, wb.status);
           const float cw = W * coeff;
           if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
           ++ti;
         };
         // sampleModels (sample.wesl:301-425) in its lobe order
-        if (c.diffuse) {  // pdf/diffuse.wesl:7-36
+        if ((kLobes & kLobeDiffuse) && c.diffuse) {  // pdf/diffuse.wesl:7-36
           const V3 macro = orientedNormal(curr, s.sn);
           const float r = sqrtf(randFloat(rng));
           const float angle = 2.0f * PI * randFloat(rng);
@@ -685,11 +712,11 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
           const V3 next = mul(makeTangentSpace(macro), local);
           push(next, M_DIFFUSE, diffusePdf(curr, next, s), diffuseDist(curr, next, s, m));
         }
-        if (c.specular_reflect) {  // pdf/specular_reflection.wesl:7-15
+        if ((kLobes & kLobeReflect) && c.specular_reflect) {  // pdf/specular_reflection.wesl:7-15
           const V3 next = specularDir(curr, s);
           push(next, M_SREFL, specularReflectPdf(curr, next, s), specularReflectDist(curr, next, s, m));
         }
-        if (c.rough_reflect) {  // pdf/rough_reflection.wesl:9-27
+        if ((kLobes & kLobeReflect) && c.rough_reflect) {  // pdf/rough_reflection.wesl:9-27
           const V3 micro = orientedNormal(curr, sampleNorm(curr, s, m.microfacet_roughness, rng));
           const V3 next = reflect(curr, micro);
           const V3 macro = orientedNormal(curr, s.sn);
@@ -698,13 +725,13 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
                                  : reflectPdf(curr, micro, macro, m.microfacet_roughness);
           push(next, M_RREFL, prob, roughReflectDist(curr, next, s, m));
         }
-        if (c.specular_transmit) {  // pdf/specular_transmission.wesl:9-27
+        if ((kLobes & kLobeTransmit) && c.specular_transmit) {  // pdf/specular_transmission.wesl:9-27
           const V3 next = m.volume ? refract(curr, orientedNormal(curr, s.sn), relIor(s.sn, curr, m).re)
                                    : curr;
           push(next, M_STRANS, specularTransmitPdf(curr, next, s, m),
                specularTransmitDist(curr, next, s, m));
         }
-        if (c.rough_transmit) {  // pdf/rough_transmission.wesl:9-32
+        if ((kLobes & kLobeTransmit) && c.rough_transmit) {  // pdf/rough_transmission.wesl:9-32
           const V3 macro = orientedNormal(curr, s.sn);
           const V3 micro = orientedNormal(curr, sampleNorm(curr, s, m.microfacet_roughness, rng));
           const V3 next = refract(curr, micro, relIorT(relIor(micro, curr, m)));
@@ -743,7 +770,8 @@ __global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, Wave
             float ec = diffuseDist(curr, next, s, m) + roughReflectDist(curr, next, s, m);
             if (m.transmission != 0.0f) ec = ec + roughTransmitDist(curr, next, s, m);
             const float rad = radiance * ec * sproj /
-                              balanceDenom(sc, curr, next, s, m, c, M_NONE, -1.0f, sapdf, wb.status);
+                              balanceDenom<kLobes>(sc, curr, next, s, m, c, M_NONE, -1.0f, sapdf,
+                                                   wb.status);
             const float contrib = W * rad;
             if (contrib != 0.0f) {
               const float expected_dist = sqrtf(dsq);
@@ -914,8 +942,12 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
   if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
-    k_shade<kShadeSortGlobal><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    return 2;
+    // one launch per lobe group, each over its keys' range of the permutation
+    k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade<kShadeSortGlobal, kLobeHit | kLobeDiffuse | kLobeReflect>
+        <<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade<kShadeSortGlobal, kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    return 4;
   }
   if (ls.shade_sort == kShadeSortBlock)
     k_shade<kShadeSortBlock><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
