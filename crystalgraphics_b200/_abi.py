@@ -115,7 +115,8 @@ class CgServerStats(C.Structure):
                 ("cancelled", C.c_uint64), ("rejected", C.c_uint64),
                 ("samples", C.c_uint64), ("active", u32), ("pending", u32),
                 ("bytes_in_use", C.c_uint64), ("peak_bytes", C.c_uint64),
-                ("chunks", C.c_uint64), ("busy_s", C.c_double), ("copy_out_s", C.c_double)]
+                ("chunks", C.c_uint64), ("busy_s", C.c_double), ("all_busy_s", C.c_double),
+                ("copy_out_s", C.c_double)]
 
 
 # numpy record layouts of the scene arrays (must match include/cg_cuda.h)

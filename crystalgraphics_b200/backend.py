@@ -438,13 +438,22 @@ class Server:
         self._h = h.value
         self._films = {}
 
-    def submit(self, scene_index, position, direction, width, height, spp, seed=0, viewport=None):
+    def submit(self, scene_index, position, direction, width, height, spp, seed=0, viewport=None,
+               out: np.ndarray | None = None):
+        """Queues a request; its XYZ film lands in `out` (a C-contiguous
+        (height, width, 3) float32 array that a caller may reuse across
+        requests) or in a new array.  Returns the request id."""
         req = _abi.CgRequest()
         req.scene = scene_index
         vp = viewport or (0.5 * width / height, 0.5)
         req.view.camera = _abi.make_camera(position, direction, vp)
         req.view.width, req.view.height, req.view.spp, req.view.seed = width, height, spp, seed
-        film = np.empty((height, width, 3), np.float32)
+        if out is None:
+            film = np.empty((height, width, 3), np.float32)
+        else:
+            assert out.shape == (height, width, 3) and out.dtype == np.float32 \
+                and out.flags["C_CONTIGUOUS"]
+            film = out
         rid = C.c_uint64()
         _check(lib.cg_server_submit(self._h, C.byref(req), film.ctypes.data, C.byref(rid)))
         self._films[rid.value] = film

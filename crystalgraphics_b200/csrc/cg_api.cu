@@ -22,7 +22,22 @@
 #include "cg_kernels.h"
 #include "cg_scene.h"
 
+#include <sys/mman.h>
+#include <unistd.h>
+
 namespace cg {
+
+void prefaultHostBuffer(void* p, size_t bytes) {
+#ifdef MADV_POPULATE_WRITE
+  static const uintptr_t page = static_cast<uintptr_t>(sysconf(_SC_PAGESIZE));
+  const uintptr_t lo = (reinterpret_cast<uintptr_t>(p) + page - 1) & ~(page - 1);
+  const uintptr_t hi = (reinterpret_cast<uintptr_t>(p) + bytes) & ~(page - 1);
+  if (hi > lo) (void)madvise(reinterpret_cast<void*>(lo), hi - lo, MADV_POPULATE_WRITE);
+#else
+  (void)p;
+  (void)bytes;
+#endif
+}
 
 thread_local std::string tl_error;
 
@@ -823,6 +838,7 @@ CG_API int cg_film_read(void* host, size_t bytes, int format) {
   Env& env = *g_env;
   const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
   CG_CUDA(cudaSetDevice(env.device));
+  prefaultHostBuffer(host, std::min(bytes, npx * (format == CG_FILM_RGBA8 ? 4 : 12)));
   if (format == CG_FILM_RGBA8) {
     if (bytes < npx * 4) return fail(CG_E_INVALID, "buffer too small for RGBA8");
     CG_CUDA(cudaMemcpyAsync(host, env.rgba, npx * 4, cudaMemcpyDeviceToHost, env.stream));

@@ -29,6 +29,12 @@ int cudaFail(cudaError_t e, const char* what);
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Populates the page tables of a caller's host buffer (the whole pages inside
+// it) as if written, without changing its contents, so a later copy into a
+// freshly allocated buffer does not take one page fault per 4 KB page.  Best
+// effort: errors (an older kernel, a pinned or unmapped range) are ignored.
+void prefaultHostBuffer(void* p, size_t bytes);
+
 struct DeviceArena {
   void* base = nullptr;
   size_t size = 0;

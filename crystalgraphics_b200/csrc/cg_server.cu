@@ -9,10 +9,12 @@
 // others are on the GPU start with the next chunk and share the device with
 // them (continuous batching); with two chunks in flight the host builds and
 // retires chunks while the GPU stays busy.  A request finishes
-// when its last pixel is resolved: the worker enqueues the film's packing and
-// its copy into a pinned staging buffer and goes on dispatching; a copy-out
-// thread waits for that copy, writes the caller's buffer (whose first-touch
-// page faults would otherwise stall dispatch) and completes the request.
+// when its last pixel is resolved: the worker enqueues the film's copy into a
+// pinned staging buffer (a copy-engine transfer, so it does not wait for SMs
+// that the other lane's kernels hold) and goes on dispatching; a copy-out
+// thread waits for that copy, packs it into the caller's buffer (whose page
+// tables a prefault thread populated after the submit) and completes the
+// request.
 // Sample streams are keyed by (request seed, pixel, sample), so a result does
 // not depend on the requests it was batched with.
 #include <cuda_runtime.h>
@@ -64,7 +66,6 @@ struct ServerLane {
   std::vector<cg::ViewDev> slices;
   std::vector<cg::ServerReq*> slice_req;
   uint32_t used = 0;
-  uint64_t issued = 0;          // dispatch order of the chunk in flight
   bool busy = false;
   uint32_t* status_host = nullptr;  // pinned: the chunk's status word
   cudaEvent_t done = nullptr;
@@ -106,7 +107,6 @@ struct cg_server_s {
   int fatal = CG_OK;
   std::string fatal_msg;
   uint64_t next_id = 1;
-  uint64_t dispatched = 0;
   cg_server_stats st{};
   uint32_t cur_scene = 0;  // scene of the current run of chunks
   uint32_t run = 0;        // chunks dispatched in that run
@@ -118,6 +118,12 @@ struct cg_server_s {
   bool copy_stop = false;
   std::vector<StagingBuf> staging;   // guarded by copy_mu
   std::vector<cudaEvent_t> free_events;  // guarded by copy_mu
+  // prefault thread: populates each submitted film buffer while the GPU works
+  std::thread prefaulter;
+  std::mutex pf_mu;
+  std::condition_variable pf_cv;
+  std::deque<std::pair<void*, size_t>> pf_q;
+  bool pf_stop = false;
   ~cg_server_s() {
     for (StagingBuf& b : staging)
       if (b.p) cudaFreeHost(b.p);
@@ -129,15 +135,14 @@ struct cg_server_s {
 namespace cg {
 namespace {
 
-// Film bytes (the float4 film and its packed three-float readback) plus the
-// path state the request can occupy in one chunk.
+// Film bytes plus the path state the request can occupy in one chunk.
 size_t requestBytes(const cg_server_s& sv, const SceneDev& scene, const cg_request& r) {
   const size_t npx = size_t(r.view.width) * r.view.height;
   const LevelPlan plan = planLevels(capsOf(sv.conf), std::max(1u, scene.max_lobes));
   const size_t per_sample = 12 + plan.max_product * (36 + 20 + 36);
   const size_t samples =
       std::min<size_t>(npx * r.view.spp, sv.lanes[0].rend.chunkSamples(scene, capsOf(sv.conf)));
-  return npx * (16 + 12) + samples * per_sample;
+  return npx * 16 + samples * per_sample;
 }
 
 void finishRequest(cg_server_s& sv, ServerReq* r, int status) {
@@ -286,6 +291,8 @@ bool takeStaging(cg_server_s* sv, size_t bytes, size_t& slot, cudaEvent_t& ev) {
   return true;
 }
 
+constexpr int kCopyThreads = 4;
+
 void copyLoop(cg_server_s* sv, int device) {
   cudaSetDevice(device);
   while (true) {
@@ -305,7 +312,29 @@ void copyLoop(cg_server_s* sv, int device) {
       cudaGetLastError();
       st = CG_E_CUDA;
     } else {
-      std::memcpy(job.r->out, src, size_t(job.r->npx) * 12);
+      // float4 -> three floats per pixel; large films are packed by
+      // kCopyThreads threads (this one and helpers), so one slow core on a
+      // busy host does not hold the request back
+      const size_t npx = job.r->npx;
+      float* dst = job.r->out;
+      const float* from = static_cast<const float*>(src);
+      auto pack = [dst, from](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+          dst[3 * i] = from[4 * i];
+          dst[3 * i + 1] = from[4 * i + 1];
+          dst[3 * i + 2] = from[4 * i + 2];
+        }
+      };
+      const int parts = npx >= (size_t(1) << 18) ? kCopyThreads : 1;
+      const size_t step = (npx + parts - 1) / parts;
+      std::thread helpers[kCopyThreads];
+      for (int k = 1; k < parts; ++k) {
+        const size_t b = std::min(npx, step * k), e = std::min(npx, step * (k + 1));
+        if (e > b) helpers[k] = std::thread(pack, b, e);
+      }
+      pack(0, std::min(npx, step));
+      for (int k = 1; k < parts; ++k)
+        if (helpers[k].joinable()) helpers[k].join();
     }
     {
       std::lock_guard<std::mutex> lk(sv->copy_mu);
@@ -319,6 +348,20 @@ void copyLoop(cg_server_s* sv, int device) {
     }
     sv->done_cv.notify_all();
     sv->cv.notify_all();  // its memory may let the worker admit a waiting request
+  }
+}
+
+void prefaultLoop(cg_server_s* sv) {
+  while (true) {
+    std::pair<void*, size_t> job;
+    {
+      std::unique_lock<std::mutex> lk(sv->pf_mu);
+      sv->pf_cv.wait(lk, [&] { return sv->pf_stop || !sv->pf_q.empty(); });
+      if (sv->pf_stop) break;
+      job = sv->pf_q.front();
+      sv->pf_q.pop_front();
+    }
+    prefaultHostBuffer(job.first, job.second);
   }
 }
 
@@ -336,6 +379,7 @@ void serverLoop(cg_server_s* sv) {
   cudaSetDevice(sv->lanes[0].rend.device);
   const Caps caps = capsOf(sv->conf);
   double busy_since = 0.0;  // start of the current stretch with a chunk in flight
+  double all_since = 0.0;   // start of the current stretch with every lane busy
   std::unique_lock<std::mutex> lk(sv->mu);
   while (true) {
     // ---- admission (FIFO under the HBM budget) ----
@@ -359,7 +403,7 @@ void serverLoop(cg_server_s* sv) {
         continue;
       }
       sv->pending.pop_front();
-      const size_t fb = size_t(r->npx) * (16 + 12);  // film, then its packed readback
+      const size_t fb = size_t(r->npx) * 16;
       void* film = nullptr;
       if (cudaMallocAsync(&film, fb, sv->alloc_stream) != cudaSuccess ||
           cudaStreamSynchronize(sv->alloc_stream) != cudaSuccess) {
@@ -392,14 +436,15 @@ void serverLoop(cg_server_s* sv) {
         return;
       }
       lane.busy = true;
-      lane.issued = ++sv->dispatched;
       ++sv->st.chunks;
       if (!was_busy && busy_since == 0.0) busy_since = nowSeconds();
     }
-    ServerLane* oldest = nullptr;
-    for (ServerLane& lane : sv->lanes)
-      if (lane.busy && (!oldest || lane.issued < oldest->issued)) oldest = &lane;
-    if (!oldest) {
+    if (all_since == 0.0 && std::all_of(std::begin(sv->lanes), std::end(sv->lanes),
+                                        [](const ServerLane& l) { return l.busy; }))
+      all_since = nowSeconds();
+    const bool any_busy = std::any_of(std::begin(sv->lanes), std::end(sv->lanes),
+                                      [](const ServerLane& l) { return l.busy; });
+    if (!any_busy) {
       // nothing in flight: retire requests that were cancelled before they ran
       bool any = false;
       for (auto it = sv->active.begin(); it != sv->active.end();) {
@@ -425,50 +470,64 @@ void serverLoop(cg_server_s* sv) {
       sv->cv.wait_for(lk, std::chrono::milliseconds(50));
       continue;
     }
-    // ---- retire the oldest chunk in flight ----
+    // ---- retire the first chunk to finish (a lane whose chunk is done must
+    // not wait for a longer chunk on the other lane) ----
     lk.unlock();
-    const bool ok = cudaEventSynchronize(oldest->done) == cudaSuccess;
+    ServerLane* fin = nullptr;  // a lane whose chunk is done
+    bool ok = true;
+    while (!fin) {
+      for (ServerLane& lane : sv->lanes) {  // `busy` is only written by this thread
+        if (!lane.busy) continue;
+        const cudaError_t e = cudaEventQuery(lane.done);
+        if (e == cudaErrorNotReady) continue;
+        ok = e == cudaSuccess;
+        fin = &lane;
+        break;
+      }
+      if (!fin) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
     lk.lock();
-    oldest->busy = false;
+    fin->busy = false;
+    if (all_since != 0.0) {
+      sv->st.all_busy_s += nowSeconds() - all_since;
+      all_since = 0.0;
+    }
     if (std::none_of(std::begin(sv->lanes), std::end(sv->lanes),
                      [](const ServerLane& l) { return l.busy; })) {
       sv->st.busy_s += nowSeconds() - busy_since;
       busy_since = 0.0;
     }
-    if (!ok || *oldest->status_host) {
+    if (!ok || *fin->status_host) {
       cudaGetLastError();
       failAll(sv, ok ? CG_E_DEVICE : CG_E_CUDA,
               ok ? "kernel status word set (stack or queue overflow)" : "CUDA failure in the server loop");
       return;
     }
-    sv->st.samples += oldest->used;
-    for (size_t k = 0; k < oldest->slice_req.size(); ++k)
-      oldest->slice_req[k]->resolved += oldest->slices[k].pixel_count;
+    sv->st.samples += fin->used;
+    for (size_t k = 0; k < fin->slice_req.size(); ++k)
+      fin->slice_req[k]->resolved += fin->slices[k].pixel_count;
     bool any = false;
-    cudaStream_t s = oldest->rend.stream;
+    cudaStream_t s = fin->rend.stream;
     for (auto it = sv->active.begin(); it != sv->active.end();) {
       ServerReq* r = *it;
       const bool complete = r->resolved == r->npx;
       if (complete || (r->cancelled && r->resolved == r->next_pixel)) {
         int st = CG_E_CANCELLED;
         if (complete && !r->cancelled) {
-          // packed on the device behind the film, one contiguous copy into
-          // pinned staging; the copy-out thread completes the request
+          // one contiguous copy of the float4 film into pinned staging; the
+          // copy-out thread packs it and completes the request
           size_t slot = 0;
           cudaEvent_t ev = nullptr;
-          const size_t bytes = size_t(r->npx) * 12;
+          const size_t bytes = size_t(r->npx) * 16;
           st = CG_E_OOM;
           if (takeStaging(sv, bytes, slot, ev)) {
-            float* packed = reinterpret_cast<float*>(r->film + r->npx);
-            launchFilmPack(r->film, packed, r->npx, false, s);
             void* dst = nullptr;
             {
               std::lock_guard<std::mutex> clk(sv->copy_mu);
               dst = sv->staging[slot].p;
             }
             const bool queued =
-                cudaGetLastError() == cudaSuccess &&
-                cudaMemcpyAsync(dst, packed, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                cudaMemcpyAsync(dst, r->film, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
                 cudaEventRecord(ev, s) == cudaSuccess;
             std::lock_guard<std::mutex> clk(sv->copy_mu);
             if (queued) {
@@ -542,6 +601,7 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
   }
   sv->worker = std::thread(serverLoop, sv.get());
   sv->copier = std::thread(copyLoop, sv.get(), device);
+  sv->prefaulter = std::thread(prefaultLoop, sv.get());
   *out = sv.release();
   return CG_OK;
 }
@@ -562,6 +622,12 @@ CG_API int cg_server_destroy(cg_server_t server) {
   }
   server->copy_cv.notify_all();
   if (server->copier.joinable()) server->copier.join();
+  {
+    std::lock_guard<std::mutex> lk(server->pf_mu);
+    server->pf_stop = true;  // buffers not yet populated are simply written later
+  }
+  server->pf_cv.notify_all();
+  if (server->prefaulter.joinable()) server->prefaulter.join();
   delete server;
   return CG_OK;
 }
@@ -587,6 +653,11 @@ CG_API int cg_server_submit(cg_server_t server, const cg_request* request, float
   r->id = server->next_id++;
   if (request_id) *request_id = r->id;
   server->pending.push_back(r.get());
+  {
+    std::lock_guard<std::mutex> plk(server->pf_mu);
+    server->pf_q.emplace_back(film_xyz, size_t(r->npx) * 12);
+  }
+  server->pf_cv.notify_one();
   server->reqs[r->id] = std::move(r);
   ++server->st.submitted;
   server->cv.notify_all();

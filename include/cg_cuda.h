@@ -419,6 +419,7 @@ typedef struct cg_server_stats {
   uint64_t chunks;     /* wavefront chunks dispatched */
   double busy_s;       /* seconds with at least one chunk in flight (host clock,
                           dispatch to retirement) */
+  double all_busy_s;   /* seconds with a chunk in flight on every lane */
   double copy_out_s;   /* seconds the copy-out thread spent waiting for finished
                           films' device-to-host copies and writing them into
                           the callers' buffers (overlaps the rendering) */
