@@ -587,8 +587,10 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 // kShadeSortGlobal — the level was sorted (keys from the closest-hit kernel,
 // permutation from k_shade_scatter) and the kernel takes rays in that order.  Either way a warp shades misses,
 // cut hits or one material kind rather than a mix of code paths.
+// At most 96 registers: five blocks of 128 threads per SM (the lobe groups
+// need 90-93 without spills; uncapped they took 98, which left room for four).
 template <int kSort, int kLobes = kLobesAll>
-__global__ void __launch_bounds__(256) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
+__global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                int depth, int parity) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
   // [lo, hi): the queue slice (or, in global order, the permutation range of
