@@ -47,6 +47,44 @@ def test_struct_layouts_match_reference_sizes():
     assert _abi.ALIAS_DTYPE.itemsize == 8
 
 
+# ctypes mirror -> C struct of include/cg_cuda.h
+_MIRRORS = {"CgConf": "cg_conf", "CgCamera": "cg_camera", "CgSceneDesc": "cg_scene_desc",
+            "CgTexture": "cg_texture", "CgSceneInfo": "cg_scene_info", "CgHit": "cg_hit",
+            "CgStats": "cg_stats", "CgProfile": "cg_profile", "CgViewDesc": "cg_view_desc",
+            "CgTuning": "cg_tuning", "CgRequest": "cg_request",
+            "CgRequestResult": "cg_request_result", "CgServerStats": "cg_server_stats"}
+
+
+def test_ctypes_mirrors_match_the_header(tmp_path):
+    """Every ctypes structure has the size and field offsets of its C struct
+    (compiled against include/cg_cuda.h with the host C compiler)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    inc = os.path.join(ROOT, "include")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cg_cuda.h"', 'int main(void) {']
+    for py, c in _MIRRORS.items():
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in getattr(_abi, py)._fields_:
+            lines.append(f'  printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "sizes.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "sizes"
+    subprocess.run([cc, "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    bad = []
+    for line in out.splitlines():
+        py, field, value = line.split()
+        cls = getattr(_abi, py)
+        got = C.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        if got != int(value):
+            bad.append((py, field, got, int(value)))
+    assert not bad, bad
+
+
 def test_calls_without_init_fail_with_reference_message():
     if B.EnvStatus():
         pytest.skip("environment initialised by another test")
