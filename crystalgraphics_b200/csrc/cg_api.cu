@@ -550,6 +550,7 @@ int Env::uploadViews(const std::vector<ViewDev>& views, cudaStream_t s) {
 Env::~Env() {
   if (stream) cudaStreamSynchronize(stream);
   graphs.clear();
+  dropViewGraph();
   if (views_dev) cudaFree(views_dev);
   if (film) cudaFree(film);
   if (rgba) cudaFree(rgba);
@@ -815,14 +816,54 @@ CG_API int cg_view(cg_scene_t scene, const cg_camera* camera) {
   const Caps caps = capsOf(env.conf);
   int rc = env.ensureWave(env.tuning.queue_capacity);
   if (rc != CG_OK) return rc;
+  const bool use_graph = env.tuning.use_graph && !env.profiling;
+  if (use_graph && env.tuning.pipelines > 1u) {  // before any capture
+    rc = env.ensurePipelines(static_cast<int>(env.tuning.pipelines));
+    if (rc != CG_OK) return rc;
+  }
   rc = env.beginStats(env.stream);
   if (rc != CG_OK) return rc;
   rc = env.uploadViews(views, env.stream);
   if (rc != CG_OK) return rc;
+  const ViewDev* table = static_cast<const ViewDev*>(env.views_dev);
   RenderRecord rec;
-  CG_CUDA(cudaEventRecord(env.ev0, env.stream));
-  rc = env.enqueueViews(*s, views, static_cast<const ViewDev*>(env.views_dev), caps, env.stream, rec);
-  if (rc != CG_OK) return rc;
+  if (use_graph) {
+    // the launch sequence depends only on the scene, the conf, the tuning and
+    // the buffers, so it is captured once and replayed: a small frame's ~60
+    // launches then cost one graph launch
+    Env::ViewGraph& vg = env.view_graph;
+    if (!(vg.exec && vg.scene_tag == s->tag && vg.counting == env.counting && vg.table == table)) {
+      env.dropViewGraph();
+      CG_CUDA(cudaStreamSynchronize(env.stream));
+      cudaGraph_t graph = nullptr;
+      CG_CUDA(cudaStreamBeginCapture(env.stream, cudaStreamCaptureModeThreadLocal));
+      RenderRecord r;
+      rc = env.enqueueViews(*s, views, table, caps, env.stream, r);
+      cudaError_t ce = cudaStreamEndCapture(env.stream, &graph);
+      if (rc != CG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ce != cudaSuccess) return cudaFail(ce, "cudaStreamEndCapture");
+      ce = cudaGraphInstantiate(&vg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) {
+        vg.exec = nullptr;
+        return cudaFail(ce, "cudaGraphInstantiate");
+      }
+      vg.scene_tag = s->tag;
+      vg.counting = env.counting;
+      vg.table = table;
+      vg.rec = r;
+    }
+    CG_CUDA(cudaEventRecord(env.ev0, env.stream));
+    CG_CUDA(cudaGraphLaunch(vg.exec, env.stream));
+    rec = vg.rec;
+  } else {
+    CG_CUDA(cudaEventRecord(env.ev0, env.stream));
+    rc = env.enqueueViews(*s, views, table, caps, env.stream, rec);
+    if (rc != CG_OK) return rc;
+  }
   CG_CUDA(cudaEventRecord(env.ev1, env.stream));
   CG_CUDA(cudaGetLastError());
   CG_CUDA(cudaEventSynchronize(env.ev1));

@@ -174,6 +174,18 @@ struct Env : Renderer {
   size_t view_cap = 0;
   cg_stats last{};
   std::vector<std::unique_ptr<BatchGraph>> graphs;
+  // View()'s launch sequence, captured once per scene and replayed (the view
+  // table it reads is uploaded before every replay); valid while the scene,
+  // the counting mode and the table's address are the ones it was captured
+  // with (tuning changes drop it)
+  struct ViewGraph {
+    uint64_t scene_tag = 0;
+    bool counting = false;
+    const void* table = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    RenderRecord rec;
+  } view_graph;
+  void dropViewGraph();
 
   int uploadViews(const std::vector<ViewDev>& views, cudaStream_t s);
   int endStats(cudaStream_t s, const RenderRecord& rec, float ms) {

@@ -27,8 +27,16 @@ void Env::dropGraphsFor(uint64_t tag) {
   graphs.erase(std::remove_if(graphs.begin(), graphs.end(),
                               [&](const std::unique_ptr<BatchGraph>& g) { return g->scene_tag == tag; }),
                graphs.end());
+  if (view_graph.exec && view_graph.scene_tag == tag) dropViewGraph();
 }
-void Env::dropAllGraphs() { graphs.clear(); }
+void Env::dropAllGraphs() {
+  graphs.clear();
+  dropViewGraph();
+}
+void Env::dropViewGraph() {
+  if (view_graph.exec) cudaGraphExecDestroy(view_graph.exec);
+  view_graph = ViewGraph{};
+}
 
 // Builds the view table of a batch into `g` (films allocated per view).
 static int buildBatch(Env& env, const SceneDev& scene, const cg_view_desc* views, uint32_t n,

@@ -139,6 +139,34 @@ def test_chunk_pipelines_render_the_same_films(cornell, use_graph):
     B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
 
 
+def test_view_graph_replay_matches_direct_launches(cornell):
+    """View() replays its captured launch sequence; accumulated frames, a
+    camera change and a switch to another scene (a new capture) give the films
+    of direct launches."""
+    s, g = cornell
+    s2 = small_instanced()
+    g2 = B.LoadScene(s2)
+    conf = B.PathTraceConf(render_width=80, render_height=64, sample_count=2, trace_depth=4)
+    cam = B.Camera.from_c(s.camera)
+    moved = B.Camera(tuple(x + 0.01 for x in s.camera.position[:]), tuple(s.camera.direction[:]),
+                     (0.5 * 80 / 64, 0.5))
+    films = {}
+    for use_graph in (0, 1):
+        B.EnvInit(conf)
+        B.SetTuning(use_graph=use_graph)
+        out = []
+        for scene, c in ((g, cam), (g, cam), (g, cam), (g, moved), (g2, B.Camera.from_c(s2.camera)),
+                         (g, cam)):
+            B.View(scene, c)
+            out.append((B.ReadFilm(), B.FilmFrames(), B.LastStats().kernel_launches))
+        films[use_graph] = out
+    for (a, fa, la), (b, fb, lb) in zip(films[0], films[1]):
+        assert fa == fb and la == lb
+        assert _close(b, a) < RTOL
+    g2.close()
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
+
+
 def test_server_results_same_alone_and_in_the_mix(cornell):
     s, g = cornell
     s2 = small_instanced()
