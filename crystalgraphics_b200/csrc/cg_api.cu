@@ -217,6 +217,7 @@ int Renderer::init(int dev) {
   CG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CG_CUDA(cudaEventCreate(&ev0));
   CG_CUDA(cudaEventCreate(&ev1));
+  CG_CUDA(cudaMallocHost(&stats_host, kMaxPipelines * kStatsHostStride));
   if (wl_tree) return CG_OK;  // adopted from a previous renderer
   CG_CUDA(cudaMalloc(&wl_tree, 65535 * sizeof(float)));
   CG_CUDA(cudaMalloc(&wl_const, 4 * sizeof(float)));
@@ -258,6 +259,7 @@ Renderer::~Renderer() {
   if (wl_const) cudaFree(wl_const);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (stats_host) cudaFreeHost(stats_host);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -503,14 +505,23 @@ int Renderer::beginStats(cudaStream_t s) {
 int Renderer::readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_stats& out) {
   unsigned long long st[kMaxPipelines][8] = {};
   uint32_t status[kMaxPipelines] = {};
-  CG_CUDA(cudaMemcpyAsync(st[0], wave.stats, sizeof(st[0]), cudaMemcpyDeviceToHost, s));
-  CG_CUDA(cudaMemcpyAsync(&status[0], wave.status, 4, cudaMemcpyDeviceToHost, s));
+  bool used[kMaxPipelines] = {true};
   for (int k = 0; k < kMaxPipelines - 1; ++k)
-    if (xwave_arena[k].base) {  // zeroed by beginStats; after the join, in stream order on s
-      CG_CUDA(cudaMemcpyAsync(st[k + 1], xwave[k].stats, sizeof(st[0]), cudaMemcpyDeviceToHost, s));
-      CG_CUDA(cudaMemcpyAsync(&status[k + 1], xwave[k].status, 4, cudaMemcpyDeviceToHost, s));
-    }
+    used[k + 1] = xwave_arena[k].base != nullptr;  // zeroed by beginStats; read after the join
+  for (int p = 0; p < kMaxPipelines; ++p) {
+    if (!used[p]) continue;
+    const WaveBuffers& w = p ? xwave[p - 1] : wave;
+    unsigned char* h = stats_host + p * kStatsHostStride;
+    CG_CUDA(cudaMemcpyAsync(h, w.stats, sizeof(st[0]), cudaMemcpyDeviceToHost, s));
+    CG_CUDA(cudaMemcpyAsync(h + sizeof(st[0]), w.status, 4, cudaMemcpyDeviceToHost, s));
+  }
   CG_CUDA(cudaStreamSynchronize(s));
+  for (int p = 0; p < kMaxPipelines; ++p) {
+    if (!used[p]) continue;
+    const unsigned char* h = stats_host + p * kStatsHostStride;
+    std::memcpy(st[p], h, sizeof(st[0]));
+    std::memcpy(&status[p], h + sizeof(st[0]), 4);
+  }
   for (int p = 1; p < kMaxPipelines; ++p) {
     for (int k = 0; k < 8; ++k) st[0][k] += st[p][k];
     status[0] |= status[p];

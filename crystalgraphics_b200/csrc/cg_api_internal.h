@@ -91,6 +91,10 @@ struct Renderer {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float* wl_tree = nullptr;
   float* wl_const = nullptr;
+  // pinned: each pipeline's statistics (64 B) and status word, read back
+  // with asynchronous copies and one synchronisation
+  static constexpr size_t kStatsHostStride = 128;
+  unsigned char* stats_host = nullptr;
   bool counting = false;
   // 64M rays per level queue (~9.7 GB of path state): large chunks keep every
   // level's launch full
