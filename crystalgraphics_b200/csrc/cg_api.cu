@@ -629,6 +629,7 @@ CG_API int cg_term(void) {
   std::lock_guard<std::mutex> lk(g_env_mu);
   delete g_env;
   g_env = nullptr;
+  releaseIdleStaging();
   return CG_OK;
 }
 

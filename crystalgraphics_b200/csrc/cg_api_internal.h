@@ -35,6 +35,9 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 // effort: errors (an older kernel, a pinned or unmapped range) are ignored.
 void prefaultHostBuffer(void* p, size_t bytes);
 
+// Frees the pinned film staging buffers that no server holds (cg_term).
+void releaseIdleStaging();
+
 struct DeviceArena {
   void* base = nullptr;
   size_t size = 0;

@@ -76,18 +76,18 @@ struct ServerLane {
   }
 };
 
-// A finished film on its way to the caller: pinned staging slot, the event
-// after its device-to-host copy.
-struct CopyJob {
-  cg::ServerReq* r = nullptr;
-  size_t slot = 0;
-  cudaEvent_t ev = nullptr;
-};
-
 struct StagingBuf {
   void* p = nullptr;
   size_t bytes = 0;
   bool busy = false;
+};
+
+// A finished film on its way to the caller: its pinned staging buffer, the
+// event after its device-to-host copy.
+struct CopyJob {
+  cg::ServerReq* r = nullptr;
+  StagingBuf* buf = nullptr;
+  cudaEvent_t ev = nullptr;
 };
 
 struct cg_server_s {
@@ -116,7 +116,6 @@ struct cg_server_s {
   std::condition_variable copy_cv;
   std::deque<CopyJob> copy_q;
   bool copy_stop = false;
-  std::vector<StagingBuf> staging;   // guarded by copy_mu
   std::vector<cudaEvent_t> free_events;  // guarded by copy_mu
   // prefault thread: populates each submitted film buffer while the GPU works
   std::thread prefaulter;
@@ -125,8 +124,6 @@ struct cg_server_s {
   std::deque<std::pair<void*, size_t>> pf_q;
   bool pf_stop = false;
   ~cg_server_s() {
-    for (StagingBuf& b : staging)
-      if (b.p) cudaFreeHost(b.p);
     for (cudaEvent_t e : free_events) cudaEventDestroy(e);
     if (alloc_stream) cudaStreamDestroy(alloc_stream);
   }
@@ -257,9 +254,51 @@ int enqueueLane(ServerLane& lane, SceneDev& scene, const ChunkDesc& ch, const Ca
   return CG_OK;
 }
 
-// A free pinned staging buffer of at least `bytes` (allocated if none is)
-// and an event; false if pinned memory or the event cannot be had.
-bool takeStaging(cg_server_s* sv, size_t bytes, size_t& slot, cudaEvent_t& ev) {
+// Pinned staging buffers shared by every server of the process.  Pinning
+// fresh memory zeroes and locks new pages, which on a busy host can take
+// seconds for a burst of films; a server created later reuses the buffers
+// instead.  Portable, so a server on any device can copy into them.
+// cg_term frees the buffers no server holds.
+struct StagingPool {
+  std::mutex mu;
+  std::vector<std::unique_ptr<StagingBuf>> bufs;
+};
+StagingPool& stagingPool() {
+  static StagingPool pool;
+  return pool;
+}
+
+// A free pinned staging buffer of at least `bytes` (the smallest that fits,
+// allocated in whole MiB if none does), or null.
+StagingBuf* takeStagingBuf(size_t bytes) {
+  StagingPool& pool = stagingPool();
+  std::lock_guard<std::mutex> lk(pool.mu);
+  StagingBuf* best = nullptr;
+  for (auto& b : pool.bufs)
+    if (!b->busy && b->bytes >= bytes && (!best || b->bytes < best->bytes)) best = b.get();
+  if (!best) {
+    auto b = std::make_unique<StagingBuf>();
+    const size_t size = (bytes + (size_t(1) << 20) - 1) & ~((size_t(1) << 20) - 1);
+    if (cudaHostAlloc(&b->p, size, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    b->bytes = size;
+    best = b.get();
+    pool.bufs.push_back(std::move(b));
+  }
+  best->busy = true;
+  return best;
+}
+
+void giveStagingBuf(StagingBuf* b) {
+  std::lock_guard<std::mutex> lk(stagingPool().mu);
+  b->busy = false;
+}
+
+// A staging buffer of at least `bytes` and an event; false if pinned memory
+// or the event cannot be had.
+bool takeStaging(cg_server_s* sv, size_t bytes, StagingBuf*& buf, cudaEvent_t& ev) {
   std::lock_guard<std::mutex> lk(sv->copy_mu);
   if (sv->free_events.empty()) {
     cudaEvent_t e = nullptr;
@@ -269,23 +308,8 @@ bool takeStaging(cg_server_s* sv, size_t bytes, size_t& slot, cudaEvent_t& ev) {
     }
     sv->free_events.push_back(e);
   }
-  size_t best = SIZE_MAX;
-  for (size_t k = 0; k < sv->staging.size(); ++k)
-    if (!sv->staging[k].busy && sv->staging[k].bytes >= bytes &&
-        (best == SIZE_MAX || sv->staging[k].bytes < sv->staging[best].bytes))
-      best = k;
-  if (best == SIZE_MAX) {
-    StagingBuf b;
-    if (cudaMallocHost(&b.p, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return false;
-    }
-    b.bytes = bytes;
-    sv->staging.push_back(b);
-    best = sv->staging.size() - 1;
-  }
-  sv->staging[best].busy = true;
-  slot = best;
+  buf = takeStagingBuf(bytes);
+  if (!buf) return false;
   ev = sv->free_events.back();
   sv->free_events.pop_back();
   return true;
@@ -304,7 +328,7 @@ void copyLoop(cg_server_s* sv, int device) {
       if (sv->copy_q.empty()) break;
       job = sv->copy_q.front();
       sv->copy_q.pop_front();
-      src = sv->staging[job.slot].p;
+      src = job.buf->p;
     }
     const double t0 = nowSeconds();
     int st = CG_OK;
@@ -336,9 +360,9 @@ void copyLoop(cg_server_s* sv, int device) {
       for (int k = 1; k < parts; ++k)
         if (helpers[k].joinable()) helpers[k].join();
     }
+    giveStagingBuf(job.buf);
     {
       std::lock_guard<std::mutex> lk(sv->copy_mu);
-      sv->staging[job.slot].busy = false;
       sv->free_events.push_back(job.ev);
     }
     {
@@ -364,6 +388,23 @@ void prefaultLoop(cg_server_s* sv) {
     prefaultHostBuffer(job.first, job.second);
   }
 }
+
+}  // namespace
+
+void releaseIdleStaging() {
+  StagingPool& pool = stagingPool();
+  std::lock_guard<std::mutex> lk(pool.mu);
+  for (auto it = pool.bufs.begin(); it != pool.bufs.end();) {
+    if (!(*it)->busy) {
+      cudaFreeHost((*it)->p);
+      it = pool.bufs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+namespace {
 
 void failAll(cg_server_s* sv, int rc, const char* msg) {
   sv->fatal = rc;
@@ -516,27 +557,24 @@ void serverLoop(cg_server_s* sv) {
         if (complete && !r->cancelled) {
           // one contiguous copy of the float4 film into pinned staging; the
           // copy-out thread packs it and completes the request
-          size_t slot = 0;
+          StagingBuf* buf = nullptr;
           cudaEvent_t ev = nullptr;
           const size_t bytes = size_t(r->npx) * 16;
           st = CG_E_OOM;
-          if (takeStaging(sv, bytes, slot, ev)) {
-            void* dst = nullptr;
-            {
-              std::lock_guard<std::mutex> clk(sv->copy_mu);
-              dst = sv->staging[slot].p;
-            }
+          if (takeStaging(sv, bytes, buf, ev)) {
             const bool queued =
-                cudaMemcpyAsync(dst, r->film, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                cudaMemcpyAsync(buf->p, r->film, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
                 cudaEventRecord(ev, s) == cudaSuccess;
+            if (!queued) {
+              cudaGetLastError();
+              giveStagingBuf(buf);
+            }
             std::lock_guard<std::mutex> clk(sv->copy_mu);
             if (queued) {
-              sv->copy_q.push_back(CopyJob{r, slot, ev});
+              sv->copy_q.push_back(CopyJob{r, buf, ev});
               sv->copy_cv.notify_one();
               st = CG_OK;
             } else {
-              cudaGetLastError();
-              sv->staging[slot].busy = false;
               sv->free_events.push_back(ev);
               st = CG_E_CUDA;
             }

@@ -169,7 +169,9 @@ typedef struct cg_scene_s* cg_scene_t;
  * the film of render_width x render_height.  Calling it again re-creates the
  * environment. */
 CG_API int cg_init(const cg_conf* conf, int device);
-/* EnvTerm (src/environment.cpp:18-23).  Safe to call when not initialised. */
+/* EnvTerm (src/environment.cpp:18-23).  Safe to call when not initialised.
+ * Also frees the pinned film staging buffers that served requests left for
+ * reuse (those a live server still holds stay). */
 CG_API int cg_term(void);
 /* EnvStatus (src/environment.cpp:34-37): 1 when initialised. */
 CG_API int cg_status(void);
