@@ -58,7 +58,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # (ncu, cold caches: an upper bound), captured with 14 closest-hit launches per
 # frame (64M-ray queues); with another chunking the frame's traffic is spread
 # over its launches
-EXTEND_TRAFFIC_B = 721.4e6
+EXTEND_TRAFFIC_B = 718.7e6
 EXTEND_TRAFFIC_LAUNCHES = 14
 
 
