@@ -61,6 +61,9 @@ def _load():
         "cg_alias_build": (i, [vp, u32, vp]),
         "cg_view": (i, [vp, C.POINTER(_abi.CgCamera)]),
         "cg_film_read": (i, [vp, C.c_size_t, i]),
+        "cg_view_samples": (i, [vp, C.POINTER(_abi.CgCamera), u32, u32]),
+        "cg_film_device": (i, [C.POINTER(vp), C.POINTER(C.c_size_t)]),
+        "cg_film_update_rgba8": (i, []),
         "cg_film_frames": (i, [C.POINTER(u32)]),
         "cg_last_stats": (i, [C.POINTER(_abi.CgStats)]),
         "cg_set_counting": (i, [i]),
@@ -261,6 +264,77 @@ def parse_gltf(path) -> "scenes.Scene":
 def View(scene: Scene, camera: Camera | _abi.CgCamera | None = None) -> None:
     cam = camera if isinstance(camera, _abi.CgCamera) else (camera or Camera()).to_c()
     _check(lib.cg_view(scene.handle, C.byref(cam)))
+
+
+def ViewSamples(scene: Scene, camera: Camera | _abi.CgCamera | None, sample_begin: int,
+                sample_count: int) -> None:
+    """Renders samples [sample_begin, sample_begin + sample_count) of every
+    pixel (out of the conf's sample_count) as that range's share of the full
+    frame's mean (cg_view_samples)."""
+    cam = camera if isinstance(camera, _abi.CgCamera) else (camera or Camera()).to_c()
+    _check(lib.cg_view_samples(scene.handle, C.byref(cam), int(sample_begin), int(sample_count)))
+
+
+class _DeviceFilm:
+    """The environment's float4 device film as a CUDA array interface."""
+
+    def __init__(self):
+        ptr, nbytes = C.c_void_p(), C.c_size_t()
+        _check(lib.cg_film_device(C.byref(ptr), C.byref(nbytes)))
+        conf = _abi.CgConf()
+        _check(lib.cg_get_conf(C.byref(conf)))
+        shape = (conf.render_height, conf.render_width, 4)
+        assert nbytes.value == 16 * shape[0] * shape[1]
+        # the film is complete when a call of this library returns, so the
+        # consumer needs no stream synchronisation
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4",
+                                         "data": (ptr.value, False), "version": 3,
+                                         "strides": None, "stream": None}
+
+
+def FilmDevice():
+    """A torch CUDA tensor (height, width, 4) aliasing the environment's film
+    (X, Y, Z, 0 per pixel); valid until the next EnvInit or EnvTerm."""
+    import torch
+    return torch.as_tensor(_DeviceFilm(), device="cuda")
+
+
+def UpdateRgba8() -> None:
+    """Recomputes the rgba8 film from the (changed) float film."""
+    _check(lib.cg_film_update_rgba8())
+
+
+def sample_range(spp: int, rank: int, world: int) -> tuple[int, int]:
+    """(first sample, count) of rank `rank` when `world` ranks split `spp`
+    samples per pixel in contiguous, near-equal ranges."""
+    begin = spp * rank // world
+    return begin, spp * (rank + 1) // world - begin
+
+
+def sum_films(film, group=None) -> None:
+    """Sums a film tensor over the ranks of `group` in place (all-reduce; NCCL
+    over NVLink for CUDA tensors) and waits for the result."""
+    import torch
+    import torch.distributed as dist
+    dist.all_reduce(film, op=dist.ReduceOp.SUM, group=group)
+    if film.is_cuda:
+        torch.cuda.synchronize(film.device)
+
+
+def ViewSplit(scene: Scene, camera: Camera | _abi.CgCamera | None = None, group=None) -> None:
+    """One View() frame (frame 0) spread over the ranks of a torch.distributed
+    group, one GPU per rank: each rank renders its range of every pixel's
+    samples, then the device films are summed across the ranks, so every rank
+    ends with the full frame's film (equal to a one-GPU cg_view frame 0 up to
+    float summation order).  The film's running mean restarts."""
+    import torch.distributed as dist
+    conf = _abi.CgConf()
+    _check(lib.cg_get_conf(C.byref(conf)))
+    begin, count = sample_range(conf.sample_count, dist.get_rank(group),
+                                dist.get_world_size(group))
+    ViewSamples(scene, camera, begin, count)
+    sum_films(FilmDevice(), group)
+    UpdateRgba8()
 
 
 def ReadFilm(fmt: int = _abi.CG_FILM_XYZ32F, out: np.ndarray | None = None) -> np.ndarray:

@@ -602,6 +602,70 @@ static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& o
   return CG_OK;
 }
 
+// Renders one prepared view of `s` into the environment's film: uploads the
+// view table and enqueues (or, when `allow_graph`, replays the captured)
+// launch sequence, then waits and reads the statistics.
+static int renderEnvView(Env& env, SceneDev* s, std::vector<ViewDev>& views, bool allow_graph) {
+  layoutViews(views);
+  const Caps caps = capsOf(env.conf);
+  int rc = env.ensureWave(env.tuning.queue_capacity);
+  if (rc != CG_OK) return rc;
+  const bool use_graph = allow_graph && env.tuning.use_graph && !env.profiling;
+  if (use_graph && env.tuning.pipelines > 1u) {  // before any capture
+    rc = env.ensurePipelines(static_cast<int>(env.tuning.pipelines));
+    if (rc != CG_OK) return rc;
+  }
+  rc = env.beginStats(env.stream);
+  if (rc != CG_OK) return rc;
+  rc = env.uploadViews(views, env.stream);
+  if (rc != CG_OK) return rc;
+  const ViewDev* table = static_cast<const ViewDev*>(env.views_dev);
+  RenderRecord rec;
+  if (use_graph) {
+    // the launch sequence depends only on the scene, the conf, the tuning and
+    // the buffers, so it is captured once and replayed: a small frame's ~60
+    // launches then cost one graph launch
+    Env::ViewGraph& vg = env.view_graph;
+    if (!(vg.exec && vg.scene_tag == s->tag && vg.counting == env.counting && vg.table == table)) {
+      env.dropViewGraph();
+      CG_CUDA(cudaStreamSynchronize(env.stream));
+      cudaGraph_t graph = nullptr;
+      CG_CUDA(cudaStreamBeginCapture(env.stream, cudaStreamCaptureModeThreadLocal));
+      RenderRecord r;
+      rc = env.enqueueViews(*s, views, table, caps, env.stream, r);
+      cudaError_t ce = cudaStreamEndCapture(env.stream, &graph);
+      if (rc != CG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ce != cudaSuccess) return cudaFail(ce, "cudaStreamEndCapture");
+      ce = cudaGraphInstantiate(&vg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) {
+        vg.exec = nullptr;
+        return cudaFail(ce, "cudaGraphInstantiate");
+      }
+      vg.scene_tag = s->tag;
+      vg.counting = env.counting;
+      vg.table = table;
+      vg.rec = r;
+    }
+    CG_CUDA(cudaEventRecord(env.ev0, env.stream));
+    CG_CUDA(cudaGraphLaunch(vg.exec, env.stream));
+    rec = vg.rec;
+  } else {
+    CG_CUDA(cudaEventRecord(env.ev0, env.stream));
+    rc = env.enqueueViews(*s, views, table, caps, env.stream, rec);
+    if (rc != CG_OK) return rc;
+  }
+  CG_CUDA(cudaEventRecord(env.ev1, env.stream));
+  CG_CUDA(cudaGetLastError());
+  CG_CUDA(cudaEventSynchronize(env.ev1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, env.ev0, env.ev1);
+  return env.endStats(env.stream, rec, ms);
+}
+
 }  // namespace cg
 
 using namespace cg;
@@ -824,64 +888,70 @@ CG_API int cg_view(cg_scene_t scene, const cg_camera* camera) {
   v.pixel_count = v.width * v.height;
   v.film = static_cast<float4*>(env.film);
   v.rgba = static_cast<uchar4*>(env.rgba);
-  layoutViews(views);
-  const Caps caps = capsOf(env.conf);
-  int rc = env.ensureWave(env.tuning.queue_capacity);
-  if (rc != CG_OK) return rc;
-  const bool use_graph = env.tuning.use_graph && !env.profiling;
-  if (use_graph && env.tuning.pipelines > 1u) {  // before any capture
-    rc = env.ensurePipelines(static_cast<int>(env.tuning.pipelines));
-    if (rc != CG_OK) return rc;
+  return renderEnvView(env, s, views, true);
+}
+
+CG_API int cg_view_samples(cg_scene_t scene, const cg_camera* camera, uint32_t sample_begin,
+                           uint32_t sample_count) {
+  if (!scene || !camera) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  Env& env = *g_env;
+  if (sample_begin > env.conf.sample_count ||
+      sample_count > env.conf.sample_count - sample_begin)
+    return fail(CG_E_INVALID, "sample range beyond the conf's sample_count");
+  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+  CG_CUDA(cudaSetDevice(env.device));
+  env.has_prev = false;  // a share of a frame: the next View() starts a fresh mean
+  const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
+  if (sample_count == 0) {  // this share holds no samples
+    CG_CUDA(cudaMemsetAsync(env.film, 0, npx * sizeof(float4), env.stream));
+    launchFilmRgba8(static_cast<const float4*>(env.film), static_cast<uchar4*>(env.rgba), npx,
+                    env.stream);
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaStreamSynchronize(env.stream));
+    env.last = cg_stats{};
+    return CG_OK;
   }
-  rc = env.beginStats(env.stream);
-  if (rc != CG_OK) return rc;
-  rc = env.uploadViews(views, env.stream);
-  if (rc != CG_OK) return rc;
-  const ViewDev* table = static_cast<const ViewDev*>(env.views_dev);
-  RenderRecord rec;
-  if (use_graph) {
-    // the launch sequence depends only on the scene, the conf, the tuning and
-    // the buffers, so it is captured once and replayed: a small frame's ~60
-    // launches then cost one graph launch
-    Env::ViewGraph& vg = env.view_graph;
-    if (!(vg.exec && vg.scene_tag == s->tag && vg.counting == env.counting && vg.table == table)) {
-      env.dropViewGraph();
-      CG_CUDA(cudaStreamSynchronize(env.stream));
-      cudaGraph_t graph = nullptr;
-      CG_CUDA(cudaStreamBeginCapture(env.stream, cudaStreamCaptureModeThreadLocal));
-      RenderRecord r;
-      rc = env.enqueueViews(*s, views, table, caps, env.stream, r);
-      cudaError_t ce = cudaStreamEndCapture(env.stream, &graph);
-      if (rc != CG_OK) {
-        if (graph) cudaGraphDestroy(graph);
-        return rc;
-      }
-      if (ce != cudaSuccess) return cudaFail(ce, "cudaStreamEndCapture");
-      ce = cudaGraphInstantiate(&vg.exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (ce != cudaSuccess) {
-        vg.exec = nullptr;
-        return cudaFail(ce, "cudaGraphInstantiate");
-      }
-      vg.scene_tag = s->tag;
-      vg.counting = env.counting;
-      vg.table = table;
-      vg.rec = r;
-    }
-    CG_CUDA(cudaEventRecord(env.ev0, env.stream));
-    CG_CUDA(cudaGraphLaunch(vg.exec, env.stream));
-    rec = vg.rec;
-  } else {
-    CG_CUDA(cudaEventRecord(env.ev0, env.stream));
-    rc = env.enqueueViews(*s, views, table, caps, env.stream, rec);
-    if (rc != CG_OK) return rc;
-  }
-  CG_CUDA(cudaEventRecord(env.ev1, env.stream));
+  std::vector<ViewDev> views(1);
+  ViewDev& v = views[0];
+  std::memset(&v, 0, sizeof(v));
+  cameraBasis(*camera, v);
+  v.width = env.conf.render_width;
+  v.height = env.conf.render_height;
+  v.spp = sample_count;
+  v.sample_base = sample_begin;
+  v.spp_total = env.conf.sample_count;
+  v.seed = env.seed;
+  v.frame = 0;
+  v.sample_weight = 1.0f;
+  v.pixel_base = 0;
+  v.pixel_count = v.width * v.height;
+  v.film = static_cast<float4*>(env.film);
+  v.rgba = static_cast<uchar4*>(env.rgba);
+  // the chunking depends on the range, so the captured View() sequence does not apply
+  return renderEnvView(env, s, views, false);
+}
+
+CG_API int cg_film_device(void** film_xyzw, size_t* bytes) {
+  if (!film_xyzw || !bytes) return fail(CG_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  *film_xyzw = g_env->film;
+  *bytes = size_t(g_env->conf.render_width) * g_env->conf.render_height * sizeof(float4);
+  return CG_OK;
+}
+
+CG_API int cg_film_update_rgba8(void) {
+  std::lock_guard<std::mutex> lk(g_env_mu);
+  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+  Env& env = *g_env;
+  CG_CUDA(cudaSetDevice(env.device));
+  launchFilmRgba8(static_cast<const float4*>(env.film), static_cast<uchar4*>(env.rgba),
+                  size_t(env.conf.render_width) * env.conf.render_height, env.stream);
   CG_CUDA(cudaGetLastError());
-  CG_CUDA(cudaEventSynchronize(env.ev1));
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, env.ev0, env.ev1);
-  return env.endStats(env.stream, rec, ms);
+  CG_CUDA(cudaStreamSynchronize(env.stream));
+  return CG_OK;
 }
 
 CG_API int cg_film_read(void* host, size_t bytes, int format) {

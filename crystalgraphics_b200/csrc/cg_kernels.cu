@@ -101,7 +101,7 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   const uint32_t k = static_cast<uint32_t>(local - uint64_t(lp) * v.spp);
   const uint32_t pixel = v.pixel_base + lp;
   const uint32_t px = pixel % v.width, py = pixel / v.width;
-  const uint32_t key = sampleKey(v.seed, v.frame, pixel, k);
+  const uint32_t key = sampleKey(v.seed, v.frame, pixel, k + v.sample_base);
   Rng wr;
   seedRng(wr, wavelengthKey(key));
   const float lambda = sampleWavelengthTree(fc.wl_tree, randFloat(wr));
@@ -839,7 +839,9 @@ __global__ void k_resolve(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   const uint32_t pixel = v.pixel_base + lp;
   const uint64_t first = v.sample_offset + uint64_t(lp) * v.spp - ch.sample_begin;
   const float avg = fc.wl_const[1];
-  const float spp = static_cast<float>(v.spp);
+  // each sample adds its term / the full frame's spp, so the films of sample
+  // ranges that partition a pixel's samples add up to the full frame
+  const float spp = static_cast<float>(v.spp_total ? v.spp_total : v.spp);
   V3 acc{0.0f, 0.0f, 0.0f};
   for (uint32_t k = 0; k < v.spp; ++k) {
     const float L = wb.s_L[first + k];
@@ -1011,6 +1013,22 @@ __global__ void k_film_pack(const float4* __restrict__ film, float* __restrict__
   out[3 * i] = a;
   out[3 * i + 1] = b;
   out[3 * i + 2] = c;
+}
+
+__global__ void k_film_rgba8(const float4* __restrict__ film, uchar4* __restrict__ rgba, size_t npx) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= npx) return;
+  const float4 f = film[i];
+  const V3 lin = xyzToLinearSrgb(V3{f.x, f.y, f.z});
+  rgba[i] = make_uchar4(static_cast<unsigned char>(__float2uint_rn(encodeChannel(lin.x) * 255.0f)),
+                        static_cast<unsigned char>(__float2uint_rn(encodeChannel(lin.y) * 255.0f)),
+                        static_cast<unsigned char>(__float2uint_rn(encodeChannel(lin.z) * 255.0f)),
+                        255);
+}
+
+void launchFilmRgba8(const float4* film, uchar4* rgba, size_t npx, cudaStream_t s) {
+  if (npx == 0) return;
+  k_film_rgba8<<<static_cast<unsigned>((npx + 255) / 256), 256, 0, s>>>(film, rgba, npx);
 }
 
 void launchFilmPack(const float4* film, float* out, size_t npx, bool rgb, cudaStream_t s) {

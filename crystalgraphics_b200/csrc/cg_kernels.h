@@ -27,6 +27,8 @@ struct ViewDev {
   float sample_weight;         // 1 / (frame + 1)
   uint32_t pixel_base;         // first image pixel this entry covers
   uint32_t pixel_count;        // image pixels this entry covers
+  uint32_t sample_base;        // per-pixel index of the first sample rendered (sample keys)
+  uint32_t spp_total;          // divisor of the pixel mean: the full frame's spp (0: spp)
   uint64_t pixel_offset;       // first global pixel index of this entry
   uint64_t sample_offset;      // first global sample index of this entry
   float4* film;                // running-mean XYZ (w unused)
@@ -110,6 +112,8 @@ void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc&
                    cudaStream_t s);
 // Packs a float4 film to three floats per pixel (XYZ, or linear sRGB).
 void launchFilmPack(const float4* film, float* out, size_t npx, bool rgb, cudaStream_t s);
+// Re-resolves the rgba8 film from the float4 XYZ film (the resolve's sRGB step).
+void launchFilmRgba8(const float4* film, uchar4* rgba, size_t npx, cudaStream_t s);
 void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, float4* out_tuv,
                         int4* out_ids, uint32_t* status, int nodes, cudaStream_t s);
 

@@ -278,6 +278,31 @@ enum {
 };
 /* Copies the film into `host` (row-major, row y = pixel.y of cameraRay). */
 CG_API int cg_film_read(void* host, size_t bytes, int format);
+
+/* ---- one view split across GPUs -------------------------------------------
+ * No counterpart in the reference (its View() renders on one adapter).  For
+ * spreading one large frame over several GPUs: each process renders a share
+ * of every pixel's samples and the films are summed across GPUs (NCCL
+ * all-reduce of the device films; backend.ViewSplit does all of it).
+ *
+ * cg_view_samples renders samples [sample_begin, sample_begin + sample_count)
+ * of each pixel out of the conf's sample_count, with the sample keys of a
+ * full cg_view frame 0 of the same seed, into the film as that range's share
+ * of the pixel mean (every sample's term divided by sample_count of the
+ * conf).  Films of ranges that partition [0, sample_count) add up to the full
+ * frame (up to float summation order).  The film's running mean restarts:
+ * the next cg_view begins a fresh accumulation.  An empty range writes a zero
+ * film.  Ranges beyond the conf's sample_count are rejected (CG_E_INVALID). */
+CG_API int cg_view_samples(cg_scene_t scene, const cg_camera* camera,
+                           uint32_t sample_begin, uint32_t sample_count);
+/* The environment's device film: float4 (X, Y, Z, 0) per pixel, row-major,
+ * `*bytes` long, owned by the environment (valid until cg_init or cg_term).
+ * Work on it on another stream must be complete before the next call of
+ * this library that touches the film. */
+CG_API int cg_film_device(void** film_xyzw, size_t* bytes);
+/* Recomputes the rgba8 film from the float film (after it was changed on the
+ * device, e.g. summed across GPUs), with the resolve's sRGB step. */
+CG_API int cg_film_update_rgba8(void);
 /* Frames accumulated so far in the film (iter_count + 1 after a View). */
 CG_API int cg_film_frames(uint32_t* frames);
 
