@@ -18,6 +18,9 @@ Metric: Msamples/s (one sample = one render() iteration of one pixel).
           counting pass of the same kernels) over its CUDA-event time.
   cpu_baseline the oracle (the reference's estimator restated in C++,
           multithreaded) on a bounded pixel sample of the same frame.
+  forms   (one GPU, default workload) the batched form (256 mixed views in
+          one graph-replayed wavefront) and the served form (Poisson request
+          streams over four resident scenes) against the plain path.
 
 --impl reference times that CPU implementation alone on the same workload.
 Multi-GPU (torchrun): every rank renders its own frames of the workload

@@ -375,12 +375,16 @@ CG_API int cg_batch_render(cg_scene_t scene, const cg_view_desc* views,
  * searches these for a scene and a representative view (cg_autotune_views:
  * several views) and keeps the best. */
 typedef struct cg_tuning {
-  uint32_t queue_capacity;
+  uint32_t queue_capacity;  /* rays per level queue, in [4096, 2^28] (default
+                               64M: ~9.7 GB of path state per pipeline) */
   uint32_t extend_block;  /* threads per block of the traversal launches: a
                              multiple of 32 in [32, 256] (default 128; 0 = keep) */
   uint32_t shade_block;   /* the same for the shading launch (larger values
                              run as 256) */
-  uint32_t use_graph;   /* 1 = capture the chunk pipeline as a CUDA graph */
+  uint32_t use_graph;   /* 1 (default) = capture the launch sequence as a CUDA
+                           graph and replay it: per batch in cg_batch_render,
+                           per scene in cg_view (not while profiling);
+                           always written (0 = launch directly) */
   uint32_t bvh_width;   /* 4 (default) or 2: node width the traversal walks */
   uint32_t persistent;  /* 1 (default) = persistent traversal warps that refill
                            idle lanes, 2 = one ray per thread, 0 = keep */
