@@ -161,13 +161,17 @@ class _Builder:
         return len(self.textures) - 1
 
     def build(self, name, camera, conf, env=None) -> Scene:
+        """The scene (empty arrays where nothing was added: a scene without
+        geometry renders the environment alone)."""
+        def cat(parts, dtype):
+            return np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(0, dtype))
         meshes = np.array(self.meshes, np.uint32).reshape(-1, 4).copy().view(_abi.MESH_DTYPE).reshape(-1)
         return Scene(name=name,
-                     vertices=np.ascontiguousarray(np.concatenate(self.verts)),
-                     indices=np.ascontiguousarray(np.concatenate(self.idx)),
+                     vertices=cat(self.verts, _abi.VERTEX_DTYPE),
+                     indices=cat(self.idx, np.uint32),
                      meshes=np.ascontiguousarray(meshes),
-                     instances=np.ascontiguousarray(np.concatenate(self.instances)),
-                     materials=np.ascontiguousarray(np.concatenate(self.materials)),
+                     instances=cat(self.instances, _abi.INSTANCE_DTYPE),
+                     materials=cat(self.materials, _abi.MATERIAL_DTYPE),
                      env=env, camera=camera, conf=conf, textures=list(self.textures))
 
 

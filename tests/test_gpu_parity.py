@@ -132,6 +132,77 @@ def test_keyed_streams_match_oracle(case):
         assert bias < 0.5, bias
 
 
+def _empty_scene():
+    """No geometry at all: every camera ray misses and sees the environment."""
+    b = scenes._Builder()
+    cam = _abi.make_camera((0.0, -3.0, 1.0), (0.0, 1.0, 0.0), scenes.camera_viewport(32, 24, 0.5))
+    return b.build("empty", cam, dict(width=32, height=24, spp=2, depth=3))
+
+
+def _unlit_cornell():
+    """The Cornell room without its ceiling light: no emissive triangle, so
+    light sampling is off and the room is lit through its open side by the
+    environment alone."""
+    s = scenes.cornell(64, 64)
+    s.materials["emissive_factor"] = 0.0
+    return s
+
+
+# (name, scene, W, H, spp, depth, tuning): the edge cases of the reference's
+# semantics, compared in keyed mode like KEYED.  The oracle gets the
+# environment's conf after EnvInit's clamping, as the reference's shader does.
+EDGE = [
+    ("empty_scene", _empty_scene, 32, 24, 2, 3, {}),
+    ("no_emitters_d4", _unlit_cornell, 64, 64, 2, 4, {}),
+    ("depth1_all_cut", lambda: scenes.cornell(), 64, 64, 4, 1, {}),
+    ("odd_17x9_16spp_many_chunks", lambda: scenes.icosphere_scene(subdiv=3), 17, 9, 16, 5,
+     dict(queue_capacity=4096, pipelines=2)),
+]
+
+
+@pytest.mark.parametrize("case", EDGE, ids=[k[0] for k in EDGE])
+def test_edge_cases_match_oracle(case):
+    name, mk, W, H, spp, D, tuning = case
+    s = mk()
+    g = B.LoadScene(s)
+    B.EnvInit(B.PathTraceConf(render_width=W, render_height=H, sample_count=spp, trace_depth=D))
+    if tuning:
+        B.SetTuning(**tuning)
+    conf = B.GetConf()
+    assert conf.trace_depth == min(max(D, 1), 64)
+    B.View(g, B.Camera.from_c(s.camera))
+    gpu = B.ReadFilm(_abi.CG_FILM_XYZ32F)
+    st = B.LastStats()
+    if tuning:  # several chunks, spread over both pipelines
+        assert st.chunks > 1
+    o = O.OracleScene(s)
+    ora, _, _ = o.render(conf.to_c(), s.camera, rng=O.RNG_KEYED, prune=True)
+    assert np.all(np.isfinite(gpu))
+    if name == "depth1_all_cut":  # every hit is at the depth cut: only misses add light
+        assert st.shadow_rays == 0
+    tie = primary_tie_mask(o, s.camera, W, H)
+    keep = ~tie
+    lum_g, lum_o = gpu[..., 1][keep], ora[..., 1][keep]
+    scale = max(float(np.abs(lum_o).mean()), 1e-6)
+    close = float((np.abs(lum_g - lum_o) / scale <= 1e-3).mean())
+    print(f"{name}: {int(tie.sum())} tie pixels excluded; {close:.4%} within 1e-3; "
+          f"chunks {st.chunks}, extend rays {st.extend_rays}")
+    assert close >= 0.995, close
+    assert abs(float(lum_g.mean()) - float(lum_o.mean())) / scale < 0.005
+    g.close()
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
+
+
+def test_trace_depth_is_clamped_to_1_64():
+    """EnvInit clamps trace_depth to [1, 64] (src/wgpu/environment.cpp:20).
+    No frame is rendered at 64: with two lobes per diffuse hit the sample
+    tree of this room would grow exponentially."""
+    for asked, got in ((0, 1), (1, 1), (64, 64), (70, 64), (1000, 64)):
+        B.EnvInit(B.PathTraceConf(render_width=8, render_height=8, sample_count=1, trace_depth=asked))
+        assert B.GetConf().trace_depth == got
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
+
+
 def test_converged_image_matches_reference_order_oracle():
     """GPU (keyed streams) vs the oracle in the reference's own RNG order
     (per-pixel PCG-hash streams consumed depth first), both converged:
