@@ -78,6 +78,8 @@ def _load():
         "cg_autotune_views": (i, [vp, vp, u32, C.POINTER(_abi.CgTuning)]),
         "cg_set_bvh_build": (i, [i]),
         "cg_png_decode": (i, [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), vp]),
+        "cg_hdr_decode": (i, [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), vp]),
+        "cg_env_from_cube": (i, [vp, u32, u32, vp, vp]),
         "cg_bvh_build": (i, [vp, u32, i, vp, u32, C.POINTER(u32), vp]),
         "cg_server_create": (i, [vp, u32, C.c_uint64, C.POINTER(vp)]),
         "cg_server_destroy": (i, [vp]),
@@ -231,6 +233,28 @@ def LoadScene(scene) -> Scene:
     return Scene(h.value, scene)
 
 
+def hdr_decode(data: bytes) -> np.ndarray:
+    """A Radiance .hdr image as (height, width, 4) float32 RGBA (alpha 1)."""
+    buf = np.frombuffer(data, np.uint8)
+    w, h = C.c_uint32(), C.c_uint32()
+    _check(lib.cg_hdr_decode(buf.ctypes.data, buf.size, C.byref(w), C.byref(h), None))
+    out = np.empty((h.value, w.value, 4), np.float32)
+    _check(lib.cg_hdr_decode(buf.ctypes.data, buf.size, C.byref(w), C.byref(h), out.ctypes.data))
+    return out
+
+
+def env_from_cube(faces: np.ndarray, rotation=(0.0, 0.0, 0.0, 1.0)) -> np.ndarray:
+    """The lat-long environment (2h, 4w, 4) of six (h, w, 4) float32 cube faces
+    (+X, -X, +Y, -Y, +Z, -Z) seen through the quaternion `rotation` (x, y, z, w)."""
+    f = np.ascontiguousarray(faces, np.float32)
+    assert f.ndim == 4 and f.shape[0] == 6 and f.shape[3] == 4
+    h, w = f.shape[1], f.shape[2]
+    q = np.ascontiguousarray(rotation, np.float32)
+    out = np.empty((2 * h, 4 * w, 4), np.float32)
+    _check(lib.cg_env_from_cube(f.ctypes.data, w, h, q.ctypes.data, out.ctypes.data))
+    return out
+
+
 def parse_gltf(path) -> "scenes.Scene":
     """Parses a glTF file with the native loader (no device needed) into an
     in-memory scene description (copies)."""
@@ -250,13 +274,17 @@ def parse_gltf(path) -> "scenes.Scene":
             for t in tex:
                 img = arr(t.rgba8, t.width * t.height * 4, np.uint8).reshape(t.height, t.width, 4)
                 textures.append((img, int(t.wrap_s), int(t.wrap_t)))
+        env = None
+        if d.env_rgba32f:
+            env = arr(d.env_rgba32f, d.env_width * d.env_height * 4,
+                      np.float32).reshape(d.env_height, d.env_width, 4)
         return scenes.Scene(name=os.fspath(path),
                             vertices=arr(d.vertices, d.vertex_count, _abi.VERTEX_DTYPE),
                             indices=arr(d.indices, d.index_count, np.uint32),
                             meshes=arr(d.meshes, d.mesh_count, _abi.MESH_DTYPE),
                             instances=arr(d.instances, d.instance_count, _abi.INSTANCE_DTYPE),
                             materials=arr(d.materials, d.material_count, _abi.MATERIAL_DTYPE),
-                            textures=textures)
+                            env=env, textures=textures)
     finally:
         lib.cg_gltf_free(st)
 

@@ -31,6 +31,7 @@
 #include "../../include/cg_cuda.h"
 #include "cg_api_internal.h"
 
+#include "cg_envmap.h"
 #include "cg_png.h"
 
 namespace cg {
@@ -275,6 +276,9 @@ struct Loader {
   std::vector<std::vector<uint8_t>> image_rgba;
   std::vector<std::array<uint32_t, 2>> image_size;
   std::vector<cg_texture> textures;
+  // the environment of an image-based light (lat-long RGBA32F), if any
+  std::vector<float> env;
+  uint32_t env_w = 0, env_h = 0;
 
   bool fail(const std::string& m) {
     if (err.empty()) err = m;
@@ -425,6 +429,62 @@ struct Loader {
       }
       textures.push_back(tx);
     }
+    return true;
+  }
+
+  // EXT_lights_image_based: the first specular cube (six images, the first
+  // mip level) and the first rotation, resampled to the lat-long environment
+  // (LoadImageBasedEnvironmentTexture, src/scene.cpp:588-625; the reference
+  // finds both by searching the extension's JSON text for the first
+  // "specularImages" and "rotation" keys).  No light, no complete image set:
+  // no environment (the fallback sky is used).
+  bool loadImageBasedLight() {
+    const Json* ext = doc.get("extensions");
+    const Json* ibl = ext ? ext->get("EXT_lights_image_based") : nullptr;
+    const Json* lights = ibl ? ibl->get("lights") : nullptr;
+    if (!lights || lights->kind != Json::Arr) return true;
+    const Json* set = nullptr;
+    float rotation[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+    bool have_rotation = false;
+    for (const Json& l : lights->a) {
+      const Json* si = l.get("specularImages");
+      if (!set && si && si->kind == Json::Arr && !si->a.empty() && si->a[0].kind == Json::Arr &&
+          si->a[0].a.size() >= 6)
+        set = &si->a[0];
+      const Json* r = l.get("rotation");
+      if (!have_rotation && r && r->kind == Json::Arr && r->a.size() == 4) {
+        for (int k = 0; k < 4; ++k) rotation[k] = static_cast<float>(r->a[k].n);
+        have_rotation = true;
+      }
+    }
+    if (!set) return true;
+    const Json* imgs = doc.get("images");
+    const size_t nimg = imgs ? imgs->a.size() : 0;
+    std::vector<float> faces[6];
+    uint32_t fw = 0, fh = 0;
+    for (int i = 0; i < 6; ++i) {
+      const Json& e = set->a[i];
+      if (e.kind != Json::Num || e.n < 0 || e.n != static_cast<double>(static_cast<int64_t>(e.n)))
+        return true;  // not an image index: the reference reads no image set
+      const size_t index = static_cast<size_t>(e.n);
+      if (index >= nimg) return fail("Image based light references an invalid image.");
+      std::vector<uint8_t> bytes;
+      if (!imageBytes(imgs->a[index], bytes)) return false;
+      uint32_t w = 0, h = 0;
+      std::string err;
+      if (!decodeImageRgba32f(bytes.data(), bytes.size(), w, h, faces[i], err))
+        return fail("image " + std::to_string(index) + ": " + err);
+      if (w == 0 || h == 0) return fail("Image based light has an empty cube face.");
+      if (i > 0 && (w != fw || h != fh))
+        return fail("Image based light cube faces do not share one size.");
+      fw = w;
+      fh = h;
+    }
+    const float* fp[6];
+    for (int i = 0; i < 6; ++i) fp[i] = faces[i].data();
+    cubeToLatLong(fp, fw, fh, rotation, env);
+    env_w = fw * 4;
+    env_h = fh * 2;
     return true;
   }
 
@@ -616,6 +676,7 @@ struct Loader {
     if (!p.parse(doc)) return fail("invalid JSON: " + p.err);
     if (!loadBuffers(glb ? &bin : nullptr)) return false;
     if (!loadTextures()) return false;
+    if (!loadImageBasedLight()) return false;
     loadMaterials();
     if (!loadMeshes()) return false;
     // root: Rx(+90 deg), glTF y-up -> z-up (scene.cpp:1000)
@@ -659,6 +720,11 @@ extern "C" CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void**
   d.material_count = static_cast<uint32_t>(L->materials.size());
   d.textures = L->textures.data();
   d.texture_count = static_cast<uint32_t>(L->textures.size());
+  if (!L->env.empty()) {
+    d.env_rgba32f = L->env.data();
+    d.env_width = L->env_w;
+    d.env_height = L->env_h;
+  }
   *out = d;
   *storage = L.release();
   return CG_OK;
@@ -674,6 +740,33 @@ extern "C" CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* 
   *width = w;
   *height = h;
   if (rgba_out) std::memcpy(rgba_out, rgba.data(), rgba.size());
+  return CG_OK;
+}
+
+extern "C" CG_API int cg_hdr_decode(const uint8_t* data, size_t size, uint32_t* width,
+                                   uint32_t* height, float* rgba_out) {
+  if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
+  std::vector<float> px;
+  std::string e;
+  uint32_t w = 0, h = 0;
+  if (!decodeRadianceHdr(data, size, w, h, px, e)) return fail(CG_E_INVALID, e);
+  *width = w;
+  *height = h;
+  if (rgba_out) std::memcpy(rgba_out, px.data(), px.size() * sizeof(float));
+  return CG_OK;
+}
+
+extern "C" CG_API int cg_env_from_cube(const float* faces, uint32_t face_width,
+                                      uint32_t face_height, const float* rotation, float* env_out) {
+  if (!faces || !rotation || !env_out) return fail(CG_E_INVALID, "null argument");
+  if (face_width == 0 || face_height == 0 || face_width > (1u << 14) || face_height > (1u << 14))
+    return fail(CG_E_INVALID, "cube face size must be in [1, 16384]");
+  const size_t face = size_t(face_width) * face_height * 4;
+  const float* fp[6];
+  for (int i = 0; i < 6; ++i) fp[i] = faces + i * face;
+  std::vector<float> out;
+  cubeToLatLong(fp, face_width, face_height, rotation, out);
+  std::memcpy(env_out, out.data(), out.size() * sizeof(float));
   return CG_OK;
 }
 

@@ -203,6 +203,22 @@ CG_API int cg_gltf_free(void* storage);
  * hold width * height * 4 bytes. */
 CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* width, uint32_t* height,
                          uint8_t* rgba_out);
+/* A Radiance RGBE (.hdr) image to linear RGBA32F, alpha 1 (stb_image's HDR
+ * loader, which the reference's DecodeImageRgba32f uses for environment
+ * faces, src/image_decode.cpp:51-88): "-Y height +X width" images, flat or
+ * run-length-encoded scanlines.  With rgba_out == NULL only the size is set;
+ * otherwise rgba_out holds width * height * 4 floats. */
+CG_API int cg_hdr_decode(const uint8_t* data, size_t size, uint32_t* width, uint32_t* height,
+                         float* rgba_out);
+/* The lat-long environment of an image-based light's cube
+ * (CubeToEnvironmentTexture, src/scene.cpp:541-575): `faces` holds six
+ * face_width x face_height RGBA32F images (+X, -X, +Y, -Y, +Z, -Z as
+ * EXT_lights_image_based lists them) one after another; `rotation` is the
+ * light's quaternion (x, y, z, w); `env_out` receives (2 * face_height) rows
+ * of (4 * face_width) RGBA32F texels.  cg_scene_load_gltf / cg_gltf_parse do
+ * this for a file's first image-based light (PNG or HDR faces). */
+CG_API int cg_env_from_cube(const float* faces, uint32_t face_width, uint32_t face_height,
+                            const float* rotation, float* env_out);
 
 typedef struct cg_scene_info {
   uint32_t instance_count, mesh_count, triangle_count, material_count;

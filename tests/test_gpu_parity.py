@@ -148,12 +148,35 @@ def _unlit_cornell():
     return s
 
 
+def _ibl_env(seed=7):
+    """A lat-long environment made from a random HDR cube (an image-based
+    light, cg_env_from_cube) instead of the fallback sky."""
+    rng = np.random.default_rng(seed)
+    faces = np.ones((6, 16, 16, 4), np.float32)
+    faces[..., :3] = rng.lognormal(-0.5, 1.0, (6, 16, 16, 3)).astype(np.float32)
+    return B.env_from_cube(faces, (0.1, 0.6, -0.2, 0.77))
+
+
+def _empty_ibl():
+    s = _empty_scene()
+    s.env = _ibl_env()
+    return s
+
+
+def _unlit_cornell_ibl():
+    s = _unlit_cornell()
+    s.env = _ibl_env(8)
+    return s
+
+
 # (name, scene, W, H, spp, depth, tuning): the edge cases of the reference's
 # semantics, compared in keyed mode like KEYED.  The oracle gets the
 # environment's conf after EnvInit's clamping, as the reference's shader does.
 EDGE = [
     ("empty_scene", _empty_scene, 32, 24, 2, 3, {}),
     ("no_emitters_d4", _unlit_cornell, 64, 64, 2, 4, {}),
+    ("empty_scene_ibl_env", _empty_ibl, 32, 24, 2, 3, {}),
+    ("no_emitters_ibl_env_d4", _unlit_cornell_ibl, 64, 64, 2, 4, {}),
     ("depth1_all_cut", lambda: scenes.cornell(), 64, 64, 4, 1, {}),
     ("odd_17x9_16spp_many_chunks", lambda: scenes.icosphere_scene(subdiv=3), 17, 9, 16, 5,
      dict(queue_capacity=4096, pipelines=2)),
