@@ -121,14 +121,30 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons during the timed region:
+    read-only NVML queries every 20 ms from a thread (nvidia-smi at 200 ms
+    where NVML is not available)."""
+
+    NVML_PERIOD_S = 0.02
 
     def __init__(self, index):
         self.index = index
         self.samples = []
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml = pynvml
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         cmd = ["nvidia-smi", "-i", str(self.index),
                "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -143,6 +159,23 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        n = self.nvml
+        bits = [n.nvmlClocksEventReasonHwSlowdown, n.nvmlClocksEventReasonHwThermalSlowdown,
+                n.nvmlClocksEventReasonSwThermalSlowdown, n.nvmlClocksEventReasonSwPowerCap]
+        while not self.stop.is_set():
+            try:
+                sm = n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)
+                mx = n.nvmlDeviceGetMaxClockInfo(self.handle, n.NVML_CLOCK_SM)
+                r = n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+            except Exception:
+                return
+            # the same row layout as the nvidia-smi query below
+            row = [str(sm), str(mx), "", hex(r)] + \
+                ["Active" if r & b else "Not Active" for b in bits]
+            self.samples.append((time.perf_counter(), row))
+            self.stop.wait(self.NVML_PERIOD_S)
+
     def _read(self):
         for line in self.proc.stdout:
             self.samples.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
@@ -153,6 +186,13 @@ class ClockSampler:
         self.samples = inside if inside else self.samples[-1:]
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=5)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -174,7 +214,8 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 # --workload: the plain-path configurations (the icosphere frame is the default
