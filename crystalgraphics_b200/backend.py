@@ -79,6 +79,7 @@ def _load():
         "cg_set_bvh_build": (i, [i]),
         "cg_png_decode": (i, [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), vp]),
         "cg_hdr_decode": (i, [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), vp]),
+        "cg_jpeg_decode": (i, [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), vp]),
         "cg_env_from_cube": (i, [vp, u32, u32, vp, vp]),
         "cg_bvh_build": (i, [vp, u32, i, vp, u32, C.POINTER(u32), vp]),
         "cg_server_create": (i, [vp, u32, C.c_uint64, C.POINTER(vp)]),
@@ -231,6 +232,16 @@ def LoadScene(scene) -> Scene:
     h = C.c_void_p()
     _check(lib.cg_scene_create(C.byref(desc), C.byref(h)))
     return Scene(h.value, scene)
+
+
+def jpeg_decode(data: bytes) -> np.ndarray:
+    """A JPEG image as (height, width, 4) uint8 RGBA (alpha 255)."""
+    buf = np.frombuffer(data, np.uint8)
+    w, h = C.c_uint32(), C.c_uint32()
+    _check(lib.cg_jpeg_decode(buf.ctypes.data, buf.size, C.byref(w), C.byref(h), None))
+    out = np.empty((h.value, w.value, 4), np.uint8)
+    _check(lib.cg_jpeg_decode(buf.ctypes.data, buf.size, C.byref(w), C.byref(h), out.ctypes.data))
+    return out
 
 
 def hdr_decode(data: bytes) -> np.ndarray:

@@ -5,16 +5,15 @@
 // reads (src/scene.cpp:541-625, LoadImageBasedEnvironmentTexture /
 // CubeToEnvironmentTexture), decoding the faces with stb_image's float loader
 // (src/image_decode.cpp:51-88).  stb_image is not available here, so the two
-// formats it would see in practice are decoded by this file (Radiance HDR)
-// and cg_png.cpp (PNG), and stb's 8-bit-to-float rule is restated; JPEG
-// faces are not supported.
+// formats are decoded by this file (Radiance HDR) and cg_png.cpp /
+// cg_jpeg.cpp (PNG, JPEG), and stb's 8-bit-to-float rule is restated.
 #include "cg_envmap.h"
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 
-#include "cg_png.h"
+#include "cg_jpeg.h"
 
 namespace cg {
 namespace {
@@ -133,7 +132,7 @@ bool decodeImageRgba32f(const uint8_t* data, size_t size, uint32_t& width, uint3
   if (size >= 2 && data[0] == '#' && data[1] == '?')
     return decodeRadianceHdr(data, size, width, height, rgba, err);
   std::vector<uint8_t> px;
-  if (!decodePng(data, size, width, height, px, err)) return false;
+  if (!decodeImageRgba8(data, size, width, height, px, err)) return false;
   // stb_image's LDR -> float (stbi__ldr_to_hdr with its default gamma 2.2 and
   // scale 1): colour channels (c / 255)^2.2, alpha c / 255.  The reference
   // compiles stb in a C++ file, where pow(float, float) is the float overload.

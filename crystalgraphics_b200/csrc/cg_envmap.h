@@ -16,8 +16,8 @@ bool decodeRadianceHdr(const uint8_t* data, size_t size, uint32_t& width, uint32
                        std::vector<float>& rgba, std::string& err);
 
 // Decodes an image to linear RGBA32F as the reference's DecodeImageRgba32f
-// does: Radiance HDR as is, PNG through its 8-bit RGBA with the colour
-// channels raised to the power 2.2 and alpha scaled to [0, 1].
+// does: Radiance HDR as is, PNG and JPEG through their 8-bit RGBA with the
+// colour channels raised to the power 2.2 and alpha scaled to [0, 1].
 bool decodeImageRgba32f(const uint8_t* data, size_t size, uint32_t& width, uint32_t& height,
                         std::vector<float>& rgba, std::string& err);
 

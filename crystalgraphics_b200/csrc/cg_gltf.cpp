@@ -32,6 +32,7 @@
 #include "cg_api_internal.h"
 
 #include "cg_envmap.h"
+#include "cg_jpeg.h"
 #include "cg_png.h"
 
 namespace cg {
@@ -413,7 +414,7 @@ struct Loader {
         if (!imageBytes(imgs->a[src], bytes)) return false;
         std::string e;
         uint32_t w = 0, h = 0;
-        if (!decodePng(bytes.data(), bytes.size(), w, h, image_rgba[src], e))
+        if (!decodeImageRgba8(bytes.data(), bytes.size(), w, h, image_rgba[src], e))
           return fail("image " + std::to_string(src) + ": " + e);
         image_size[src] = {w, h};
       }
@@ -740,6 +741,19 @@ extern "C" CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* 
   *width = w;
   *height = h;
   if (rgba_out) std::memcpy(rgba_out, rgba.data(), rgba.size());
+  return CG_OK;
+}
+
+extern "C" CG_API int cg_jpeg_decode(const uint8_t* data, size_t size, uint32_t* width,
+                                    uint32_t* height, uint8_t* rgba_out) {
+  if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
+  std::vector<uint8_t> px;
+  std::string e;
+  uint32_t w = 0, h = 0;
+  if (!decodeJpeg(data, size, w, h, px, e)) return fail(CG_E_INVALID, e);
+  *width = w;
+  *height = h;
+  if (rgba_out) std::memcpy(rgba_out, px.data(), px.size());
   return CG_OK;
 }
 

@@ -198,11 +198,21 @@ CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out);
 CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage);
 CG_API int cg_gltf_free(void* storage);
 /* Decodes a PNG file image to RGBA8 (the reference decodes glTF images with
- * stb_image, src/image_decode.cpp:12-45; JPEG is not supported here).  With
+ * stb_image, src/image_decode.cpp:12-45; JPEG: cg_jpeg_decode).  With
  * rgba_out == NULL only *width and *height are set; otherwise rgba_out must
  * hold width * height * 4 bytes. */
 CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* width, uint32_t* height,
                          uint8_t* rgba_out);
+/* A JPEG image to RGBA8 (the JPEG half of the reference's DecodeImageRgba8,
+ * src/image_decode.cpp:12-45, written from ITU-T T.81 since stb_image is not
+ * available): baseline, extended sequential and progressive Huffman-coded
+ * 8-bit images, grey or three components, any sampling factors, restart
+ * intervals.  Values can differ from stb_image's by a level or two (IDCT and
+ * colour-conversion rounding).  Same calling convention as cg_png_decode;
+ * glTF images and image-based-light faces are decoded as PNG or JPEG by their
+ * signatures. */
+CG_API int cg_jpeg_decode(const uint8_t* data, size_t size, uint32_t* width, uint32_t* height,
+                          uint8_t* rgba_out);
 /* A Radiance RGBE (.hdr) image to linear RGBA32F, alpha 1 (stb_image's HDR
  * loader, which the reference's DecodeImageRgba32f uses for environment
  * faces, src/image_decode.cpp:51-88): "-Y height +X width" images, flat or
