@@ -1,8 +1,9 @@
 // cg_gltf.cpp — glTF 2.0 loader for LoadScene(path).
 //
-// The reference loads glTF through cgltf (src/scene.cpp:829-1003); cgltf is
-// not available here, so this is a self-contained reader of the subset the
-// path tracer consumes, with the reference's conventions:
+// The reference loads glTF through cgltf v1.14 (src/scene.cpp:829-1003; the
+// library is fetched at build time by lib/cgltf/CMakeLists.txt), which is not
+// available here, so this is a self-contained reader of the subset the path
+// tracer consumes, with the reference's conventions:
 //   - material 0 is the default material, glTF material i becomes i + 1, a
 //     primitive without a material uses 0 (scene.cpp:869-872, 952-956);
 //   - the default material is glTF's defaults (scene.cpp:659-690);
@@ -14,9 +15,11 @@
 //   - the y-up glTF world is rotated by +90 degrees about x to z-up
 //     (scene.cpp:1000).
 // Supported: .gltf with external .bin or base64 data URIs, and .glb.
+//   - sparse accessors read as zeros, as cgltf's per-element readers return
+//     them (see readAccessor).
 // Material extensions read: KHR_materials_emissive_strength, _ior,
-// _transmission, _volume (thickness), _dispersion.  Textured materials are
-// rejected by the scene packer.
+// _transmission, _volume (thickness), _dispersion; the four textures the
+// shader samples; EXT_lights_image_based (the environment).
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -316,7 +319,6 @@ struct Loader {
     const Json* acc = doc.get("accessors");
     if (!acc || idx < 0 || size_t(idx) >= acc->a.size()) return fail("bad accessor index");
     const Json& a = acc->a[idx];
-    if (a.get("sparse")) return fail("sparse accessors are not supported");
     count = static_cast<size_t>(a.integer("count", 0));
     const int64_t ctype = a.integer("componentType", 5126);
     const bool normalized = a.get("normalized") && a.get("normalized")->b;
@@ -325,6 +327,14 @@ struct Loader {
     if (ncomp == 0) return fail("unsupported accessor type " + type);
     int csize = (ctype == 5120 || ctype == 5121) ? 1 : (ctype == 5122 || ctype == 5123) ? 2 : 4;
     out.assign(count * comps, 0.0);
+    if (const Json* sp = a.get("sparse")) {
+      // cgltf v1.14 (the reference's glTF library) validates the sparse
+      // block, but its cgltf_accessor_read_float / cgltf_accessor_read_index
+      // return without reading an element of a sparse accessor, so every
+      // element of one reaches the reference's vertices and indices as the
+      // zero they were resized to (src/scene.cpp:900-945).
+      return checkSparse(*sp, count, size_t(ncomp * csize));
+    }
     if (!a.get("bufferView")) return true;  // all zeros
     const Json* bvs = doc.get("bufferViews");
     const int64_t bvi = a.integer("bufferView", -1);
@@ -346,16 +356,52 @@ struct Loader {
         switch (ctype) {
           case 5126: { float f; std::memcpy(&f, q, 4); v = f; break; }
           case 5125: { uint32_t u; std::memcpy(&u, q, 4); v = u; break; }
-          case 5123: { uint16_t u; std::memcpy(&u, q, 2); v = normalized ? u / 65535.0 : u; break; }
-          case 5121: { uint8_t u = *q; v = normalized ? u / 255.0 : u; break; }
-          case 5122: { int16_t s; std::memcpy(&s, q, 2); v = normalized ? std::max(s / 32767.0, -1.0) : s; break; }
-          case 5120: { int8_t s = static_cast<int8_t>(*q); v = normalized ? std::max(s / 127.0, -1.0) : s; break; }
+          // normalized integers divide in float, as cgltf does
+          case 5123: { uint16_t u; std::memcpy(&u, q, 2); v = normalized ? u / 65535.0f : u; break; }
+          case 5121: { uint8_t u = *q; v = normalized ? u / 255.0f : u; break; }
+          case 5122: { int16_t s; std::memcpy(&s, q, 2); v = normalized ? std::max(s / 32767.0f, -1.0f) : s; break; }
+          case 5120: { int8_t s = static_cast<int8_t>(*q); v = normalized ? std::max(s / 127.0f, -1.0f) : s; break; }
           default: return fail("unsupported component type");
         }
         out[e * comps + c] = v;
       }
     }
     return true;
+  }
+
+  // The sparse block of an accessor with `count` elements of `elem_bytes`:
+  // its indices (unsigned, each below `count`) and values must lie in their
+  // buffer views, the checks cgltf_validate makes.
+  bool checkSparse(const Json& sp, size_t count, size_t elem_bytes) {
+    const int64_t n = sp.integer("count", 0);
+    const Json* ix = sp.get("indices");
+    const Json* vs = sp.get("values");
+    if (n < 1 || size_t(n) > count || !ix || !vs) return fail("invalid sparse accessor");
+    const int64_t ct = ix->integer("componentType", 0);
+    const size_t isz = ct == 5121 ? 1 : ct == 5123 ? 2 : ct == 5125 ? 4 : 0;
+    if (!isz) return fail("invalid sparse accessor index type");
+    const uint8_t* idx = viewBytes(ix->integer("bufferView", -1), ix->integer("byteOffset", 0), size_t(n) * isz);
+    if (!idx || !viewBytes(vs->integer("bufferView", -1), vs->integer("byteOffset", 0), size_t(n) * elem_bytes))
+      return fail("sparse accessor data exceeds its buffer view");
+    for (int64_t k = 0; k < n; ++k) {
+      uint32_t v = 0;
+      std::memcpy(&v, idx + size_t(k) * isz, isz);  // little-endian
+      if (size_t(v) >= count) return fail("invalid sparse accessor index");
+    }
+    return true;
+  }
+
+  // `size` bytes at `offset` in buffer view `bvi`, or null when they do not
+  // lie inside the view and its buffer.
+  const uint8_t* viewBytes(int64_t bvi, int64_t offset, size_t size) {
+    const Json* bvs = doc.get("bufferViews");
+    if (!bvs || bvi < 0 || size_t(bvi) >= bvs->a.size() || offset < 0) return nullptr;
+    const Json& bv = bvs->a[bvi];
+    const int64_t bi = bv.integer("buffer", -1);
+    if (bi < 0 || size_t(bi) >= buffers.size()) return nullptr;
+    const size_t vo = size_t(bv.integer("byteOffset", 0)), vl = size_t(bv.integer("byteLength", 0));
+    if (size_t(offset) + size > vl || vo + vl > buffers[bi].size()) return nullptr;
+    return buffers[bi].data() + vo + size_t(offset);
   }
 
   int32_t textureIndex(const Json* info) {

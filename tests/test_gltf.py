@@ -2,6 +2,7 @@
 (default material first, glTF material i -> i + 1, y-up -> z-up root
 rotation), checked on the host against the in-memory descriptions it was
 written from, and the C++23 crystal::graphics layer's error path."""
+import base64
 import json
 import os
 import struct
@@ -117,3 +118,56 @@ def test_gltf_textures_round_trip(tmp_path):
     a, aa, _ = O.OracleScene(s).emissive()
     b, ba, _ = O.OracleScene(p).emissive()
     assert a.tobytes() == b.tobytes() and aa.tobytes() == ba.tobytes()
+
+
+def _one_triangle_doc(pos_accessor, extra_views=(), blob=b""):
+    """A glTF with one indexed triangle whose POSITION accessor is given."""
+    idx = np.array([0, 1, 2], np.uint16).tobytes() + b"\0\0"
+    uv = np.array([[0, 255], [128, 7], [255, 0]], np.uint8).tobytes() + b"\0\0"
+    data = idx + uv + blob
+    views = [{"buffer": 0, "byteOffset": 0, "byteLength": 6},
+             {"buffer": 0, "byteOffset": 8, "byteLength": 6}] + list(extra_views)
+    accs = [{"bufferView": 0, "componentType": 5123, "count": 3, "type": "SCALAR"},
+            {"bufferView": 1, "componentType": 5121, "normalized": True, "count": 3, "type": "VEC2"},
+            pos_accessor]
+    return {"asset": {"version": "2.0"},
+            "buffers": [{"byteLength": len(data),
+                         "uri": "data:application/octet-stream;base64," + base64.b64encode(data).decode()}],
+            "bufferViews": views, "accessors": accs,
+            "meshes": [{"primitives": [{"attributes": {"POSITION": 2, "TEXCOORD_0": 1}, "indices": 0}]}],
+            "nodes": [{"mesh": 0}], "scenes": [{"nodes": [0]}], "scene": 0}
+
+
+def _load(tmp_path, doc):
+    p = tmp_path / "t.gltf"
+    p.write_text(json.dumps(doc))
+    return B.parse_gltf(str(p))
+
+
+def test_normalized_and_sparse_accessors(tmp_path):
+    # normalized u8 texture coordinates: c / 255 divided in float (cgltf)
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32).tobytes()
+    dense = {"bufferView": 2, "componentType": 5126, "count": 3, "type": "VEC3"}
+    p = _load(tmp_path, _one_triangle_doc(dense, [{"buffer": 0, "byteOffset": 16, "byteLength": 36}], pos))
+    uv = np.array([[0, 255], [128, 7], [255, 0]], np.float32) / np.float32(255)
+    assert p.vertices["tex_coord0"].tobytes() == uv.astype(np.float32).tobytes()
+    assert p.vertices["position"].reshape(-1).tobytes() == pos
+    # a sparse POSITION accessor: cgltf's element reader does not apply it, so
+    # the reference's vertices keep the zero they were resized to
+    sp_idx = np.array([1], np.uint8).tobytes() + b"\0\0\0"
+    sp_val = np.array([5, 6, 7], np.float32).tobytes()
+    views = [{"buffer": 0, "byteOffset": 16, "byteLength": 36},
+             {"buffer": 0, "byteOffset": 52, "byteLength": 1},
+             {"buffer": 0, "byteOffset": 56, "byteLength": 12}]
+    sparse = dict(dense, sparse={"count": 1, "indices": {"bufferView": 3, "componentType": 5121},
+                                 "values": {"bufferView": 4}})
+    p = _load(tmp_path, _one_triangle_doc(sparse, views, pos + sp_idx + sp_val))
+    assert len(p.vertices) == 3 and not p.vertices["position"].any()
+    np.testing.assert_array_equal(p.indices, [0, 1, 2])
+    # cgltf_validate's checks of the sparse block
+    bad_index = np.array([3], np.uint8).tobytes() + b"\0\0\0"
+    with pytest.raises(B.Error, match="sparse accessor index"):
+        _load(tmp_path, _one_triangle_doc(sparse, views, pos + bad_index + sp_val))
+    short = [views[0], views[1], dict(views[2], byteLength=8)]
+    with pytest.raises(B.Error, match="exceeds its buffer view"):
+        _load(tmp_path, _one_triangle_doc(sparse, short, pos + sp_idx + sp_val))
