@@ -11,7 +11,7 @@ import time
 import numpy as np
 import pytest
 
-from crystalgraphics_b200 import _abi, gltf, scenes
+from crystalgraphics_b200 import _abi, film_io, gltf, scenes
 from crystalgraphics_b200 import backend as B
 
 from gpu_common import small_instanced
@@ -321,10 +321,16 @@ def test_gltf_scene_renders_like_the_in_memory_scene(tmp_path, cornell):
         [str(x) for x in list(cam.position) + list(cam.direction) + list(cam.viewport)]
     r = subprocess.run(args, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
-    data = out.read_bytes()
-    header_end = data.index(b"255\n") + 4
-    img = np.frombuffer(data[header_end:], np.uint8).reshape(64, 64, 3)
+    img = film_io.load_ppm(out)
+    # the same frame as a PFM of the linear RGB32F film
+    args[2] = str(tmp_path / "c.pfm")
+    r = subprocess.run(args, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    lin = film_io.load_pfm(tmp_path / "c.pfm")
     B.EnvInit(conf)
     B.View(g, cam)
     ref = B.ReadFilm(_abi.CG_FILM_RGBA8)[..., :3]
     assert np.abs(img.astype(int) - ref.astype(int)).max() <= 1
+    ref_lin = B.ReadFilm(_abi.CG_FILM_RGB32F)
+    assert lin.shape == ref_lin.shape == (64, 64, 3)
+    np.testing.assert_allclose(lin, ref_lin, rtol=1e-4, atol=1e-6 * float(np.abs(ref_lin).mean()))
