@@ -215,3 +215,21 @@ def test_gltf_ibl_errors_and_absence(tmp_path):
     # fewer than six images: no environment, as in the reference
     s = B.parse_gltf(_gltf_with_ibl(tmp_path, [one] * 6, "image/png", sets=[[0, 1, 2]]))
     assert s.env is None
+
+
+def test_corrupt_hdr_files_fail_cleanly():
+    rng = np.random.default_rng(8)
+    seeds = [_hdr_bytes(_rgbe(rng.lognormal(0, 2, (4, 16, 3))), True),
+             _hdr_bytes(_rgbe(rng.lognormal(0, 2, (3, 9, 3))), False)]
+    for trial in range(400):  # errors are fine; a crash would end the test run
+        d = bytearray(seeds[trial % 2])
+        for _ in range(int(rng.integers(1, 6))):
+            p = int(rng.integers(0, len(d)))
+            d[p] = int(rng.integers(0, 256)) if rng.random() < 0.7 else d[p] ^ 1
+        if trial % 3 == 0:
+            d = d[: int(rng.integers(1, len(d)))]
+        try:
+            img = B.hdr_decode(bytes(d))
+            assert img.ndim == 3 and img.shape[2] == 4
+        except B.Error:
+            pass

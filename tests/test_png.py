@@ -3,6 +3,9 @@ depth, the five scanline filters, Adam7 interlacing, stored / fixed / dynamic
 DEFLATE blocks, and tRNS transparency, against the expected RGBA8 (8-bit
 expansion as stb_image does it: 16-bit keeps the high byte, low-depth grey is
 scaled to 0..255)."""
+import struct
+import zlib
+
 import numpy as np
 import pytest
 
@@ -89,3 +92,55 @@ def test_jpeg_and_garbage_are_rejected():
     good = png.encode_rgba8(np.zeros((3, 3, 4), np.uint8))
     with pytest.raises(B.Error):
         B.png_decode(good[: len(good) - 30])  # truncated stream
+
+
+def _chunks(data):
+    p, out = 8, []
+    while p + 8 <= len(data):
+        n = struct.unpack(">I", data[p:p + 4])[0]
+        out.append([data[p + 4:p + 8], bytearray(data[p + 8:p + 8 + n])])
+        p += 12 + n
+    return out
+
+
+def _assemble(chunks):
+    out = b"\x89PNG\r\n\x1a\n"
+    for kind, body in chunks:
+        out += struct.pack(">I", len(body)) + kind + bytes(body) + struct.pack(">I", zlib.crc32(kind + bytes(body)))
+    return out
+
+
+@pytest.mark.parametrize("color_type,depth", [(png.RGBA, 8), (png.RGB, 16), (png.PALETTE, 4), (png.GREY, 1)])
+def test_corrupt_pngs_with_valid_checksums_fail_cleanly(color_type, depth):
+    """Header fields, palette / transparency lengths and scanline bytes changed
+    with the chunk CRCs and the zlib stream kept valid, so that the checks
+    after decompression are what reject them (or the image decodes)."""
+    rng = np.random.default_rng(depth)
+    ch = {png.RGBA: 4, png.RGB: 3, png.PALETTE: 1, png.GREY: 1}[color_type]
+    samples = rng.integers(0, 1 << depth, (9, 13, ch))
+    pal = rng.integers(0, 256, (16, 3)) if color_type == png.PALETTE else None
+    trns = rng.integers(0, 256, 5) if color_type == png.PALETTE else None
+    chunks = _chunks(png.encode(samples, color_type, depth, palette=pal, trns=trns, interlace=depth == 4))
+    raw0 = zlib.decompress(b"".join(bytes(b) for k, b in chunks if k == b"IDAT"))
+    head = [c for c in chunks if c[0] not in (b"IDAT", b"IEND")]
+    for _ in range(150):  # errors are fine; a crash would end the test run
+        cs = [[k, bytearray(b)] for k, b in head]
+        for k, b in cs:
+            if k == b"IHDR" and rng.random() < 0.6:
+                f = int(rng.integers(0, 13))
+                b[f] = int(rng.integers(0, 256)) if f >= 8 else b[f] ^ (1 << int(rng.integers(0, 8)))
+            if k in (b"PLTE", b"tRNS") and rng.random() < 0.3:
+                del b[int(rng.integers(0, len(b) + 1)):]
+        raw = bytearray(raw0)
+        for _ in range(int(rng.integers(0, 4))):
+            p = int(rng.integers(0, len(raw)))
+            if rng.random() < 0.5:
+                raw[p] = int(rng.integers(0, 256))
+            else:
+                del raw[p:p + int(rng.integers(1, 20))]
+        data = _assemble(cs + [[b"IDAT", zlib.compress(bytes(raw))], [b"IEND", b""]])
+        try:
+            out = B.png_decode(data)
+            assert out.ndim == 3 and out.shape[2] == 4
+        except B.Error:
+            pass
