@@ -27,6 +27,7 @@
 #include <fstream>
 #include <map>
 #include <memory>
+#include <new>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -59,16 +60,29 @@ struct Json {
     const Json* j = get(k);
     return (j && j->kind == Num) ? j->n : def;
   }
+  // The number truncated to an integer, clamped to +-2^53 (exact in a
+  // double) so that the conversion is defined and a sum of two cannot overflow.
+  int64_t asInt() const {
+    constexpr double kLim = 9007199254740992.0;
+    return static_cast<int64_t>(std::fmax(-kLim, std::fmin(n, kLim)));
+  }
   int64_t integer(const std::string& k, int64_t def) const {
     const Json* j = get(k);
-    return (j && j->kind == Num) ? static_cast<int64_t>(j->n) : def;
+    return j && j->kind == Num ? j->asInt() : def;
   }
 };
+
+// [off, off + len) lies inside [0, limit).
+bool within(int64_t off, int64_t len, size_t limit) {
+  return off >= 0 && len >= 0 && uint64_t(off) <= limit && uint64_t(len) <= limit - uint64_t(off);
+}
 
 struct Parser {
   const char* p;
   const char* end;
   std::string err;
+  int depth = 0;  // open arrays and objects; bounded so that recursion cannot exhaust the stack
+  static constexpr int kMaxDepth = 256;
 
   void ws() {
     while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
@@ -77,8 +91,12 @@ struct Parser {
     ws();
     if (p >= end) return fail("unexpected end");
     char c = *p;
-    if (c == '{') return object(out);
-    if (c == '[') return array(out);
+    if (c == '{' || c == '[') {
+      if (++depth > kMaxDepth) return fail("JSON nested too deeply");
+      const bool ok = c == '{' ? object(out) : array(out);
+      --depth;
+      return ok;
+    }
     if (c == '"') {
       out.kind = Json::Str;
       return string(out.s);
@@ -116,10 +134,19 @@ struct Parser {
     return fail("bad literal");
   }
   bool number(Json& out) {
+    // the JSON number grammar's characters, copied so that strtod cannot read
+    // past the end of the text (a GLB's JSON chunk is not NUL-terminated)
+    char buf[64];
+    size_t n = 0;
+    while (p + n < end && n < sizeof(buf) - 1 && std::strchr("0123456789+-.eE", p[n]) && p[n]) {
+      buf[n] = p[n];
+      ++n;
+    }
+    buf[n] = '\0';
     char* e = nullptr;
-    out.n = std::strtod(p, &e);
-    if (e == p) return fail("bad number");
-    p = e;
+    out.n = std::strtod(buf, &e);
+    if (e == buf) return fail("bad number");
+    p += e - buf;
     out.kind = Json::Num;
     return true;
   }
@@ -138,8 +165,14 @@ struct Parser {
           case 'f': s += '\f'; break;
           case 'u': {
             if (end - p < 4) return fail("bad unicode escape");
-            unsigned v = static_cast<unsigned>(std::stoul(std::string(p, 4), nullptr, 16));
-            p += 4;
+            unsigned v = 0;
+            for (int k = 0; k < 4; ++k, ++p) {
+              const char h = *p;
+              const int d = h >= '0' && h <= '9' ? h - '0' : h >= 'a' && h <= 'f' ? h - 'a' + 10
+                          : h >= 'A' && h <= 'F' ? h - 'A' + 10 : -1;
+              if (d < 0) return fail("bad unicode escape");
+              v = v * 16 + unsigned(d);
+            }
             if (v < 0x80) {
               s += static_cast<char>(v);
             } else if (v < 0x800) {
@@ -314,44 +347,64 @@ struct Loader {
     return true;
   }
 
+  // Elements allowed in an accessor without a bufferView (all zeros): 2^26,
+  // far above any mesh's vertex count (a 1.3M-triangle sphere has 0.66M), so
+  // that a damaged count fails instead of allocating gigabytes of zeros.
+  static constexpr size_t kMaxZeroAccessor = size_t(1) << 26;
+
   // Reads accessor `idx` as `comps` floats per element (or as indices).
   bool readAccessor(int64_t idx, int comps, std::vector<double>& out, size_t& count) {
     const Json* acc = doc.get("accessors");
     if (!acc || idx < 0 || size_t(idx) >= acc->a.size()) return fail("bad accessor index");
     const Json& a = acc->a[idx];
-    count = static_cast<size_t>(a.integer("count", 0));
+    const int64_t n = a.integer("count", 0);
+    if (n < 0 || n > int64_t(UINT32_MAX)) return fail("invalid accessor count");
+    count = static_cast<size_t>(n);
     const int64_t ctype = a.integer("componentType", 5126);
     const bool normalized = a.get("normalized") && a.get("normalized")->b;
     const std::string type = a.get("type") ? a.get("type")->s : "SCALAR";
     int ncomp = type == "SCALAR" ? 1 : type == "VEC2" ? 2 : type == "VEC3" ? 3 : type == "VEC4" ? 4 : 0;
     if (ncomp == 0) return fail("unsupported accessor type " + type);
     int csize = (ctype == 5120 || ctype == 5121) ? 1 : (ctype == 5122 || ctype == 5123) ? 2 : 4;
-    out.assign(count * comps, 0.0);
+    const size_t elem = size_t(ncomp * csize);
+    const uint8_t* src = nullptr;
+    size_t stride = elem;
+    if (a.get("bufferView")) {
+      const Json* bvs = doc.get("bufferViews");
+      const int64_t bvi = a.integer("bufferView", -1);
+      if (!bvs || bvi < 0 || size_t(bvi) >= bvs->a.size()) return fail("bad bufferView");
+      const Json& bv = bvs->a[bvi];
+      const int64_t bi = bv.integer("buffer", -1);
+      if (bi < 0 || size_t(bi) >= buffers.size()) return fail("bad buffer index");
+      const std::vector<uint8_t>& buf = buffers[bi];
+      // the view inside its buffer and the accessor inside its view, the
+      // checks cgltf_validate makes (before anything is allocated for it)
+      const int64_t vo = bv.integer("byteOffset", 0), vl = bv.integer("byteLength", 0);
+      const int64_t ao = a.integer("byteOffset", 0), bs = bv.integer("byteStride", 0);
+      if (!within(vo, vl, buf.size())) return fail("bufferView exceeds its buffer");
+      if (bs < 0 || bs > 252) return fail("invalid byteStride");
+      if (bs) stride = size_t(bs);
+      if (count && !within(ao, int64_t((count - 1) * stride + elem), size_t(vl)))
+        return fail("accessor exceeds its buffer");
+      src = buf.data() + size_t(vo + ao);
+    } else if (count > kMaxZeroAccessor) {
+      return fail("accessor without a bufferView has too many elements");
+    }
     if (const Json* sp = a.get("sparse")) {
       // cgltf v1.14 (the reference's glTF library) validates the sparse
       // block, but its cgltf_accessor_read_float / cgltf_accessor_read_index
       // return without reading an element of a sparse accessor, so every
       // element of one reaches the reference's vertices and indices as the
       // zero they were resized to (src/scene.cpp:900-945).
-      return checkSparse(*sp, count, size_t(ncomp * csize));
+      if (!checkSparse(*sp, count, elem)) return false;
+      src = nullptr;
     }
-    if (!a.get("bufferView")) return true;  // all zeros
-    const Json* bvs = doc.get("bufferViews");
-    const int64_t bvi = a.integer("bufferView", -1);
-    if (!bvs || bvi < 0 || size_t(bvi) >= bvs->a.size()) return fail("bad bufferView");
-    const Json& bv = bvs->a[bvi];
-    const int64_t bi = bv.integer("buffer", -1);
-    if (bi < 0 || size_t(bi) >= buffers.size()) return fail("bad buffer index");
-    const std::vector<uint8_t>& buf = buffers[bi];
-    const size_t base = size_t(bv.integer("byteOffset", 0)) + size_t(a.integer("byteOffset", 0));
-    const size_t stride = bv.integer("byteStride", 0) ? size_t(bv.integer("byteStride", 0))
-                                                      : size_t(ncomp * csize);
-    if (count && base + (count - 1) * stride + size_t(ncomp * csize) > buf.size())
-      return fail("accessor exceeds its buffer");
+    out.assign(count * comps, 0.0);
+    if (!src) return true;  // all zeros
     for (size_t e = 0; e < count; ++e) {
-      const uint8_t* src = buf.data() + base + e * stride;
+      const uint8_t* el = src + e * stride;
       for (int c = 0; c < std::min(ncomp, comps); ++c) {
-        const uint8_t* q = src + c * csize;
+        const uint8_t* q = el + c * csize;
         double v = 0;
         switch (ctype) {
           case 5126: { float f; std::memcpy(&f, q, 4); v = f; break; }
@@ -399,9 +452,9 @@ struct Loader {
     const Json& bv = bvs->a[bvi];
     const int64_t bi = bv.integer("buffer", -1);
     if (bi < 0 || size_t(bi) >= buffers.size()) return nullptr;
-    const size_t vo = size_t(bv.integer("byteOffset", 0)), vl = size_t(bv.integer("byteLength", 0));
-    if (size_t(offset) + size > vl || vo + vl > buffers[bi].size()) return nullptr;
-    return buffers[bi].data() + vo + size_t(offset);
+    const int64_t vo = bv.integer("byteOffset", 0), vl = bv.integer("byteLength", 0);
+    if (!within(vo, vl, buffers[bi].size()) || !within(offset, int64_t(size), size_t(vl))) return nullptr;
+    return buffers[bi].data() + size_t(vo + offset);
   }
 
   int32_t textureIndex(const Json* info) {
@@ -434,8 +487,8 @@ struct Loader {
     const Json& bv = bvs->a[bvi];
     const int64_t bi = bv.integer("buffer", -1);
     if (bi < 0 || size_t(bi) >= buffers.size()) return fail("bad buffer index");
-    const size_t off = size_t(bv.integer("byteOffset", 0)), len = size_t(bv.integer("byteLength", 0));
-    if (off + len > buffers[bi].size()) return fail("image bufferView exceeds its buffer");
+    const int64_t off = bv.integer("byteOffset", 0), len = bv.integer("byteLength", 0);
+    if (!within(off, len, buffers[bi].size())) return fail("image bufferView exceeds its buffer");
     out.assign(buffers[bi].begin() + off, buffers[bi].begin() + off + len);
     return true;
   }
@@ -511,7 +564,7 @@ struct Loader {
     uint32_t fw = 0, fh = 0;
     for (int i = 0; i < 6; ++i) {
       const Json& e = set->a[i];
-      if (e.kind != Json::Num || e.n < 0 || e.n != static_cast<double>(static_cast<int64_t>(e.n)))
+      if (e.kind != Json::Num || e.n < 0 || e.n != static_cast<double>(e.asInt()))
         return true;  // not an image index: the reference reads no image set
       const size_t index = static_cast<size_t>(e.n);
       if (index >= nimg) return fail("Image based light references an invalid image.");
@@ -692,7 +745,7 @@ struct Loader {
     }
     if (const Json* ch = n.get("children"))
       for (const Json& c : ch->a)
-        if (!walk(static_cast<int64_t>(c.n), world, depth + 1)) return false;
+        if (!walk(c.asInt(), world, depth + 1)) return false;
     return true;
   }
 
@@ -738,7 +791,7 @@ struct Loader {
       if (sc < 0 || size_t(sc) >= scenes->a.size()) sc = 0;
       if (const Json* nodes = scenes->a[sc].get("nodes"))
         for (const Json& n : nodes->a)
-          if (!walk(static_cast<int64_t>(n.n), root, 0)) return false;
+          if (!walk(n.asInt(), root, 0)) return false;
     }
     return true;
   }
@@ -749,85 +802,111 @@ struct Loader {
 
 using namespace cg;
 
-extern "C" CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage) {
-  if (!path || !out || !storage) return fail(CG_E_INVALID, "null argument");
-  *storage = nullptr;
-  auto L = std::make_unique<Loader>();
-  if (!L->load(path)) return fail(CG_E_INVALID, std::string(path) + ": " + L->err);
-  cg_scene_desc d{};
-  d.vertices = L->vertices.data();
-  d.vertex_count = static_cast<uint32_t>(L->vertices.size());
-  d.indices = L->indices.data();
-  d.index_count = static_cast<uint32_t>(L->indices.size());
-  d.meshes = L->meshes.data();
-  d.mesh_count = static_cast<uint32_t>(L->meshes.size());
-  d.instances = L->instances.data();
-  d.instance_count = static_cast<uint32_t>(L->instances.size());
-  d.materials = L->materials.data();
-  d.material_count = static_cast<uint32_t>(L->materials.size());
-  d.textures = L->textures.data();
-  d.texture_count = static_cast<uint32_t>(L->textures.size());
-  if (!L->env.empty()) {
-    d.env_rgba32f = L->env.data();
-    d.env_width = L->env_w;
-    d.env_height = L->env_h;
+namespace {
+// Runs an entry point's body; a C++ exception (an allocation that failed for
+// an absurd size in a damaged file, say) becomes an error status instead of
+// crossing the C ABI.
+template <class Body>
+int guarded(Body&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return cg::fail(CG_E_OOM, "out of host memory");
+  } catch (const std::exception& e) {
+    return cg::fail(CG_E_INVALID, e.what());
   }
-  *out = d;
-  *storage = L.release();
-  return CG_OK;
+}
+}  // namespace
+
+extern "C" CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage) {
+  return guarded([&]() -> int {
+    if (!path || !out || !storage) return fail(CG_E_INVALID, "null argument");
+    *storage = nullptr;
+    auto L = std::make_unique<Loader>();
+    if (!L->load(path)) return fail(CG_E_INVALID, std::string(path) + ": " + L->err);
+    cg_scene_desc d{};
+    d.vertices = L->vertices.data();
+    d.vertex_count = static_cast<uint32_t>(L->vertices.size());
+    d.indices = L->indices.data();
+    d.index_count = static_cast<uint32_t>(L->indices.size());
+    d.meshes = L->meshes.data();
+    d.mesh_count = static_cast<uint32_t>(L->meshes.size());
+    d.instances = L->instances.data();
+    d.instance_count = static_cast<uint32_t>(L->instances.size());
+    d.materials = L->materials.data();
+    d.material_count = static_cast<uint32_t>(L->materials.size());
+    d.textures = L->textures.data();
+    d.texture_count = static_cast<uint32_t>(L->textures.size());
+    if (!L->env.empty()) {
+      d.env_rgba32f = L->env.data();
+      d.env_width = L->env_w;
+      d.env_height = L->env_h;
+    }
+    *out = d;
+    *storage = L.release();
+    return CG_OK;
+  });
 }
 
 extern "C" CG_API int cg_png_decode(const uint8_t* data, size_t size, uint32_t* width,
                                      uint32_t* height, uint8_t* rgba_out) {
-  if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
-  std::vector<uint8_t> rgba;
-  std::string err;
-  uint32_t w = 0, h = 0;
-  if (!decodePng(data, size, w, h, rgba, err)) return fail(CG_E_INVALID, err);
-  *width = w;
-  *height = h;
-  if (rgba_out) std::memcpy(rgba_out, rgba.data(), rgba.size());
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
+    std::vector<uint8_t> rgba;
+    std::string err;
+    uint32_t w = 0, h = 0;
+    if (!decodePng(data, size, w, h, rgba, err)) return fail(CG_E_INVALID, err);
+    *width = w;
+    *height = h;
+    if (rgba_out) std::memcpy(rgba_out, rgba.data(), rgba.size());
+    return CG_OK;
+  });
 }
 
 extern "C" CG_API int cg_jpeg_decode(const uint8_t* data, size_t size, uint32_t* width,
                                     uint32_t* height, uint8_t* rgba_out) {
-  if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
-  std::vector<uint8_t> px;
-  std::string e;
-  uint32_t w = 0, h = 0;
-  if (!decodeJpeg(data, size, w, h, px, e)) return fail(CG_E_INVALID, e);
-  *width = w;
-  *height = h;
-  if (rgba_out) std::memcpy(rgba_out, px.data(), px.size());
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
+    std::vector<uint8_t> px;
+    std::string e;
+    uint32_t w = 0, h = 0;
+    if (!decodeJpeg(data, size, w, h, px, e)) return fail(CG_E_INVALID, e);
+    *width = w;
+    *height = h;
+    if (rgba_out) std::memcpy(rgba_out, px.data(), px.size());
+    return CG_OK;
+  });
 }
 
 extern "C" CG_API int cg_hdr_decode(const uint8_t* data, size_t size, uint32_t* width,
                                    uint32_t* height, float* rgba_out) {
-  if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
-  std::vector<float> px;
-  std::string e;
-  uint32_t w = 0, h = 0;
-  if (!decodeRadianceHdr(data, size, w, h, px, e)) return fail(CG_E_INVALID, e);
-  *width = w;
-  *height = h;
-  if (rgba_out) std::memcpy(rgba_out, px.data(), px.size() * sizeof(float));
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!data || !width || !height) return fail(CG_E_INVALID, "null argument");
+    std::vector<float> px;
+    std::string e;
+    uint32_t w = 0, h = 0;
+    if (!decodeRadianceHdr(data, size, w, h, px, e)) return fail(CG_E_INVALID, e);
+    *width = w;
+    *height = h;
+    if (rgba_out) std::memcpy(rgba_out, px.data(), px.size() * sizeof(float));
+    return CG_OK;
+  });
 }
 
 extern "C" CG_API int cg_env_from_cube(const float* faces, uint32_t face_width,
                                       uint32_t face_height, const float* rotation, float* env_out) {
-  if (!faces || !rotation || !env_out) return fail(CG_E_INVALID, "null argument");
-  if (face_width == 0 || face_height == 0 || face_width > (1u << 14) || face_height > (1u << 14))
-    return fail(CG_E_INVALID, "cube face size must be in [1, 16384]");
-  const size_t face = size_t(face_width) * face_height * 4;
-  const float* fp[6];
-  for (int i = 0; i < 6; ++i) fp[i] = faces + i * face;
-  std::vector<float> out;
-  cubeToLatLong(fp, face_width, face_height, rotation, out);
-  std::memcpy(env_out, out.data(), out.size() * sizeof(float));
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!faces || !rotation || !env_out) return fail(CG_E_INVALID, "null argument");
+    if (face_width == 0 || face_height == 0 || face_width > (1u << 14) || face_height > (1u << 14))
+      return fail(CG_E_INVALID, "cube face size must be in [1, 16384]");
+    const size_t face = size_t(face_width) * face_height * 4;
+    const float* fp[6];
+    for (int i = 0; i < 6; ++i) fp[i] = faces + i * face;
+    std::vector<float> out;
+    cubeToLatLong(fp, face_width, face_height, rotation, out);
+    std::memcpy(env_out, out.data(), out.size() * sizeof(float));
+    return CG_OK;
+  });
 }
 
 extern "C" CG_API int cg_gltf_free(void* storage) {
@@ -836,13 +915,15 @@ extern "C" CG_API int cg_gltf_free(void* storage) {
 }
 
 extern "C" CG_API int cg_scene_load_gltf(const char* path, cg_scene_t* out) {
-  if (!path || !out) return fail(CG_E_INVALID, "null argument");
-  *out = nullptr;
-  cg_scene_desc d{};
-  void* storage = nullptr;
-  int rc = cg_gltf_parse(path, &d, &storage);
-  if (rc != CG_OK) return rc;
-  rc = cg_scene_create(&d, out);
-  cg_gltf_free(storage);
-  return rc;
+  return guarded([&]() -> int {
+    if (!path || !out) return fail(CG_E_INVALID, "null argument");
+    *out = nullptr;
+    cg_scene_desc d{};
+    void* storage = nullptr;
+    int rc = cg_gltf_parse(path, &d, &storage);
+    if (rc != CG_OK) return rc;
+    rc = cg_scene_create(&d, out);
+    cg_gltf_free(storage);
+    return rc;
+  });
 }

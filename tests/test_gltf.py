@@ -171,3 +171,38 @@ def test_normalized_and_sparse_accessors(tmp_path):
     short = [views[0], views[1], dict(views[2], byteLength=8)]
     with pytest.raises(B.Error, match="exceeds its buffer view"):
         _load(tmp_path, _one_triangle_doc(sparse, short, pos + sp_idx + sp_val))
+
+
+def test_damaged_documents_fail_cleanly(tmp_path):
+    """Damage found by fuzzing the loader: each fails the load with an error
+    instead of exhausting the stack, allocating for an absurd count, reading
+    outside a buffer or throwing across the C ABI."""
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32).tobytes()
+    view = [{"buffer": 0, "byteOffset": 16, "byteLength": 36}]
+    dense = {"bufferView": 2, "componentType": 5126, "count": 3, "type": "VEC3"}
+    _load(tmp_path, _one_triangle_doc(dense, view, pos))  # the undamaged document loads
+    cases = [
+        (dict(dense, count=-1), view, "invalid accessor count"),
+        (dict(dense, count=2 ** 31), view, "exceeds its buffer"),
+        ({"componentType": 5126, "count": 2 ** 31, "type": "VEC3"}, view, "too many elements"),
+        (dict(dense, byteOffset=-8), view, "exceeds its buffer"),
+        (dense, [dict(view[0], byteOffset=-16)], "bufferView exceeds its buffer"),
+        (dense, [dict(view[0], byteLength=2 ** 63)], "bufferView exceeds its buffer"),
+        (dense, [dict(view[0], byteLength=24)], "exceeds its buffer"),
+        (dense, [dict(view[0], byteStride=-4)], "invalid byteStride"),
+    ]
+    for acc, views, msg in cases:
+        with pytest.raises(B.Error, match=msg):
+            _load(tmp_path, _one_triangle_doc(acc, views, pos))
+    doc = _one_triangle_doc(dense, view, pos)
+    doc["scenes"][0]["nodes"] = [1e30]
+    with pytest.raises(B.Error, match="bad node index"):
+        _load(tmp_path, doc)
+    p = tmp_path / "deep.gltf"
+    for text in ("[" * 100000 + "]" * 100000, '{"a":' * 50000 + "1" + "}" * 50000):
+        p.write_text(text)
+        with pytest.raises(B.Error, match="nested too deeply"):
+            B.parse_gltf(str(p))
+    p.write_text('{"asset": {"version": "2.0"}, "s": "\\uZZZZ"}')
+    with pytest.raises(B.Error, match="bad unicode escape"):
+        B.parse_gltf(str(p))
