@@ -677,439 +677,489 @@ CG_API const char* cg_version(void) { return "crystalgraphics-b200 0.1 (sm_100a)
 CG_API const char* cg_last_error(void) { return tl_error.c_str(); }
 
 CG_API int cg_init(const cg_conf* conf, int device) {
-  if (!conf) return fail(CG_E_INVALID, "conf is null");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  std::unique_ptr<Env> prev(g_env);
-  g_env = nullptr;
-  std::unique_ptr<Env> env;
-  int rc = createEnv(*conf, device, env, prev.get());
-  prev.reset();
-  if (rc != CG_OK) return rc;
-  g_env = env.release();
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!conf) return fail(CG_E_INVALID, "conf is null");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    std::unique_ptr<Env> prev(g_env);
+    g_env = nullptr;
+    std::unique_ptr<Env> env;
+    int rc = createEnv(*conf, device, env, prev.get());
+    prev.reset();
+    if (rc != CG_OK) return rc;
+    g_env = env.release();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_term(void) {
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  delete g_env;
-  g_env = nullptr;
-  releaseIdleStaging();
-  return CG_OK;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    delete g_env;
+    g_env = nullptr;
+    releaseIdleStaging();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_status(void) {
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  return g_env ? 1 : 0;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    return g_env ? 1 : 0;
+  });
 }
 
 CG_API int cg_get_conf(cg_conf* out) {
-  if (!out) return fail(CG_E_INVALID, "out is null");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  *out = g_env->conf;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!out) return fail(CG_E_INVALID, "out is null");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *out = g_env->conf;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_scene_create(const cg_scene_desc* desc, cg_scene_t* out) {
-  if (!out) return fail(CG_E_INVALID, "out is null");
-  *out = nullptr;
-  auto sd = std::make_unique<SceneDev>();
-  std::string err;
-  int rc = CG_OK;
-  {
-    std::lock_guard<std::mutex> lk(g_env_mu);
-    if (g_env) cudaSetDevice(g_env->device);  // device BVH builds run there too
-  }
-  resetBvhBuildStats();
-  try {
-    rc = packScene(desc, sd->host, err);
-  } catch (const std::exception& e) {
-    return fail(CG_E_CUDA, std::string("scene build: ") + e.what());
-  }
-  if (rc != CG_OK) return fail(rc, err);
-  const BvhBuildStats bstats = bvhBuildStats();
-  if (sd->host.blas_depth + sd->host.tlas_depth + 2 > 64)
-    return fail(CG_E_INVALID, "BVH too deep for the 64-entry traversal stack");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return fail(CG_E_CUDA, "no CUDA device");
-  }
-  {
-    std::lock_guard<std::mutex> lk(g_env_mu);
-    if (g_env) cudaSetDevice(g_env->device);
-  }
-  rc = uploadScene(sd->host, *sd);
-  if (rc != CG_OK) return rc;
-  sd->max_lobes = sd->host.max_lobes;
-  sd->tag = ++g_tag_counter;
-  cg_scene_info& in = sd->info;
-  in.instance_count = static_cast<uint32_t>(sd->host.inst.size());
-  in.mesh_count = sd->host.mesh_count;
-  in.triangle_count = sd->host.triangle_count;
-  in.material_count = static_cast<uint32_t>(sd->host.mat.size());
-  in.emissive_count = static_cast<uint32_t>(sd->host.eprim.size());
-  in.blas_node_count = static_cast<uint32_t>(sd->host.blas.size());
-  in.tlas_node_count = static_cast<uint32_t>(sd->host.tlas.size());
-  in.light_node_count = static_cast<uint32_t>(sd->host.light_bvh.size());
-  in.device_bytes = sd->arena.size;
-  in.tag = sd->tag;
-  in.bvh_build_seconds = bstats.seconds;
-  in.bvh_host_builds = bstats.host_builds;
-  in.bvh_device_builds = bstats.device_builds;
-  // the device holds the geometry now
-  HostScene& h = sd->host;
-  std::vector<BvhNode>().swap(h.blas);
-  std::vector<Bvh4Node>().swap(h.blas4);
-  std::vector<Bvh4QNode>().swap(h.blas4q);
-  std::vector<float>().swap(h.tris);
-  std::vector<uint32_t>().swap(h.tri_vidx);
-  std::vector<float>().swap(h.vnormal);
-  std::vector<uint32_t>().swap(h.tex);
-  std::vector<float>().swap(h.vuv);
-  *out = reinterpret_cast<cg_scene_t>(sd.release());
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!out) return fail(CG_E_INVALID, "out is null");
+    *out = nullptr;
+    auto sd = std::make_unique<SceneDev>();
+    std::string err;
+    int rc = CG_OK;
+    {
+      std::lock_guard<std::mutex> lk(g_env_mu);
+      if (g_env) cudaSetDevice(g_env->device);  // device BVH builds run there too
+    }
+    resetBvhBuildStats();
+    try {
+      rc = packScene(desc, sd->host, err);
+    } catch (const std::exception& e) {
+      return fail(CG_E_CUDA, std::string("scene build: ") + e.what());
+    }
+    if (rc != CG_OK) return fail(rc, err);
+    const BvhBuildStats bstats = bvhBuildStats();
+    if (sd->host.blas_depth + sd->host.tlas_depth + 2 > 64)
+      return fail(CG_E_INVALID, "BVH too deep for the 64-entry traversal stack");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      return fail(CG_E_CUDA, "no CUDA device");
+    }
+    {
+      std::lock_guard<std::mutex> lk(g_env_mu);
+      if (g_env) cudaSetDevice(g_env->device);
+    }
+    rc = uploadScene(sd->host, *sd);
+    if (rc != CG_OK) return rc;
+    sd->max_lobes = sd->host.max_lobes;
+    sd->tag = ++g_tag_counter;
+    cg_scene_info& in = sd->info;
+    in.instance_count = static_cast<uint32_t>(sd->host.inst.size());
+    in.mesh_count = sd->host.mesh_count;
+    in.triangle_count = sd->host.triangle_count;
+    in.material_count = static_cast<uint32_t>(sd->host.mat.size());
+    in.emissive_count = static_cast<uint32_t>(sd->host.eprim.size());
+    in.blas_node_count = static_cast<uint32_t>(sd->host.blas.size());
+    in.tlas_node_count = static_cast<uint32_t>(sd->host.tlas.size());
+    in.light_node_count = static_cast<uint32_t>(sd->host.light_bvh.size());
+    in.device_bytes = sd->arena.size;
+    in.tag = sd->tag;
+    in.bvh_build_seconds = bstats.seconds;
+    in.bvh_host_builds = bstats.host_builds;
+    in.bvh_device_builds = bstats.device_builds;
+    // the device holds the geometry now
+    HostScene& h = sd->host;
+    std::vector<BvhNode>().swap(h.blas);
+    std::vector<Bvh4Node>().swap(h.blas4);
+    std::vector<Bvh4QNode>().swap(h.blas4q);
+    std::vector<float>().swap(h.tris);
+    std::vector<uint32_t>().swap(h.tri_vidx);
+    std::vector<float>().swap(h.vnormal);
+    std::vector<uint32_t>().swap(h.tex);
+    std::vector<float>().swap(h.vuv);
+    *out = reinterpret_cast<cg_scene_t>(sd.release());
+    return CG_OK;
+  });
 }
 
 CG_API int cg_bvh_build(const float* boxes, uint32_t count, int mode, void* nodes_out,
                         uint32_t node_capacity, uint32_t* node_count, uint32_t* order_out) {
-  if (!boxes || !node_count || (count && !order_out))
-    return fail(CG_E_INVALID, "null argument");
-  if (mode != kBuildHost && mode != kBuildDevice) return fail(CG_E_INVALID, "mode must be host or device");
-  std::vector<Box> bx(count);
-  std::memcpy(bx.data(), boxes, sizeof(Box) * size_t(count));
-  std::vector<BvhNode> nodes;
-  std::vector<uint32_t> order;
-  const int saved = bvhBuildMode();
-  setBvhBuildMode(mode);
-  try {
-    BvhBuildOptions opt;
-    buildBvh(bx, opt, 0, nodes, order);
-  } catch (const std::exception& e) {
+  return guarded([&]() -> int {
+    if (!boxes || !node_count || (count && !order_out))
+      return fail(CG_E_INVALID, "null argument");
+    if (mode != kBuildHost && mode != kBuildDevice) return fail(CG_E_INVALID, "mode must be host or device");
+    std::vector<Box> bx(count);
+    std::memcpy(bx.data(), boxes, sizeof(Box) * size_t(count));
+    std::vector<BvhNode> nodes;
+    std::vector<uint32_t> order;
+    const int saved = bvhBuildMode();
+    setBvhBuildMode(mode);
+    try {
+      BvhBuildOptions opt;
+      buildBvh(bx, opt, 0, nodes, order);
+    } catch (const std::exception& e) {
+      setBvhBuildMode(saved);
+      return fail(CG_E_CUDA, std::string("bvh build: ") + e.what());
+    }
     setBvhBuildMode(saved);
-    return fail(CG_E_CUDA, std::string("bvh build: ") + e.what());
-  }
-  setBvhBuildMode(saved);
-  *node_count = static_cast<uint32_t>(nodes.size());
-  if (nodes_out && node_capacity >= nodes.size())
-    std::memcpy(nodes_out, nodes.data(), sizeof(BvhNode) * nodes.size());
-  if (count) std::memcpy(order_out, order.data(), 4 * size_t(count));
-  return CG_OK;
+    *node_count = static_cast<uint32_t>(nodes.size());
+    if (nodes_out && node_capacity >= nodes.size())
+      std::memcpy(nodes_out, nodes.data(), sizeof(BvhNode) * nodes.size());
+    if (count) std::memcpy(order_out, order.data(), 4 * size_t(count));
+    return CG_OK;
+  });
 }
 
 CG_API int cg_set_bvh_build(int mode) {
-  if (mode < kBuildAuto || mode > kBuildDevice) return fail(CG_E_INVALID, "unknown BVH build mode");
-  setBvhBuildMode(mode);
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (mode < kBuildAuto || mode > kBuildDevice) return fail(CG_E_INVALID, "unknown BVH build mode");
+    setBvhBuildMode(mode);
+    return CG_OK;
+  });
 }
 
 CG_API int cg_scene_destroy(cg_scene_t scene) {
-  if (!scene) return CG_OK;
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  {
-    std::lock_guard<std::mutex> lk(g_env_mu);
-    if (g_env) {
-      cudaStreamSynchronize(g_env->stream);
-      g_env->dropGraphsFor(s->tag);
+  return guarded([&]() -> int {
+    if (!scene) return CG_OK;
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    {
+      std::lock_guard<std::mutex> lk(g_env_mu);
+      if (g_env) {
+        cudaStreamSynchronize(g_env->stream);
+        g_env->dropGraphsFor(s->tag);
+      }
     }
-  }
-  delete s;
-  return CG_OK;
+    delete s;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_scene_get_info(cg_scene_t scene, cg_scene_info* out) {
-  if (!scene || !out) return fail(CG_E_INVALID, "null argument");
-  *out = reinterpret_cast<SceneDev*>(scene)->info;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!scene || !out) return fail(CG_E_INVALID, "null argument");
+    *out = reinterpret_cast<SceneDev*>(scene)->info;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_scene_read_emissive(cg_scene_t scene, cg_emissive_prim* prims, cg_alias_entry* alias,
                                   uint32_t capacity, uint32_t* count) {
-  if (!scene) return fail(CG_E_INVALID, "scene is null");
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  const uint32_t n = s->info.emissive_count;
-  if (count) *count = n;
-  if (n == 0 || (!prims && !alias)) return CG_OK;  // count query
-  if (capacity < n) return fail(CG_E_INVALID, "capacity below the emissive count");
-  const char* base = static_cast<const char*>(s->arena.base);
-  if (prims)
-    CG_CUDA(cudaMemcpy(prims, base + s->eprim_off, n * sizeof(cg_emissive_prim),
-                       cudaMemcpyDeviceToHost));
-  if (alias)
-    CG_CUDA(cudaMemcpy(alias, base + s->alias_off, n * sizeof(cg_alias_entry),
-                       cudaMemcpyDeviceToHost));
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!scene) return fail(CG_E_INVALID, "scene is null");
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    const uint32_t n = s->info.emissive_count;
+    if (count) *count = n;
+    if (n == 0 || (!prims && !alias)) return CG_OK;  // count query
+    if (capacity < n) return fail(CG_E_INVALID, "capacity below the emissive count");
+    const char* base = static_cast<const char*>(s->arena.base);
+    if (prims)
+      CG_CUDA(cudaMemcpy(prims, base + s->eprim_off, n * sizeof(cg_emissive_prim),
+                         cudaMemcpyDeviceToHost));
+    if (alias)
+      CG_CUDA(cudaMemcpy(alias, base + s->alias_off, n * sizeof(cg_alias_entry),
+                         cudaMemcpyDeviceToHost));
+    return CG_OK;
+  });
 }
 
 CG_API int cg_alias_build(const double* weights, uint32_t count, cg_alias_entry* out) {
-  if (count && (!weights || !out)) return fail(CG_E_INVALID, "null argument");
-  buildAliasTable(weights, count, out);
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (count && (!weights || !out)) return fail(CG_E_INVALID, "null argument");
+    buildAliasTable(weights, count, out);
+    return CG_OK;
+  });
 }
 
 CG_API int cg_view(cg_scene_t scene, const cg_camera* camera) {
-  if (!scene || !camera) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  Env& env = *g_env;
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  CG_CUDA(cudaSetDevice(env.device));
-  // FrameHistory::NextIteration (src/wgpu/frame_history.h:12-23)
-  const bool same = env.has_prev && env.prev_tag == s->tag &&
-                    camera->position[0] == env.prev_cam.position[0] &&
-                    camera->position[1] == env.prev_cam.position[1] &&
-                    camera->position[2] == env.prev_cam.position[2] &&
-                    camera->direction[0] == env.prev_cam.direction[0] &&
-                    camera->direction[1] == env.prev_cam.direction[1] &&
-                    camera->direction[2] == env.prev_cam.direction[2] &&
-                    camera->viewport[0] == env.prev_cam.viewport[0] &&
-                    camera->viewport[1] == env.prev_cam.viewport[1];
-  uint32_t iter;
-  if (!same) {
-    env.has_prev = true;
-    env.prev_tag = s->tag;
-    env.prev_cam = *camera;
-    env.frame_count = 1;
-    iter = 0;
-  } else {
-    iter = env.frame_count++;
-  }
-  std::vector<ViewDev> views(1);
-  ViewDev& v = views[0];
-  std::memset(&v, 0, sizeof(v));
-  cameraBasis(*camera, v);
-  v.width = env.conf.render_width;
-  v.height = env.conf.render_height;
-  v.spp = env.conf.sample_count;
-  v.seed = env.seed;
-  v.frame = iter;
-  v.sample_weight = 1.0f / static_cast<float>(iter + 1u);
-  v.pixel_base = 0;
-  v.pixel_count = v.width * v.height;
-  v.film = static_cast<float4*>(env.film);
-  v.rgba = static_cast<uchar4*>(env.rgba);
-  return renderEnvView(env, s, views, true);
+  return guarded([&]() -> int {
+    if (!scene || !camera) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    CG_CUDA(cudaSetDevice(env.device));
+    // FrameHistory::NextIteration (src/wgpu/frame_history.h:12-23)
+    const bool same = env.has_prev && env.prev_tag == s->tag &&
+                      camera->position[0] == env.prev_cam.position[0] &&
+                      camera->position[1] == env.prev_cam.position[1] &&
+                      camera->position[2] == env.prev_cam.position[2] &&
+                      camera->direction[0] == env.prev_cam.direction[0] &&
+                      camera->direction[1] == env.prev_cam.direction[1] &&
+                      camera->direction[2] == env.prev_cam.direction[2] &&
+                      camera->viewport[0] == env.prev_cam.viewport[0] &&
+                      camera->viewport[1] == env.prev_cam.viewport[1];
+    uint32_t iter;
+    if (!same) {
+      env.has_prev = true;
+      env.prev_tag = s->tag;
+      env.prev_cam = *camera;
+      env.frame_count = 1;
+      iter = 0;
+    } else {
+      iter = env.frame_count++;
+    }
+    std::vector<ViewDev> views(1);
+    ViewDev& v = views[0];
+    std::memset(&v, 0, sizeof(v));
+    cameraBasis(*camera, v);
+    v.width = env.conf.render_width;
+    v.height = env.conf.render_height;
+    v.spp = env.conf.sample_count;
+    v.seed = env.seed;
+    v.frame = iter;
+    v.sample_weight = 1.0f / static_cast<float>(iter + 1u);
+    v.pixel_base = 0;
+    v.pixel_count = v.width * v.height;
+    v.film = static_cast<float4*>(env.film);
+    v.rgba = static_cast<uchar4*>(env.rgba);
+    return renderEnvView(env, s, views, true);
+  });
 }
 
 CG_API int cg_view_samples(cg_scene_t scene, const cg_camera* camera, uint32_t sample_begin,
                            uint32_t sample_count) {
-  if (!scene || !camera) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  Env& env = *g_env;
-  if (sample_begin > env.conf.sample_count ||
-      sample_count > env.conf.sample_count - sample_begin)
-    return fail(CG_E_INVALID, "sample range beyond the conf's sample_count");
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  CG_CUDA(cudaSetDevice(env.device));
-  env.has_prev = false;  // a share of a frame: the next View() starts a fresh mean
-  const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
-  if (sample_count == 0) {  // this share holds no samples
-    CG_CUDA(cudaMemsetAsync(env.film, 0, npx * sizeof(float4), env.stream));
-    launchFilmRgba8(static_cast<const float4*>(env.film), static_cast<uchar4*>(env.rgba), npx,
-                    env.stream);
-    CG_CUDA(cudaGetLastError());
-    CG_CUDA(cudaStreamSynchronize(env.stream));
-    env.last = cg_stats{};
-    return CG_OK;
-  }
-  std::vector<ViewDev> views(1);
-  ViewDev& v = views[0];
-  std::memset(&v, 0, sizeof(v));
-  cameraBasis(*camera, v);
-  v.width = env.conf.render_width;
-  v.height = env.conf.render_height;
-  v.spp = sample_count;
-  v.sample_base = sample_begin;
-  v.spp_total = env.conf.sample_count;
-  v.seed = env.seed;
-  v.frame = 0;
-  v.sample_weight = 1.0f;
-  v.pixel_base = 0;
-  v.pixel_count = v.width * v.height;
-  v.film = static_cast<float4*>(env.film);
-  v.rgba = static_cast<uchar4*>(env.rgba);
-  // the chunking depends on the range, so the captured View() sequence does not apply
-  return renderEnvView(env, s, views, false);
+  return guarded([&]() -> int {
+    if (!scene || !camera) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    if (sample_begin > env.conf.sample_count ||
+        sample_count > env.conf.sample_count - sample_begin)
+      return fail(CG_E_INVALID, "sample range beyond the conf's sample_count");
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    CG_CUDA(cudaSetDevice(env.device));
+    env.has_prev = false;  // a share of a frame: the next View() starts a fresh mean
+    const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
+    if (sample_count == 0) {  // this share holds no samples
+      CG_CUDA(cudaMemsetAsync(env.film, 0, npx * sizeof(float4), env.stream));
+      launchFilmRgba8(static_cast<const float4*>(env.film), static_cast<uchar4*>(env.rgba), npx,
+                      env.stream);
+      CG_CUDA(cudaGetLastError());
+      CG_CUDA(cudaStreamSynchronize(env.stream));
+      env.last = cg_stats{};
+      return CG_OK;
+    }
+    std::vector<ViewDev> views(1);
+    ViewDev& v = views[0];
+    std::memset(&v, 0, sizeof(v));
+    cameraBasis(*camera, v);
+    v.width = env.conf.render_width;
+    v.height = env.conf.render_height;
+    v.spp = sample_count;
+    v.sample_base = sample_begin;
+    v.spp_total = env.conf.sample_count;
+    v.seed = env.seed;
+    v.frame = 0;
+    v.sample_weight = 1.0f;
+    v.pixel_base = 0;
+    v.pixel_count = v.width * v.height;
+    v.film = static_cast<float4*>(env.film);
+    v.rgba = static_cast<uchar4*>(env.rgba);
+    // the chunking depends on the range, so the captured View() sequence does not apply
+    return renderEnvView(env, s, views, false);
+  });
 }
 
 CG_API int cg_film_device(void** film_xyzw, size_t* bytes) {
-  if (!film_xyzw || !bytes) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  *film_xyzw = g_env->film;
-  *bytes = size_t(g_env->conf.render_width) * g_env->conf.render_height * sizeof(float4);
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!film_xyzw || !bytes) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *film_xyzw = g_env->film;
+    *bytes = size_t(g_env->conf.render_width) * g_env->conf.render_height * sizeof(float4);
+    return CG_OK;
+  });
 }
 
 CG_API int cg_film_update_rgba8(void) {
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  Env& env = *g_env;
-  CG_CUDA(cudaSetDevice(env.device));
-  launchFilmRgba8(static_cast<const float4*>(env.film), static_cast<uchar4*>(env.rgba),
-                  size_t(env.conf.render_width) * env.conf.render_height, env.stream);
-  CG_CUDA(cudaGetLastError());
-  CG_CUDA(cudaStreamSynchronize(env.stream));
-  return CG_OK;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    CG_CUDA(cudaSetDevice(env.device));
+    launchFilmRgba8(static_cast<const float4*>(env.film), static_cast<uchar4*>(env.rgba),
+                    size_t(env.conf.render_width) * env.conf.render_height, env.stream);
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaStreamSynchronize(env.stream));
+    return CG_OK;
+  });
 }
 
 CG_API int cg_film_read(void* host, size_t bytes, int format) {
-  if (!host) return fail(CG_E_INVALID, "host is null");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  Env& env = *g_env;
-  const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
-  CG_CUDA(cudaSetDevice(env.device));
-  prefaultHostBuffer(host, std::min(bytes, npx * (format == CG_FILM_RGBA8 ? 4 : 12)));
-  if (format == CG_FILM_RGBA8) {
-    if (bytes < npx * 4) return fail(CG_E_INVALID, "buffer too small for RGBA8");
-    CG_CUDA(cudaMemcpyAsync(host, env.rgba, npx * 4, cudaMemcpyDeviceToHost, env.stream));
+  return guarded([&]() -> int {
+    if (!host) return fail(CG_E_INVALID, "host is null");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    const size_t npx = size_t(env.conf.render_width) * env.conf.render_height;
+    CG_CUDA(cudaSetDevice(env.device));
+    prefaultHostBuffer(host, std::min(bytes, npx * (format == CG_FILM_RGBA8 ? 4 : 12)));
+    if (format == CG_FILM_RGBA8) {
+      if (bytes < npx * 4) return fail(CG_E_INVALID, "buffer too small for RGBA8");
+      CG_CUDA(cudaMemcpyAsync(host, env.rgba, npx * 4, cudaMemcpyDeviceToHost, env.stream));
+      CG_CUDA(cudaStreamSynchronize(env.stream));
+      return CG_OK;
+    }
+    if (format != CG_FILM_XYZ32F && format != CG_FILM_RGB32F)
+      return fail(CG_E_INVALID, "unknown film format");
+    if (bytes < npx * 12) return fail(CG_E_INVALID, "buffer too small for 3 floats per pixel");
+    // packed (and for RGB converted) on the device, then one contiguous copy
+    // (a direct DMA when `host` is pinned)
+    launchFilmPack(static_cast<const float4*>(env.film), env.film_pack, npx,
+                   format == CG_FILM_RGB32F, env.stream);
+    CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaMemcpyAsync(host, env.film_pack, npx * 12, cudaMemcpyDeviceToHost, env.stream));
     CG_CUDA(cudaStreamSynchronize(env.stream));
     return CG_OK;
-  }
-  if (format != CG_FILM_XYZ32F && format != CG_FILM_RGB32F)
-    return fail(CG_E_INVALID, "unknown film format");
-  if (bytes < npx * 12) return fail(CG_E_INVALID, "buffer too small for 3 floats per pixel");
-  // packed (and for RGB converted) on the device, then one contiguous copy
-  // (a direct DMA when `host` is pinned)
-  launchFilmPack(static_cast<const float4*>(env.film), env.film_pack, npx,
-                 format == CG_FILM_RGB32F, env.stream);
-  CG_CUDA(cudaGetLastError());
-  CG_CUDA(cudaMemcpyAsync(host, env.film_pack, npx * 12, cudaMemcpyDeviceToHost, env.stream));
-  CG_CUDA(cudaStreamSynchronize(env.stream));
-  return CG_OK;
+  });
 }
 
 CG_API int cg_film_frames(uint32_t* frames) {
-  if (!frames) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  *frames = g_env->has_prev ? g_env->frame_count : 0u;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!frames) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *frames = g_env->has_prev ? g_env->frame_count : 0u;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_last_stats(cg_stats* out) {
-  if (!out) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  *out = g_env->last;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!out) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *out = g_env->last;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_set_counting(int enable) {
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  g_env->counting = enable != 0;
-  g_env->dropAllGraphs();
-  return CG_OK;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    g_env->counting = enable != 0;
+    g_env->dropAllGraphs();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_set_profiling(int enable) {
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  g_env->profiling = enable != 0;
-  g_env->prof = cg_profile{};
-  return CG_OK;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    g_env->profiling = enable != 0;
+    g_env->prof = cg_profile{};
+    return CG_OK;
+  });
 }
 
 CG_API int cg_profile_read(cg_profile* out) {
-  if (!out) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  *out = g_env->prof;
-  g_env->prof = cg_profile{};
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!out) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *out = g_env->prof;
+    g_env->prof = cg_profile{};
+    return CG_OK;
+  });
 }
 
 CG_API int cg_set_seed(uint32_t seed) {
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  g_env->seed = seed;
-  return CG_OK;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    g_env->seed = seed;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_set_tuning(const cg_tuning* t) {
-  if (!t) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  // every field is checked before any is applied
-  auto okBlock = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 1024 && b % 32 == 0); };
-  if (!okBlock(t->extend_block) || !okBlock(t->shade_block))
-    return fail(CG_E_INVALID, "block sizes must be multiples of 32 in [32, 1024]");
-  if (t->extend_block > 256u)  // the traversal kernels' launch bounds
-    return fail(CG_E_INVALID, "extend_block must be at most 256");
-  if (t->queue_capacity && (t->queue_capacity < 4096 || t->queue_capacity > (1u << 28)))
-    return fail(CG_E_INVALID, "queue capacity must be in [4096, 2^28]");
-  if (t->bvh_width && t->bvh_width != 2 && t->bvh_width != 4)
-    return fail(CG_E_INVALID, "bvh_width must be 2 or 4");
-  if (t->box_bits && t->box_bits != 8 && t->box_bits != 32)
-    return fail(CG_E_INVALID, "box_bits must be 8 or 32");
-  if (t->pipelines > static_cast<uint32_t>(Renderer::kMaxPipelines))
-    return fail(CG_E_INVALID, "pipelines must be 1 to 4");
-  if (t->shade_sort > 3u) return fail(CG_E_INVALID, "shade_sort must be 0..3");
-  cg_tuning& g = g_env->tuning;
-  if (t->queue_capacity) g.queue_capacity = t->queue_capacity;
-  if (t->box_bits) g.box_bits = t->box_bits;
-  if (t->pipelines) g.pipelines = t->pipelines;
-  if (t->extend_block) g.extend_block = t->extend_block;
-  if (t->shade_block) g.shade_block = t->shade_block;
-  if (t->bvh_width) g.bvh_width = t->bvh_width;
-  if (t->persistent) g.persistent = t->persistent == 2u ? 2u : 1u;
-  if (t->shade_sort) g.shade_sort = t->shade_sort;
-  g_env->tuning.use_graph = t->use_graph;
-  g_env->dropAllGraphs();
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!t) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    // every field is checked before any is applied
+    auto okBlock = [](uint32_t b) { return b == 0 || (b >= 32 && b <= 1024 && b % 32 == 0); };
+    if (!okBlock(t->extend_block) || !okBlock(t->shade_block))
+      return fail(CG_E_INVALID, "block sizes must be multiples of 32 in [32, 1024]");
+    if (t->extend_block > 256u)  // the traversal kernels' launch bounds
+      return fail(CG_E_INVALID, "extend_block must be at most 256");
+    if (t->queue_capacity && (t->queue_capacity < 4096 || t->queue_capacity > (1u << 28)))
+      return fail(CG_E_INVALID, "queue capacity must be in [4096, 2^28]");
+    if (t->bvh_width && t->bvh_width != 2 && t->bvh_width != 4)
+      return fail(CG_E_INVALID, "bvh_width must be 2 or 4");
+    if (t->box_bits && t->box_bits != 8 && t->box_bits != 32)
+      return fail(CG_E_INVALID, "box_bits must be 8 or 32");
+    if (t->pipelines > static_cast<uint32_t>(Renderer::kMaxPipelines))
+      return fail(CG_E_INVALID, "pipelines must be 1 to 4");
+    if (t->shade_sort > 3u) return fail(CG_E_INVALID, "shade_sort must be 0..3");
+    cg_tuning& g = g_env->tuning;
+    if (t->queue_capacity) g.queue_capacity = t->queue_capacity;
+    if (t->box_bits) g.box_bits = t->box_bits;
+    if (t->pipelines) g.pipelines = t->pipelines;
+    if (t->extend_block) g.extend_block = t->extend_block;
+    if (t->shade_block) g.shade_block = t->shade_block;
+    if (t->bvh_width) g.bvh_width = t->bvh_width;
+    if (t->persistent) g.persistent = t->persistent == 2u ? 2u : 1u;
+    if (t->shade_sort) g.shade_sort = t->shade_sort;
+    g_env->tuning.use_graph = t->use_graph;
+    g_env->dropAllGraphs();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_get_tuning(cg_tuning* out) {
-  if (!out) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  *out = g_env->tuning;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!out) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *out = g_env->tuning;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_trace_closest(cg_scene_t scene, const float* rays, uint32_t n, cg_hit* hits) {
-  if (!scene || (n && (!rays || !hits))) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  if (n == 0) return CG_OK;
-  Env& env = *g_env;
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  CG_CUDA(cudaSetDevice(env.device));
-  DeviceArena a;
-  const size_t rb = size_t(n) * 32, ob = size_t(n) * 16;
-  int rc = a.alloc(align256(rb) + 2 * align256(ob) + 256);
-  if (rc != CG_OK) return rc;
-  char* p = static_cast<char*>(a.base);
-  float4* d_rays = reinterpret_cast<float4*>(p);
-  float4* d_tuv = reinterpret_cast<float4*>(p + align256(rb));
-  int4* d_ids = reinterpret_cast<int4*>(p + align256(rb) + align256(ob));
-  uint32_t* d_status = reinterpret_cast<uint32_t*>(p + align256(rb) + 2 * align256(ob));
-  CG_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, env.stream));
-  CG_CUDA(cudaMemsetAsync(d_status, 0, 4, env.stream));
-  launchTraceClosest(s->view, d_rays, n, d_tuv, d_ids, d_status, nodeFormatOf(env.tuning),
-                     env.stream);
-  CG_CUDA(cudaGetLastError());
-  std::vector<float4> tuv(n);
-  std::vector<int4> ids(n);
-  uint32_t status = 0;
-  CG_CUDA(cudaMemcpyAsync(tuv.data(), d_tuv, ob, cudaMemcpyDeviceToHost, env.stream));
-  CG_CUDA(cudaMemcpyAsync(ids.data(), d_ids, ob, cudaMemcpyDeviceToHost, env.stream));
-  CG_CUDA(cudaMemcpyAsync(&status, d_status, 4, cudaMemcpyDeviceToHost, env.stream));
-  CG_CUDA(cudaStreamSynchronize(env.stream));
-  if (status) return fail(CG_E_DEVICE, "traversal stack overflow in k_trace_closest");
-  for (uint32_t i = 0; i < n; ++i) {
-    cg_hit h{};
-    h.t = tuv[i].x;
-    h.u = tuv[i].y;
-    h.v = tuv[i].z;
-    h.instance = ids[i].x;
-    h.triangle = ids[i].y;
-    hits[i] = h;
-  }
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!scene || (n && (!rays || !hits))) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    if (n == 0) return CG_OK;
+    Env& env = *g_env;
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    CG_CUDA(cudaSetDevice(env.device));
+    DeviceArena a;
+    const size_t rb = size_t(n) * 32, ob = size_t(n) * 16;
+    int rc = a.alloc(align256(rb) + 2 * align256(ob) + 256);
+    if (rc != CG_OK) return rc;
+    char* p = static_cast<char*>(a.base);
+    float4* d_rays = reinterpret_cast<float4*>(p);
+    float4* d_tuv = reinterpret_cast<float4*>(p + align256(rb));
+    int4* d_ids = reinterpret_cast<int4*>(p + align256(rb) + align256(ob));
+    uint32_t* d_status = reinterpret_cast<uint32_t*>(p + align256(rb) + 2 * align256(ob));
+    CG_CUDA(cudaMemcpyAsync(d_rays, rays, rb, cudaMemcpyHostToDevice, env.stream));
+    CG_CUDA(cudaMemsetAsync(d_status, 0, 4, env.stream));
+    launchTraceClosest(s->view, d_rays, n, d_tuv, d_ids, d_status, nodeFormatOf(env.tuning),
+                       env.stream);
+    CG_CUDA(cudaGetLastError());
+    std::vector<float4> tuv(n);
+    std::vector<int4> ids(n);
+    uint32_t status = 0;
+    CG_CUDA(cudaMemcpyAsync(tuv.data(), d_tuv, ob, cudaMemcpyDeviceToHost, env.stream));
+    CG_CUDA(cudaMemcpyAsync(ids.data(), d_ids, ob, cudaMemcpyDeviceToHost, env.stream));
+    CG_CUDA(cudaMemcpyAsync(&status, d_status, 4, cudaMemcpyDeviceToHost, env.stream));
+    CG_CUDA(cudaStreamSynchronize(env.stream));
+    if (status) return fail(CG_E_DEVICE, "traversal stack overflow in k_trace_closest");
+    for (uint32_t i = 0; i < n; ++i) {
+      cg_hit h{};
+      h.t = tuv[i].x;
+      h.u = tuv[i].y;
+      h.v = tuv[i].z;
+      h.instance = ids[i].x;
+      h.triangle = ids[i].y;
+      hits[i] = h;
+    }
+    return CG_OK;
+  });
 }
 
 }  // extern "C"

@@ -8,6 +8,8 @@
 #include <cstdint>
 #include <memory>
 #include <mutex>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -19,6 +21,20 @@ namespace cg {
 
 extern thread_local std::string tl_error;
 int fail(int code, const std::string& msg);
+
+// Runs the body of a C-ABI entry point: a C++ exception (a host allocation
+// that failed, a thread that could not start) becomes an error status instead
+// of crossing the ABI.
+template <class Body>
+int guarded(Body&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return fail(CG_E_OOM, "out of host memory");
+  } catch (const std::exception& e) {
+    return fail(CG_E_INVALID, e.what());
+  }
+}
 int cudaFail(cudaError_t e, const char* what);
 
 #define CG_CUDA(call)                                  \

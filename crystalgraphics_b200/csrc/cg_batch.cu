@@ -160,158 +160,164 @@ extern "C" {
 
 CG_API int cg_batch_render(cg_scene_t scene, const cg_view_desc* views, uint32_t view_count,
                            float* films_xyz, uint8_t* films_rgba8) {
-  if (!scene || (view_count && !views)) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  if (view_count == 0) return CG_OK;
-  Env& env = *g_env;
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  CG_CUDA(cudaSetDevice(env.device));
-  int rc = env.ensureWave(env.tuning.queue_capacity);
-  if (rc != CG_OK) return rc;
-  rc = env.beginStats(env.stream);
-  if (rc != CG_OK) return rc;
-  BatchGraph* g = nullptr;
-  RenderRecord rec;
-  float ms = 0.0f;
-  rc = runBatch(env, *s, views, view_count, g, rec, ms);
-  if (rc != CG_OK) return rc;
-  rc = env.endStats(env.stream, rec, ms);
-  if (rc != CG_OK) return rc;
-  // readback
-  const char* base = static_cast<const char*>(g->films.base);
-  if (films_xyz) {
-    size_t total = 0;
-    for (uint32_t i = 0; i < view_count; ++i) total += size_t(views[i].width) * views[i].height;
-    std::vector<float> tmp;
-    size_t out = 0;
-    for (uint32_t i = 0; i < view_count; ++i) {
-      const size_t npx = size_t(views[i].width) * views[i].height;
-      tmp.resize(npx * 4);
-      CG_CUDA(cudaMemcpyAsync(tmp.data(), base + g->film_off[i], npx * 16, cudaMemcpyDeviceToHost,
-                              env.stream));
-      CG_CUDA(cudaStreamSynchronize(env.stream));
-      for (size_t p = 0; p < npx; ++p) {
-        films_xyz[3 * (out + p)] = tmp[4 * p];
-        films_xyz[3 * (out + p) + 1] = tmp[4 * p + 1];
-        films_xyz[3 * (out + p) + 2] = tmp[4 * p + 2];
+  return guarded([&]() -> int {
+    if (!scene || (view_count && !views)) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    if (view_count == 0) return CG_OK;
+    Env& env = *g_env;
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    CG_CUDA(cudaSetDevice(env.device));
+    int rc = env.ensureWave(env.tuning.queue_capacity);
+    if (rc != CG_OK) return rc;
+    rc = env.beginStats(env.stream);
+    if (rc != CG_OK) return rc;
+    BatchGraph* g = nullptr;
+    RenderRecord rec;
+    float ms = 0.0f;
+    rc = runBatch(env, *s, views, view_count, g, rec, ms);
+    if (rc != CG_OK) return rc;
+    rc = env.endStats(env.stream, rec, ms);
+    if (rc != CG_OK) return rc;
+    // readback
+    const char* base = static_cast<const char*>(g->films.base);
+    if (films_xyz) {
+      size_t total = 0;
+      for (uint32_t i = 0; i < view_count; ++i) total += size_t(views[i].width) * views[i].height;
+      std::vector<float> tmp;
+      size_t out = 0;
+      for (uint32_t i = 0; i < view_count; ++i) {
+        const size_t npx = size_t(views[i].width) * views[i].height;
+        tmp.resize(npx * 4);
+        CG_CUDA(cudaMemcpyAsync(tmp.data(), base + g->film_off[i], npx * 16, cudaMemcpyDeviceToHost,
+                                env.stream));
+        CG_CUDA(cudaStreamSynchronize(env.stream));
+        for (size_t p = 0; p < npx; ++p) {
+          films_xyz[3 * (out + p)] = tmp[4 * p];
+          films_xyz[3 * (out + p) + 1] = tmp[4 * p + 1];
+          films_xyz[3 * (out + p) + 2] = tmp[4 * p + 2];
+        }
+        out += npx;
       }
-      out += npx;
+      (void)total;
     }
-    (void)total;
-  }
-  if (films_rgba8) {
-    size_t out = 0;
-    for (uint32_t i = 0; i < view_count; ++i) {
-      const size_t npx = size_t(views[i].width) * views[i].height;
-      CG_CUDA(cudaMemcpyAsync(films_rgba8 + out, base + g->rgba_off[i], npx * 4,
-                              cudaMemcpyDeviceToHost, env.stream));
-      out += npx * 4;
+    if (films_rgba8) {
+      size_t out = 0;
+      for (uint32_t i = 0; i < view_count; ++i) {
+        const size_t npx = size_t(views[i].width) * views[i].height;
+        CG_CUDA(cudaMemcpyAsync(films_rgba8 + out, base + g->rgba_off[i], npx * 4,
+                                cudaMemcpyDeviceToHost, env.stream));
+        out += npx * 4;
+      }
+      CG_CUDA(cudaStreamSynchronize(env.stream));
     }
-    CG_CUDA(cudaStreamSynchronize(env.stream));
-  }
-  return CG_OK;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32_t count,
                              cg_tuning* best) {
-  if (!scene || !views || count == 0) return fail(CG_E_INVALID, "null argument or no views");
-  std::lock_guard<std::mutex> lk(g_env_mu);
-  if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-  Env& env = *g_env;
-  SceneDev* s = reinterpret_cast<SceneDev*>(scene);
-  CG_CUDA(cudaSetDevice(env.device));
-  const cg_tuning saved = env.tuning;
-  // Time of the probe views under tuning t: one untimed run, then two timed
-  // (un-captured, so every launch shape change takes effect); +inf if a run fails.
-  auto measure = [&](const cg_tuning& t) {
-    env.tuning = t;
-    env.tuning.use_graph = 0;
+  return guarded([&]() -> int {
+    if (!scene || !views || count == 0) return fail(CG_E_INVALID, "null argument or no views");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    SceneDev* s = reinterpret_cast<SceneDev*>(scene);
+    CG_CUDA(cudaSetDevice(env.device));
+    const cg_tuning saved = env.tuning;
+    // Time of the probe views under tuning t: one untimed run, then two timed
+    // (un-captured, so every launch shape change takes effect); +inf if a run fails.
+    auto measure = [&](const cg_tuning& t) {
+      env.tuning = t;
+      env.tuning.use_graph = 0;
+      env.dropAllGraphs();
+      float total = 0.0f;
+      for (int rep = 0; rep < 3; ++rep) {
+        BatchGraph* g = nullptr;
+        RenderRecord rec;
+        float ms = 0.0f;
+        if (runBatch(env, *s, views, count, g, rec, ms) != CG_OK) return 1e30f;
+        if (rep > 0) total += ms;
+      }
+      return total;
+    };
+    // Coordinate descent from the current tuning: kernel variant, then queue
+    // capacity, then the traversal and shading block sizes.
+    cg_tuning winner = saved;
+    float best_ms = measure(winner);
+    auto consider = [&](cg_tuning t) {
+      const float ms = measure(t);
+      if (ms < best_ms) {
+        best_ms = ms;
+        winner = t;
+      }
+    };
+    // kernel variants: (node width, persistent lane refill 1 on / 2 off, shading
+    // order 1 level-wide sort / 3 per-block sort / 2 none, bits per child box bound)
+    const uint32_t variants[][4] = {
+        {4u, 1u, 1u, 32u}, {4u, 2u, 1u, 32u}, {4u, 1u, 1u, 8u}, {4u, 1u, 3u, 32u},
+        {4u, 1u, 2u, 32u}, {2u, 1u, 1u, 32u}, {2u, 2u, 1u, 32u}};
+    {
+      const cg_tuning base = winner;
+      for (const auto& var : variants) {
+        cg_tuning t = base;
+        t.bvh_width = var[0];
+        t.persistent = var[1];
+        t.shade_sort = var[2];
+        t.box_bits = var[3];
+        consider(t);
+      }
+    }
+    {
+      const cg_tuning base = winner;
+      for (uint32_t pl : {1u, 2u, 3u, 4u}) {
+        cg_tuning t = base;
+        t.pipelines = pl;
+        consider(t);
+      }
+    }
+    {
+      const cg_tuning base = winner;
+      for (uint32_t q : {16u << 20, 64u << 20, 128u << 20}) {
+        cg_tuning t = base;
+        t.queue_capacity = q;
+        consider(t);
+      }
+    }
+    {
+      const cg_tuning base = winner;
+      for (uint32_t b : {64u, 128u, 256u}) {
+        cg_tuning t = base;
+        t.extend_block = b;
+        consider(t);
+      }
+    }
+    {
+      const cg_tuning base = winner;
+      for (uint32_t b : {64u, 128u, 256u}) {
+        cg_tuning t = base;
+        t.shade_block = b;
+        consider(t);
+      }
+    }
     env.dropAllGraphs();
-    float total = 0.0f;
-    for (int rep = 0; rep < 3; ++rep) {
-      BatchGraph* g = nullptr;
-      RenderRecord rec;
-      float ms = 0.0f;
-      if (runBatch(env, *s, views, count, g, rec, ms) != CG_OK) return 1e30f;
-      if (rep > 0) total += ms;
+    winner.use_graph = saved.use_graph;
+    env.tuning = winner;
+    // release an oversized queue if a smaller capacity won
+    if (env.wave.capacity > winner.queue_capacity) {
+      env.wave_arena.release();
+      env.wave = WaveBuffers{};
     }
-    return total;
-  };
-  // Coordinate descent from the current tuning: kernel variant, then queue
-  // capacity, then the traversal and shading block sizes.
-  cg_tuning winner = saved;
-  float best_ms = measure(winner);
-  auto consider = [&](cg_tuning t) {
-    const float ms = measure(t);
-    if (ms < best_ms) {
-      best_ms = ms;
-      winner = t;
-    }
-  };
-  // kernel variants: (node width, persistent lane refill 1 on / 2 off, shading
-  // order 1 level-wide sort / 3 per-block sort / 2 none, bits per child box bound)
-  const uint32_t variants[][4] = {
-      {4u, 1u, 1u, 32u}, {4u, 2u, 1u, 32u}, {4u, 1u, 1u, 8u}, {4u, 1u, 3u, 32u},
-      {4u, 1u, 2u, 32u}, {2u, 1u, 1u, 32u}, {2u, 2u, 1u, 32u}};
-  {
-    const cg_tuning base = winner;
-    for (const auto& var : variants) {
-      cg_tuning t = base;
-      t.bvh_width = var[0];
-      t.persistent = var[1];
-      t.shade_sort = var[2];
-      t.box_bits = var[3];
-      consider(t);
-    }
-  }
-  {
-    const cg_tuning base = winner;
-    for (uint32_t pl : {1u, 2u, 3u, 4u}) {
-      cg_tuning t = base;
-      t.pipelines = pl;
-      consider(t);
-    }
-  }
-  {
-    const cg_tuning base = winner;
-    for (uint32_t q : {16u << 20, 64u << 20, 128u << 20}) {
-      cg_tuning t = base;
-      t.queue_capacity = q;
-      consider(t);
-    }
-  }
-  {
-    const cg_tuning base = winner;
-    for (uint32_t b : {64u, 128u, 256u}) {
-      cg_tuning t = base;
-      t.extend_block = b;
-      consider(t);
-    }
-  }
-  {
-    const cg_tuning base = winner;
-    for (uint32_t b : {64u, 128u, 256u}) {
-      cg_tuning t = base;
-      t.shade_block = b;
-      consider(t);
-    }
-  }
-  env.dropAllGraphs();
-  winner.use_graph = saved.use_graph;
-  env.tuning = winner;
-  // release an oversized queue if a smaller capacity won
-  if (env.wave.capacity > winner.queue_capacity) {
-    env.wave_arena.release();
-    env.wave = WaveBuffers{};
-  }
-  if (best) *best = winner;
-  if (best_ms >= 1e30f) return fail(CG_E_CUDA, "autotune: no configuration ran");
-  return CG_OK;
+    if (best) *best = winner;
+    if (best_ms >= 1e30f) return fail(CG_E_CUDA, "autotune: no configuration ran");
+    return CG_OK;
+  });
 }
 
 CG_API int cg_autotune(cg_scene_t scene, const cg_view_desc* view, cg_tuning* best) {
-  return cg_autotune_views(scene, view, view ? 1u : 0u, best);
+  return guarded([&]() -> int {
+    return cg_autotune_views(scene, view, view ? 1u : 0u, best);
+  });
 }
 
 }  // extern "C"

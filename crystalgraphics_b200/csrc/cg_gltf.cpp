@@ -802,22 +802,6 @@ struct Loader {
 
 using namespace cg;
 
-namespace {
-// Runs an entry point's body; a C++ exception (an allocation that failed for
-// an absurd size in a damaged file, say) becomes an error status instead of
-// crossing the C ABI.
-template <class Body>
-int guarded(Body&& body) {
-  try {
-    return body();
-  } catch (const std::bad_alloc&) {
-    return cg::fail(CG_E_OOM, "out of host memory");
-  } catch (const std::exception& e) {
-    return cg::fail(CG_E_INVALID, e.what());
-  }
-}
-}  // namespace
-
 extern "C" CG_API int cg_gltf_parse(const char* path, cg_scene_desc* out, void** storage) {
   return guarded([&]() -> int {
     if (!path || !out || !storage) return fail(CG_E_INVALID, "null argument");

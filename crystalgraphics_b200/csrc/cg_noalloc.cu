@@ -124,86 +124,88 @@ using namespace cg;
 extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
                                         const cg_view_desc* view, void* film_xyzw,
                                         void* film_rgba8, void* stream) {
-  if (!scene || !conf || !view || !film_xyzw)
-    return fail(CG_E_INVALID, "null argument");
-  if (view->width == 0 || view->height == 0 || view->spp == 0)
-    return fail(CG_E_INVALID, "view has a zero size or spp");
-  SceneDev& sd = *reinterpret_cast<SceneDev*>(scene);
-  const Caps caps = capsOf(*conf);
-  const LevelPlan plan = planLevels(caps, std::max(1u, sd.max_lobes));
-  const uint64_t chunk = kNoAllocRays / std::max<uint64_t>(1, plan.max_product);
-  if (view->spp > chunk)
-    return fail(CG_E_INVALID,
-                "spp " + std::to_string(view->spp) + " exceeds the no-alloc scratch: at trace depth " +
-                    std::to_string(caps.trace_depth) + " one chunk holds at most " +
-                    std::to_string(chunk) + " samples (" + std::to_string(kNoAllocRays) +
-                    " queued rays)");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cudaFail(e, "cudaGetDevice");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  unsigned char* base = nullptr;
-  int rc = setupDevice(dev, s, &base);
-  if (rc != CG_OK) return rc;
-  // what must start at zero: counters, statistics, status word
-  e = cudaMemsetAsync(base + kOffCounts, 0, 3 * 256, s);
-  if (e != cudaSuccess) return cudaFail(e, "cudaMemsetAsync(scratch counters)");
-  ViewDev v;
-  std::memset(&v, 0, sizeof(v));
-  cameraBasis(view->camera, v);
-  v.width = view->width;
-  v.height = view->height;
-  v.spp = view->spp;
-  v.seed = view->seed;
-  v.frame = 0;
-  v.sample_weight = 1.0f;
-  v.pixel_base = 0;
-  v.pixel_count = v.width * v.height;
-  v.pixel_offset = 0;
-  v.sample_offset = 0;
-  v.film = static_cast<float4*>(film_xyzw);
-  v.rgba = static_cast<uchar4*>(film_rgba8);
-  // the view table goes into its scratch slot (a copy of a host struct, no
-  // allocation); stream order keeps it ahead of the kernels
-  e = cudaMemcpyAsync(base + kOffView, &v, sizeof(ViewDev), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return cudaFail(e, "cudaMemcpyAsync(view table)");
-  const WaveBuffers wb = scratchBuffers(base);
-  FrameConst fc;
-  fc.views = reinterpret_cast<const ViewDev*>(base + kOffView);
-  fc.view_count = 1;
-  fc.caps = caps;
-  fc.wl_tree = reinterpret_cast<const float*>(base + kOffWlTree);
-  fc.wl_const = reinterpret_cast<const float*>(base + kOffWlConst);
-  LaunchShape ls;  // default block sizes
-  const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
-  uint64_t pix = 0, smp = 0;
-  const uint64_t npx = v.pixel_count;
-  while (pix < npx) {  // the chunk sequence of Renderer::enqueueChunk
-    ChunkDesc ch;
-    ch.pixel_begin = pix;
-    ch.sample_begin = smp;
-    const uint64_t take = std::min<uint64_t>(npx - pix, chunk / v.spp);
-    ch.pixel_count = static_cast<uint32_t>(take);
-    ch.sample_count = static_cast<uint32_t>(take * v.spp);
-    launchGen(fc, wb, ch, s);
-    for (uint32_t d = 0; d < plan.levels; ++d) {
-      const int parity = static_cast<int>(d & 1u);
-      launchExtend(sd.view, wb, parity, false, ls, d >= cut_depth, s);
-      launchShade(sd.view, fc, wb, static_cast<int>(d), parity, ls, s);
-      if (plan.shadow[d]) launchShadow(sd.view, wb, false, ls, s);
+  return guarded([&]() -> int {
+    if (!scene || !conf || !view || !film_xyzw)
+      return fail(CG_E_INVALID, "null argument");
+    if (view->width == 0 || view->height == 0 || view->spp == 0)
+      return fail(CG_E_INVALID, "view has a zero size or spp");
+    SceneDev& sd = *reinterpret_cast<SceneDev*>(scene);
+    const Caps caps = capsOf(*conf);
+    const LevelPlan plan = planLevels(caps, std::max(1u, sd.max_lobes));
+    const uint64_t chunk = kNoAllocRays / std::max<uint64_t>(1, plan.max_product);
+    if (view->spp > chunk)
+      return fail(CG_E_INVALID,
+                  "spp " + std::to_string(view->spp) + " exceeds the no-alloc scratch: at trace depth " +
+                      std::to_string(caps.trace_depth) + " one chunk holds at most " +
+                      std::to_string(chunk) + " samples (" + std::to_string(kNoAllocRays) +
+                      " queued rays)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cudaFail(e, "cudaGetDevice");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* base = nullptr;
+    int rc = setupDevice(dev, s, &base);
+    if (rc != CG_OK) return rc;
+    // what must start at zero: counters, statistics, status word
+    e = cudaMemsetAsync(base + kOffCounts, 0, 3 * 256, s);
+    if (e != cudaSuccess) return cudaFail(e, "cudaMemsetAsync(scratch counters)");
+    ViewDev v;
+    std::memset(&v, 0, sizeof(v));
+    cameraBasis(view->camera, v);
+    v.width = view->width;
+    v.height = view->height;
+    v.spp = view->spp;
+    v.seed = view->seed;
+    v.frame = 0;
+    v.sample_weight = 1.0f;
+    v.pixel_base = 0;
+    v.pixel_count = v.width * v.height;
+    v.pixel_offset = 0;
+    v.sample_offset = 0;
+    v.film = static_cast<float4*>(film_xyzw);
+    v.rgba = static_cast<uchar4*>(film_rgba8);
+    // the view table goes into its scratch slot (a copy of a host struct, no
+    // allocation); stream order keeps it ahead of the kernels
+    e = cudaMemcpyAsync(base + kOffView, &v, sizeof(ViewDev), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cudaFail(e, "cudaMemcpyAsync(view table)");
+    const WaveBuffers wb = scratchBuffers(base);
+    FrameConst fc;
+    fc.views = reinterpret_cast<const ViewDev*>(base + kOffView);
+    fc.view_count = 1;
+    fc.caps = caps;
+    fc.wl_tree = reinterpret_cast<const float*>(base + kOffWlTree);
+    fc.wl_const = reinterpret_cast<const float*>(base + kOffWlConst);
+    LaunchShape ls;  // default block sizes
+    const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
+    uint64_t pix = 0, smp = 0;
+    const uint64_t npx = v.pixel_count;
+    while (pix < npx) {  // the chunk sequence of Renderer::enqueueChunk
+      ChunkDesc ch;
+      ch.pixel_begin = pix;
+      ch.sample_begin = smp;
+      const uint64_t take = std::min<uint64_t>(npx - pix, chunk / v.spp);
+      ch.pixel_count = static_cast<uint32_t>(take);
+      ch.sample_count = static_cast<uint32_t>(take * v.spp);
+      launchGen(fc, wb, ch, s);
+      for (uint32_t d = 0; d < plan.levels; ++d) {
+        const int parity = static_cast<int>(d & 1u);
+        launchExtend(sd.view, wb, parity, false, ls, d >= cut_depth, s);
+        launchShade(sd.view, fc, wb, static_cast<int>(d), parity, ls, s);
+        if (plan.shadow[d]) launchShadow(sd.view, wb, false, ls, s);
+      }
+      launchResolve(fc, wb, ch, s);
+      pix += take;
+      smp += take * v.spp;
     }
-    launchResolve(fc, wb, ch, s);
-    pix += take;
-    smp += take * v.spp;
-  }
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cudaFail(e, "wavefront launch");
-  uint32_t status = 0;
-  e = cudaMemcpyAsync(&status, base + kOffStatus, 4, cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return cudaFail(e, "cudaMemcpyAsync(status)");
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return cudaFail(e, "cudaStreamSynchronize");
-  if (status & 1u) return fail(CG_E_DEVICE, "traversal stack overflow in a kernel");
-  if (status & 2u) return fail(CG_E_DEVICE, "ray queue overflow in a kernel");
-  return CG_OK;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cudaFail(e, "wavefront launch");
+    uint32_t status = 0;
+    e = cudaMemcpyAsync(&status, base + kOffStatus, 4, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cudaFail(e, "cudaMemcpyAsync(status)");
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cudaFail(e, "cudaStreamSynchronize");
+    if (status & 1u) return fail(CG_E_DEVICE, "traversal stack overflow in a kernel");
+    if (status & 2u) return fail(CG_E_DEVICE, "ray queue overflow in a kernel");
+    return CG_OK;
+  });
 }

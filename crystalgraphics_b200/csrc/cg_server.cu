@@ -602,145 +602,157 @@ extern "C" {
 
 CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint64_t hbm_budget_bytes,
                             cg_server_t* out) {
-  if (!scenes || scene_count == 0 || !out) return fail(CG_E_INVALID, "null argument");
-  *out = nullptr;
-  cg_conf conf;
-  cg_tuning tuning;
-  int device = 0;
-  {
-    std::lock_guard<std::mutex> lk(g_env_mu);
-    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
-    conf = g_env->conf;
-    tuning = g_env->tuning;
-    device = g_env->device;
-  }
-  for (uint32_t i = 0; i < scene_count; ++i)
-    if (!scenes[i]) return fail(CG_E_INVALID, "null scene");
-  auto sv = std::make_unique<cg_server_s>();
-  for (uint32_t i = 0; i < scene_count; ++i) sv->scenes.push_back(reinterpret_cast<SceneDev*>(scenes[i]));
-  sv->budget = hbm_budget_bytes;
-  sv->conf = conf;
-  for (ServerLane& lane : sv->lanes) {
-    lane.rend.tuning = tuning;
-    int rc = lane.rend.init(device);
-    if (rc != CG_OK) return rc;
-    rc = lane.rend.ensureWave(tuning.queue_capacity);
-    if (rc != CG_OK) return rc;
-    if (cudaMallocHost(&lane.status_host, sizeof(uint32_t)) != cudaSuccess ||
-        cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(CG_E_CUDA, "server lane setup failed");
+  return guarded([&]() -> int {
+    if (!scenes || scene_count == 0 || !out) return fail(CG_E_INVALID, "null argument");
+    *out = nullptr;
+    cg_conf conf;
+    cg_tuning tuning;
+    int device = 0;
+    {
+      std::lock_guard<std::mutex> lk(g_env_mu);
+      if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+      conf = g_env->conf;
+      tuning = g_env->tuning;
+      device = g_env->device;
     }
-    *lane.status_host = 0u;
-  }
-  if (cudaStreamCreateWithFlags(&sv->alloc_stream, cudaStreamNonBlocking) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(CG_E_CUDA, "server stream setup failed");
-  }
-  sv->worker = std::thread(serverLoop, sv.get());
-  sv->copier = std::thread(copyLoop, sv.get(), device);
-  sv->prefaulter = std::thread(prefaultLoop, sv.get());
-  *out = sv.release();
-  return CG_OK;
+    for (uint32_t i = 0; i < scene_count; ++i)
+      if (!scenes[i]) return fail(CG_E_INVALID, "null scene");
+    auto sv = std::make_unique<cg_server_s>();
+    for (uint32_t i = 0; i < scene_count; ++i) sv->scenes.push_back(reinterpret_cast<SceneDev*>(scenes[i]));
+    sv->budget = hbm_budget_bytes;
+    sv->conf = conf;
+    for (ServerLane& lane : sv->lanes) {
+      lane.rend.tuning = tuning;
+      int rc = lane.rend.init(device);
+      if (rc != CG_OK) return rc;
+      rc = lane.rend.ensureWave(tuning.queue_capacity);
+      if (rc != CG_OK) return rc;
+      if (cudaMallocHost(&lane.status_host, sizeof(uint32_t)) != cudaSuccess ||
+          cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CG_E_CUDA, "server lane setup failed");
+      }
+      *lane.status_host = 0u;
+    }
+    if (cudaStreamCreateWithFlags(&sv->alloc_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CG_E_CUDA, "server stream setup failed");
+    }
+    sv->worker = std::thread(serverLoop, sv.get());
+    sv->copier = std::thread(copyLoop, sv.get(), device);
+    sv->prefaulter = std::thread(prefaultLoop, sv.get());
+    *out = sv.release();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_server_destroy(cg_server_t server) {
-  if (!server) return CG_OK;
-  {
-    std::lock_guard<std::mutex> lk(server->mu);
-    for (ServerReq* r : server->pending) r->cancelled = true;
-    for (ServerReq* r : server->active) r->cancelled = true;
-    server->stop = true;
-  }
-  server->cv.notify_all();
-  if (server->worker.joinable()) server->worker.join();
-  {
-    std::lock_guard<std::mutex> lk(server->copy_mu);
-    server->copy_stop = true;  // the copier drains its queue first
-  }
-  server->copy_cv.notify_all();
-  if (server->copier.joinable()) server->copier.join();
-  {
-    std::lock_guard<std::mutex> lk(server->pf_mu);
-    server->pf_stop = true;  // buffers not yet populated are simply written later
-  }
-  server->pf_cv.notify_all();
-  if (server->prefaulter.joinable()) server->prefaulter.join();
-  delete server;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!server) return CG_OK;
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      for (ServerReq* r : server->pending) r->cancelled = true;
+      for (ServerReq* r : server->active) r->cancelled = true;
+      server->stop = true;
+    }
+    server->cv.notify_all();
+    if (server->worker.joinable()) server->worker.join();
+    {
+      std::lock_guard<std::mutex> lk(server->copy_mu);
+      server->copy_stop = true;  // the copier drains its queue first
+    }
+    server->copy_cv.notify_all();
+    if (server->copier.joinable()) server->copier.join();
+    {
+      std::lock_guard<std::mutex> lk(server->pf_mu);
+      server->pf_stop = true;  // buffers not yet populated are simply written later
+    }
+    server->pf_cv.notify_all();
+    if (server->prefaulter.joinable()) server->prefaulter.join();
+    delete server;
+    return CG_OK;
+  });
 }
 
 CG_API int cg_server_submit(cg_server_t server, const cg_request* request, float* film_xyz,
                             uint64_t* request_id) {
-  if (!server || !request || !film_xyz) return fail(CG_E_INVALID, "null argument");
-  const cg_view_desc& v = request->view;
-  if (request->scene >= server->scenes.size()) return fail(CG_E_INVALID, "scene index out of range");
-  if (v.width == 0 || v.height == 0 || v.spp == 0) return fail(CG_E_INVALID, "zero size or spp");
-  SceneDev& scene = *server->scenes[request->scene];
-  if (v.spp > server->lanes[0].rend.chunkSamples(scene, capsOf(server->conf)))
-    return fail(CG_E_INVALID, "spp exceeds the wavefront chunk");
-  auto r = std::make_unique<ServerReq>();
-  r->req = *request;
-  r->out = film_xyz;
-  r->npx = v.width * v.height;
-  r->submit_s = nowSeconds();
-  r->bytes = requestBytes(*server, scene, *request);
-  std::lock_guard<std::mutex> lk(server->mu);
-  if (server->fatal != CG_OK) return fail(server->fatal, server->fatal_msg);
-  if (server->stop) return fail(CG_E_INVALID, "server is shutting down");
-  r->id = server->next_id++;
-  if (request_id) *request_id = r->id;
-  server->pending.push_back(r.get());
-  {
-    std::lock_guard<std::mutex> plk(server->pf_mu);
-    server->pf_q.emplace_back(film_xyz, size_t(r->npx) * 12);
-  }
-  server->pf_cv.notify_one();
-  server->reqs[r->id] = std::move(r);
-  ++server->st.submitted;
-  server->cv.notify_all();
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!server || !request || !film_xyz) return fail(CG_E_INVALID, "null argument");
+    const cg_view_desc& v = request->view;
+    if (request->scene >= server->scenes.size()) return fail(CG_E_INVALID, "scene index out of range");
+    if (v.width == 0 || v.height == 0 || v.spp == 0) return fail(CG_E_INVALID, "zero size or spp");
+    SceneDev& scene = *server->scenes[request->scene];
+    if (v.spp > server->lanes[0].rend.chunkSamples(scene, capsOf(server->conf)))
+      return fail(CG_E_INVALID, "spp exceeds the wavefront chunk");
+    auto r = std::make_unique<ServerReq>();
+    r->req = *request;
+    r->out = film_xyz;
+    r->npx = v.width * v.height;
+    r->submit_s = nowSeconds();
+    r->bytes = requestBytes(*server, scene, *request);
+    std::lock_guard<std::mutex> lk(server->mu);
+    if (server->fatal != CG_OK) return fail(server->fatal, server->fatal_msg);
+    if (server->stop) return fail(CG_E_INVALID, "server is shutting down");
+    r->id = server->next_id++;
+    if (request_id) *request_id = r->id;
+    server->pending.push_back(r.get());
+    {
+      std::lock_guard<std::mutex> plk(server->pf_mu);
+      server->pf_q.emplace_back(film_xyz, size_t(r->npx) * 12);
+    }
+    server->pf_cv.notify_one();
+    server->reqs[r->id] = std::move(r);
+    ++server->st.submitted;
+    server->cv.notify_all();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_server_wait(cg_server_t server, uint64_t request_id, int timeout_ms,
                           cg_request_result* result) {
-  if (!server) return fail(CG_E_INVALID, "null argument");
-  std::unique_lock<std::mutex> lk(server->mu);
-  auto it = server->reqs.find(request_id);
-  if (it == server->reqs.end()) return fail(CG_E_INVALID, "unknown request id");
-  ServerReq* r = it->second.get();
-  auto pred = [&] { return r->done; };
-  if (timeout_ms < 0)
-    server->done_cv.wait(lk, pred);
-  else if (!server->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred))
-    return fail(CG_E_TIMEOUT, "request not finished within the timeout");
-  if (result) {
-    result->status = r->status;
-    result->submit_s = r->submit_s;
-    result->start_s = r->start_s;
-    result->finish_s = r->finish_s;
-  }
-  const int st = r->status;
-  server->reqs.erase(it);
-  if (st != CG_OK) return fail(st, st == CG_E_CANCELLED ? "request cancelled" : "request failed");
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!server) return fail(CG_E_INVALID, "null argument");
+    std::unique_lock<std::mutex> lk(server->mu);
+    auto it = server->reqs.find(request_id);
+    if (it == server->reqs.end()) return fail(CG_E_INVALID, "unknown request id");
+    ServerReq* r = it->second.get();
+    auto pred = [&] { return r->done; };
+    if (timeout_ms < 0)
+      server->done_cv.wait(lk, pred);
+    else if (!server->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred))
+      return fail(CG_E_TIMEOUT, "request not finished within the timeout");
+    if (result) {
+      result->status = r->status;
+      result->submit_s = r->submit_s;
+      result->start_s = r->start_s;
+      result->finish_s = r->finish_s;
+    }
+    const int st = r->status;
+    server->reqs.erase(it);
+    if (st != CG_OK) return fail(st, st == CG_E_CANCELLED ? "request cancelled" : "request failed");
+    return CG_OK;
+  });
 }
 
 CG_API int cg_server_cancel(cg_server_t server, uint64_t request_id) {
-  if (!server) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(server->mu);
-  auto it = server->reqs.find(request_id);
-  if (it == server->reqs.end()) return fail(CG_E_INVALID, "unknown request id");
-  it->second->cancelled = true;
-  server->cv.notify_all();
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!server) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(server->mu);
+    auto it = server->reqs.find(request_id);
+    if (it == server->reqs.end()) return fail(CG_E_INVALID, "unknown request id");
+    it->second->cancelled = true;
+    server->cv.notify_all();
+    return CG_OK;
+  });
 }
 
 CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out) {
-  if (!server || !out) return fail(CG_E_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(server->mu);
-  *out = server->st;
-  return CG_OK;
+  return guarded([&]() -> int {
+    if (!server || !out) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(server->mu);
+    *out = server->st;
+    return CG_OK;
+  });
 }
 
 }  // extern "C"
