@@ -164,6 +164,10 @@ def test_normalized_and_sparse_accessors(tmp_path):
     p = _load(tmp_path, _one_triangle_doc(sparse, views, pos + sp_idx + sp_val))
     assert len(p.vertices) == 3 and not p.vertices["position"].any()
     np.testing.assert_array_equal(p.indices, [0, 1, 2])
+    # the usual form, a sparse accessor with no bufferView, reads as zeros too
+    no_view = {k: v for k, v in sparse.items() if k != "bufferView"}
+    p = _load(tmp_path, _one_triangle_doc(no_view, views, pos + sp_idx + sp_val))
+    assert len(p.vertices) == 3 and not p.vertices["position"].any()
     # cgltf_validate's checks of the sparse block
     bad_index = np.array([3], np.uint8).tobytes() + b"\0\0\0"
     with pytest.raises(B.Error, match="sparse accessor index"):
