@@ -425,6 +425,17 @@ struct Decoder {
   }
 
   // ---- blocks -> samples -> RGBA ----
+  // floor(h) clamped to 0..255, exactly as std::floor gives it, without the
+  // library call that x86-64's baseline instruction set needs for std::floor.
+  // h is bounded first: a damaged stream's coefficients can take a sum far
+  // outside the int range (and fmax/fmin take a NaN to a bound).
+  static uint8_t floorToByte(float h) {
+    h = std::fmin(std::fmax(h, -1.0f), 256.0f);
+    int i = static_cast<int>(h);
+    i -= static_cast<float>(i) > h;
+    return static_cast<uint8_t>(std::clamp(i, 0, 255));
+  }
+
   void idct(const int16_t* b, const uint16_t* q, uint8_t* out, int stride) {
     static float ctab[8][8];
     static bool init = false;
@@ -447,8 +458,7 @@ struct Decoder {
       for (int x = 0; x < 8; ++x) {
         float s = 0.0f;
         for (int v = 0; v < 8; ++v) s += ctab[y][v] * rows[v * 8 + x];
-        const float px = std::floor(s + 128.5f);
-        out[y * stride + x] = static_cast<uint8_t>(std::clamp(px, 0.0f, 255.0f));
+        out[y * stride + x] = floorToByte(s + 128.5f);
       }
   }
 
@@ -524,9 +534,9 @@ struct Decoder {
       }
       const float y = a[i], cb = b[i] - 128.0f, cr = c[i] - 128.0f;  // JFIF YCbCr
       const float r = y + 1.402f * cr, g = y - 0.344136f * cb - 0.714136f * cr, bl = y + 1.772f * cb;
-      rgba[4 * i] = static_cast<uint8_t>(std::clamp(std::floor(r + 0.5f), 0.0f, 255.0f));
-      rgba[4 * i + 1] = static_cast<uint8_t>(std::clamp(std::floor(g + 0.5f), 0.0f, 255.0f));
-      rgba[4 * i + 2] = static_cast<uint8_t>(std::clamp(std::floor(bl + 0.5f), 0.0f, 255.0f));
+      rgba[4 * i] = floorToByte(r + 0.5f);
+      rgba[4 * i + 1] = floorToByte(g + 0.5f);
+      rgba[4 * i + 2] = floorToByte(bl + 0.5f);
     }
   }
 
