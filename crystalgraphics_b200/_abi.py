@@ -82,7 +82,8 @@ class CgStats(C.Structure):
     _fields_ = [
         ("samples", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
         ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64), ("inst_visits", C.c_uint64),
-        ("chunks", u32), ("kernel_launches", u32), ("device_ms", f32),
+        ("chunks", u32), ("kernel_launches", u32), ("device_ms", f32), ("_pad", u32),
+        ("nonfinite_samples", C.c_uint64),
     ]
 
 

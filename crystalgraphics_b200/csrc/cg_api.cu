@@ -52,6 +52,39 @@ int cudaFail(cudaError_t e, const char* what) {
               std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+int currentContextId(unsigned long long* id) {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(fn);
+    fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(fn);
+    cudaGetLastError();
+  });
+  if (!get_current || !get_id) return fail(CG_E_CUDA, "the driver has no cuCtxGetId");
+  void* ctx = nullptr;
+  if (get_current(&ctx) != 0) return fail(CG_E_CUDA, "cuCtxGetCurrent failed");
+  if (!ctx) {
+    // nothing current yet: the runtime's primary context of the current
+    // device (cudaSetDevice initialises it; it allocates nothing)
+    int dev = 0;
+    CG_CUDA(cudaGetDevice(&dev));
+    CG_CUDA(cudaSetDevice(dev));
+    if (get_current(&ctx) != 0 || !ctx) return fail(CG_E_CUDA, "no current CUDA context");
+  }
+  if (get_id(ctx, id) != 0) return fail(CG_E_CUDA, "cuCtxGetId failed");
+  return CG_OK;
+}
+
 int DeviceArena::alloc(size_t bytes) {
   release();
   if (bytes == 0) bytes = 256;
@@ -101,7 +134,10 @@ int uploadScene(const HostScene& h, SceneDev& s) {
     p.off = total;
     total += align256(std::max<size_t>(p.bytes, 16));
   }
-  int rc = s.arena.alloc(total);
+  CG_CUDA(cudaGetDevice(&s.device));
+  int rc = currentContextId(&s.ctx_id);
+  if (rc != CG_OK) return rc;
+  rc = s.arena.alloc(total);
   if (rc != CG_OK) return rc;
   char* base = static_cast<char*>(s.arena.base);
   for (auto& p : parts)
@@ -533,6 +569,7 @@ int Renderer::readStats(cudaStream_t s, const RenderRecord& rec, float ms, cg_st
   out.node_visits = st[0][2];
   out.tri_tests = st[0][3];
   out.inst_visits = st[0][4];
+  out.nonfinite_samples = st[0][5];
   out.chunks = rec.chunks;
   out.kernel_launches = rec.launches;
   out.device_ms = ms;

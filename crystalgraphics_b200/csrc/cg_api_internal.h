@@ -37,6 +37,12 @@ int guarded(Body&& body) {
 }
 int cudaFail(cudaError_t e, const char* what);
 
+// The identity of the calling thread's current CUDA context: a 64-bit id the
+// driver never reuses within a process (cuCtxGetId, reached through the
+// runtime's driver entry points so that the library does not link libcuda).
+// A device reset or a context switch changes it.  Returns CG_OK or an error.
+int currentContextId(unsigned long long* id);
+
 #define CG_CUDA(call)                                  \
   do {                                                 \
     cudaError_t e_ = (call);                           \
@@ -74,6 +80,10 @@ struct SceneDev {
   uint32_t max_lobes = 1;
   uint64_t tag = 0;
   cg_scene_info info{};
+  // where the device buffers live: the device current at upload and its
+  // context (entry points that run on the caller's current device check both)
+  int device = -1;
+  unsigned long long ctx_id = 0;
 };
 
 int uploadScene(const HostScene& h, SceneDev& s);

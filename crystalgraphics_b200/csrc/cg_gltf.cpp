@@ -725,6 +725,41 @@ struct Loader {
     return r;
   }
 
+  // Every node has at most one parent and the parent links form no loop, as
+  // cgltf v1.14 checks while it parses and validates a file (the reference
+  // loads through cgltf_parse_file and cgltf_validate, src/scene.cpp:838-850).
+  // It also keeps the walk below linear in the number of nodes: a node shared
+  // by two parents at every level would otherwise multiply the paths.
+  bool checkHierarchy() {
+    const Json* ns = doc.get("nodes");
+    if (!ns) return true;
+    const size_t n = ns->a.size();
+    std::vector<int64_t> parent(n, -1);
+    for (size_t i = 0; i < n; ++i)
+      if (const Json* ch = ns->a[i].get("children"))
+        for (const Json& c : ch->a) {
+          const int64_t k = c.asInt();
+          if (k < 0 || size_t(k) >= n) return fail("bad node index");
+          if (parent[k] >= 0) return fail("node " + std::to_string(k) + " has two parents");
+          parent[k] = int64_t(i);
+        }
+    // 0 = not seen, 1 = on the chain being followed, 2 = reaches a root
+    std::vector<uint8_t> state(n, 0);
+    std::vector<int64_t> chain;
+    for (size_t i = 0; i < n; ++i) {
+      chain.clear();
+      int64_t k = int64_t(i);
+      while (k >= 0 && state[k] == 0) {
+        state[k] = 1;
+        chain.push_back(k);
+        k = parent[k];
+      }
+      if (k >= 0 && state[k] == 1) return fail("node hierarchy has a cycle");
+      for (int64_t c : chain) state[c] = 2;
+    }
+    return true;
+  }
+
   bool walk(int64_t node, const M4& parent, int depth) {
     const Json* ns = doc.get("nodes");
     if (!ns || node < 0 || size_t(node) >= ns->a.size()) return fail("bad node index");
@@ -785,6 +820,7 @@ struct Loader {
     root.m[6] = 1.0;
     root.m[9] = -1.0;  // column 2: (0, -1, 0)
     root.m[10] = 0.0;
+    if (!checkHierarchy()) return false;
     const Json* scenes = doc.get("scenes");
     int64_t sc = doc.integer("scene", 0);
     if (scenes && !scenes->a.empty()) {

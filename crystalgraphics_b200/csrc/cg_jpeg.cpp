@@ -437,15 +437,21 @@ struct Decoder {
   }
 
   void idct(const int16_t* b, const uint16_t* q, uint8_t* out, int stride) {
-    static float ctab[8][8];
-    static bool init = false;
-    if (!init) {  // ctab[x][u] = C(u) / 2 * cos((2x + 1) u pi / 16), C(0) = 1 / sqrt(2)
+    // ctab[x][u] = C(u) / 2 * cos((2x + 1) u pi / 16), C(0) = 1 / sqrt(2); a
+    // function-local static is initialised once even when threads decode at
+    // the same time
+    struct CosTable {
+      float v[8][8];
+    };
+    static const CosTable tab = [] {
+      CosTable t{};
       for (int x = 0; x < 8; ++x)
         for (int u = 0; u < 8; ++u)
-          ctab[x][u] = static_cast<float>((u == 0 ? std::sqrt(0.5) : 1.0) * 0.5 *
-                                          std::cos((2 * x + 1) * u * M_PI / 16.0));
-      init = true;
-    }
+          t.v[x][u] = static_cast<float>((u == 0 ? std::sqrt(0.5) : 1.0) * 0.5 *
+                                         std::cos((2 * x + 1) * u * M_PI / 16.0));
+      return t;
+    }();
+    const auto& ctab = tab.v;
     float f[64], rows[64];
     for (int i = 0; i < 64; ++i) f[i] = static_cast<float>(b[i]) * static_cast<float>(q[i]);
     for (int v = 0; v < 8; ++v)

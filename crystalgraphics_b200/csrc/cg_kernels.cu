@@ -843,13 +843,21 @@ __global__ void k_resolve(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   // ranges that partition a pixel's samples add up to the full frame
   const float spp = static_cast<float>(v.spp_total ? v.spp_total : v.spp);
   V3 acc{0.0f, 0.0f, 0.0f};
+  uint32_t dropped = 0;
   for (uint32_t k = 0; k < v.spp; ++k) {
     const float L = wb.s_L[first + k];
     const float lambda = wb.s_lambda[first + k];
     const float prob = wb.s_prob[first + k];
     const V3 il = xyzMatch(lambda) * L / avg;
-    acc = acc + il / prob / spp;
+    const V3 term = il / prob / spp;
+    // a sample whose estimate is not finite adds nothing (and is counted):
+    // one NaN would otherwise stay in the pixel's running mean for good
+    if (isfinite(term.x) && isfinite(term.y) && isfinite(term.z))
+      acc = acc + term;
+    else
+      ++dropped;
   }
+  if (dropped) atomicAdd(&wb.stats[5], static_cast<unsigned long long>(dropped));
   V3 lum{0.0f, 0.0f, 0.0f};
   if (v.frame > 0u) {
     const float4 f = v.film[pixel];

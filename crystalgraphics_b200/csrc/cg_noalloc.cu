@@ -58,21 +58,26 @@ static_assert(kOffCounts % 256 == 0 && kOffWlTree % 256 == 0, "256-byte aligned 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 struct DeviceSetup {
-  bool done = false;
-  unsigned char* base = nullptr;  // device address of g_noalloc_scratch
+  unsigned long long ctx_id = 0;  // the context the set-up belongs to (0 = none yet)
+  unsigned char* base = nullptr;  // device address of g_noalloc_scratch there
 };
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mu;
 
-// Once per device, with that device current: the device address of the
-// scratch (the host-side symbol is only a stand-in, never a device pointer)
-// and the wavelength table, computed into the scratch.
-int setupDevice(int dev, cudaStream_t stream, unsigned char** base) {
+// Once per device and context, with that device current: the device address
+// of the scratch (the host-side symbol is only a stand-in, never a device
+// pointer) and the wavelength table, computed into the scratch.  A new context
+// on the device (after a device reset, or another context made current) gets
+// the set-up again: its copy of the array starts as zeros at a possibly new
+// address.
+int setupDevice(int dev, unsigned long long ctx, cudaStream_t stream, unsigned char** base) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
   if (dev < 0 || dev >= kMaxDevices) return fail(CG_E_INVALID, "device index out of range");
   DeviceSetup& s = g_setup[dev];
-  if (!s.done) {
+  if (s.ctx_id != ctx) {
+    s.ctx_id = 0;
+    s.base = nullptr;
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess) return cudaFail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
@@ -84,9 +89,54 @@ int setupDevice(int dev, cudaStream_t stream, unsigned char** base) {
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cudaFail(e, "wavelength table");
     s.base = b;
-    s.done = true;
+    s.ctx_id = ctx;
   }
   *base = s.base;
+  return CG_OK;
+}
+
+// The size of the device allocation that holds `p` from `p` on
+// (cuMemGetAddressRange through the runtime's driver entry points); 0 when the
+// driver cannot tell, in which case the caller's size is taken on trust.
+size_t deviceBytesFrom(const void* p) {
+  using GetRange = int (*)(unsigned long long*, size_t*, unsigned long long);
+  static GetRange get_range = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_range = reinterpret_cast<GetRange>(fn);
+    cudaGetLastError();
+  });
+  if (!get_range) return 0;
+  unsigned long long lo = 0;
+  size_t size = 0;
+  const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+  if (get_range(&lo, &size, a) != 0 || a < lo || a - lo > size) return 0;
+  return static_cast<size_t>(lo + size - a);
+}
+
+// A film argument must be device (or managed) memory of device `dev` with
+// room for `bytes`.
+int checkFilm(const void* p, size_t bytes, int dev, const char* name) {
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CG_E_INVALID, std::string(name) + " is not a device pointer");
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return fail(CG_E_INVALID, std::string(name) + " is not device memory");
+  if (a.type == cudaMemoryTypeDevice && a.device != dev)
+    return fail(CG_E_INVALID, std::string(name) + " belongs to device " + std::to_string(a.device) +
+                                  ", not the current device " + std::to_string(dev));
+  const size_t have = deviceBytesFrom(p);
+  if (have != 0 && have < bytes)
+    return fail(CG_E_INVALID, std::string(name) + " holds " + std::to_string(have) +
+                                  " bytes from its start; the view needs " + std::to_string(bytes));
   return CG_OK;
 }
 
@@ -129,6 +179,9 @@ extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
       return fail(CG_E_INVALID, "null argument");
     if (view->width == 0 || view->height == 0 || view->spp == 0)
       return fail(CG_E_INVALID, "view has a zero size or spp");
+    const uint64_t npx = uint64_t(view->width) * view->height;
+    if (npx > 0xffffffffull)
+      return fail(CG_E_INVALID, "view has more than 2^32 - 1 pixels");
     SceneDev& sd = *reinterpret_cast<SceneDev*>(scene);
     const Caps caps = capsOf(*conf);
     const LevelPlan plan = planLevels(caps, std::max(1u, sd.max_lobes));
@@ -139,12 +192,39 @@ extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
                       std::to_string(caps.trace_depth) + " one chunk holds at most " +
                       std::to_string(chunk) + " samples (" + std::to_string(kNoAllocRays) +
                       " queued rays)");
+    // everything runs on the caller's current device, which must be the one
+    // (and the context) the scene was uploaded in
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cudaFail(e, "cudaGetDevice");
+    if (dev != sd.device)
+      return fail(CG_E_INVALID, "the scene was uploaded on device " + std::to_string(sd.device) +
+                                    " but the current device is " + std::to_string(dev) +
+                                    ": make the scene's device current first");
+    unsigned long long ctx = 0;
+    int rc = currentContextId(&ctx);
+    if (rc != CG_OK) return rc;
+    if (ctx != sd.ctx_id)
+      return fail(CG_E_INVALID,
+                  "the scene was uploaded in another CUDA context of this device (the device was "
+                  "reset, or another context is current): its buffers are not valid here");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (s) {
+      int sdev = -1;
+      e = cudaStreamGetDevice(s, &sdev);
+      if (e != cudaSuccess) return cudaFail(e, "cudaStreamGetDevice");
+      if (sdev != dev)
+        return fail(CG_E_INVALID, "the stream belongs to device " + std::to_string(sdev) +
+                                      ", not the current device " + std::to_string(dev));
+    }
+    rc = checkFilm(film_xyzw, npx * 16, dev, "film_xyzw");
+    if (rc != CG_OK) return rc;
+    if (film_rgba8) {
+      rc = checkFilm(film_rgba8, npx * 4, dev, "film_rgba8");
+      if (rc != CG_OK) return rc;
+    }
     unsigned char* base = nullptr;
-    int rc = setupDevice(dev, s, &base);
+    rc = setupDevice(dev, ctx, s, &base);
     if (rc != CG_OK) return rc;
     // what must start at zero: counters, statistics, status word
     e = cudaMemsetAsync(base + kOffCounts, 0, 3 * 256, s);
@@ -159,7 +239,7 @@ extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
     v.frame = 0;
     v.sample_weight = 1.0f;
     v.pixel_base = 0;
-    v.pixel_count = v.width * v.height;
+    v.pixel_count = static_cast<uint32_t>(npx);
     v.pixel_offset = 0;
     v.sample_offset = 0;
     v.film = static_cast<float4*>(film_xyzw);
@@ -178,7 +258,6 @@ extern "C" CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf,
     LaunchShape ls;  // default block sizes
     const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
     uint64_t pix = 0, smp = 0;
-    const uint64_t npx = v.pixel_count;
     while (pix < npx) {  // the chunk sequence of Renderer::enqueueChunk
       ChunkDesc ch;
       ch.pixel_begin = pix;

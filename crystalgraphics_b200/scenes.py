@@ -478,7 +478,8 @@ def _random_rotation(rng):
 
 
 def instanced_scene(width=1920, height=1080, spp=64, depth=12, instances=4096, lights=10000,
-                    seed=2, mesh_scale=1.0, extent=50.0, camera_distance=150.0) -> Scene:
+                    seed=2, mesh_scale=1.0, extent=50.0, camera_distance=150.0,
+                    radiance_sigma=2.0) -> Scene:
     rng = np.random.default_rng(seed)
     b = _Builder()
     meshes = []
@@ -506,7 +507,7 @@ def instanced_scene(width=1920, height=1080, spp=64, depth=12, instances=4096, l
         b.add_instance(meshes[rng.integers(8)], mat,
                        _trs((s, s, s), translate=rng.uniform(-extent, extent, 3),
                             rot=_random_rotation(rng)))
-    radiance = np.exp(rng.normal(0.0, 2.0, lights))
+    radiance = np.exp(rng.normal(0.0, radiance_sigma, lights))
     centers = rng.uniform(-extent, extent, (lights, 3))
     _emissive_triangles(b, rng, lights, radiance, centers, 0.5)
     cam = _abi.make_camera((0.0, -camera_distance, 0.13 * camera_distance), (0.0, 1.0, -0.13),

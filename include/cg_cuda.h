@@ -343,6 +343,10 @@ typedef struct cg_stats {
   uint32_t chunks;           /* wavefront chunks the work was split into      */
   uint32_t kernel_launches;  /* kernels this library launched                 */
   float device_ms;           /* CUDA-event time of the device work            */
+  uint32_t _pad;
+  uint64_t nonfinite_samples; /* samples whose estimate was NaN or infinite:
+                                 they add nothing to the film, so one bad
+                                 sample cannot stay in a pixel's running mean */
 } cg_stats;
 CG_API int cg_last_stats(cg_stats* out);
 /* 1 = count node visits / triangle tests in the traversal kernels (slower;
@@ -496,11 +500,19 @@ CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out);
  * It calls no cudaMalloc or cudaFree: the ray queues and tables live in a
  * library-owned device array of about 19.3 MB (131072 queued rays) that every
  * GPU loading the library holds until the process exits.  A view whose spp
- * cannot fit that array in one chunk is rejected with CG_E_INVALID.  The first
- * call on a device sets the array up (finds its device address, fills the
- * wavelength table); make that first call before any stream capture.  All
- * calls share the array: calls that overlap on the GPU (other threads, other
- * streams of the same device) race and must be serialised by the caller. */
+ * cannot fit that array in one chunk is rejected with CG_E_INVALID.  The call
+ * runs on the caller's current device, which must be the device and CUDA
+ * context the scene was uploaded in (a scene from another device, or from
+ * before a device reset, is rejected with CG_E_INVALID); `stream` must belong
+ * to that device.  Films must be device (or managed) memory of that device;
+ * a host pointer, a film the driver reports as smaller than the view
+ * (16 B / 4 B per pixel), or a view of more than 2^32 - 1 pixels is rejected
+ * with CG_E_INVALID before anything runs.  The first call in a device's
+ * context sets the array up (finds its device address, fills the wavelength
+ * table), and so does the first call after that context changes (a device
+ * reset); make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (other threads, other streams of
+ * the same device) race and must be serialised by the caller. */
 CG_API int cg_render_noalloc(cg_scene_t scene, const cg_conf* conf, const cg_view_desc* view,
                              void* film_xyzw, void* film_rgba8, void* stream);
 

@@ -470,7 +470,7 @@ inline TriHit rayIntersectTriangle(const Ray& ray, V3 v0, V3 v1, V3 v2) {
 }
 
 struct Counters {
-  uint64_t extend = 0, shadow = 0, nodes = 0, tris = 0;
+  uint64_t extend = 0, shadow = 0, nodes = 0, tris = 0, nonfinite = 0;
 };
 
 struct ClosestHit {
@@ -1441,7 +1441,13 @@ int oracle_render(oracle_scene_t s, const oracle_render_args* a, float* film, ui
         ws = sampleWavelengthCdf(randFloat(seq));
       }
       float L = trace(tc, ray, ws.wavelength, 0, key);
-      acc = acc + illuminate(ws.wavelength, L) / ws.prob / static_cast<float>(spp);
+      const V3 term = illuminate(ws.wavelength, L) / ws.prob / static_cast<float>(spp);
+      // the library's film policy: a sample whose estimate is not finite adds
+      // nothing (the reference's running mean would keep the NaN for good)
+      if (std::isfinite(term.x) && std::isfinite(term.y) && std::isfinite(term.z))
+        acc = acc + term;
+      else
+        ++per[tid].nonfinite;
     }
     lum = lum + acc * sample_weight;
     f[0] = lum.x;
@@ -1460,11 +1466,13 @@ int oracle_render(oracle_scene_t s, const oracle_render_args* a, float* film, ui
       t.shadow += c.shadow;
       t.nodes += c.nodes;
       t.tris += c.tris;
+      t.nonfinite += c.nonfinite;
     }
     stats[0] = t.extend;
     stats[1] = t.shadow;
     stats[2] = t.nodes;
     stats[3] = t.tris;
+    stats[4] = t.nonfinite;
   }
   return 0;
 }

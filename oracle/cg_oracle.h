@@ -81,7 +81,8 @@ typedef struct oracle_render_args {
  * update (compute.wesl:32-62).  film_xyz: W*H*3 floats (in/out running mean),
  * seeds: W*H u32 (in/out, reference mode), both may be updated in place.
  * stats (may be NULL): [0] extend rays, [1] shadow rays, [2] node visits,
- * [3] triangle tests. */
+ * [3] triangle tests, [4] samples whose estimate was not finite (they add
+ * nothing to the film, as in the library). */
 int oracle_render(oracle_scene_t scene, const oracle_render_args* args,
                   float* film_xyz, uint32_t* seeds, uint64_t* stats);
 

@@ -19,12 +19,24 @@ RNG_REFERENCE = 0
 RNG_KEYED = 1
 
 
+def reference_dir() -> str | None:
+    """The reference source tree: $CG_REFERENCE when set, else a `reference`
+    directory beside this repository's; None when neither holds its
+    src/pathtracing/."""
+    for d in (os.environ.get("CG_REFERENCE"),
+              os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")):
+        if d and os.path.isdir(os.path.join(d, "src", "pathtracing")):
+            return os.path.abspath(d)
+    return None
+
+
 def build(reference: bool = True) -> None:
     """Compiles the oracle (and, when the reference tree is present, the
     reference's own alias_table.h into _ref/)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if reference and os.path.isdir("/root/reference/src/pathtracing"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref = reference_dir() if reference else None
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
 
 
 def _abi():
@@ -138,7 +150,7 @@ class OracleScene:
         a.prune = 1 if prune else 0
         if pixel_range is not None:
             a.pixel_begin, a.pixel_end = pixel_range
-        stats = np.zeros(4, np.uint64)
+        stats = np.zeros(5, np.uint64)
         rc = lib().oracle_render(self.h, C.byref(a), film.ctypes.data, seeds.ctypes.data,
                                  stats.ctypes.data)
         assert rc == 0

@@ -91,3 +91,19 @@ def pooled_masked(img, keep, k):
     m = keep[:h - h % k, :w - w % k].reshape(h // k, k, w // k, k, 1).astype(np.float64)
     x = img[:h - h % k, :w - w % k].reshape(h // k, k, w // k, k, c) * m
     return x.sum(axis=(1, 3)) / np.maximum(m.sum(axis=(1, 3)), 1)
+
+
+def keyed_compare(gpu, ora, keep, tol=1e-3):
+    """GPU film vs oracle film rendered from the same keyed sample streams, on
+    X, Y and Z.  Each channel is scaled by the oracle's mean magnitude of that
+    channel over the kept pixels.  Returns (fraction of kept pixel-channels
+    within `tol`, the largest relative difference of a channel's mean, the
+    scaled differences beyond `tol`)."""
+    g = gpu[keep].reshape(-1, 3).astype(np.float64)
+    o = ora[keep].reshape(-1, 3).astype(np.float64)
+    scale = np.maximum(np.abs(o).mean(0), 1e-6)
+    diff = (g - o) / scale
+    close = float((np.abs(diff) <= tol).mean())
+    rel_mean = float(np.max(np.abs(g.mean(0) - o.mean(0)) / scale))
+    far = diff[np.abs(diff) > tol]
+    return close, rel_mean, far

@@ -210,3 +210,27 @@ def test_damaged_documents_fail_cleanly(tmp_path):
     p.write_text('{"asset": {"version": "2.0"}, "s": "\\uZZZZ"}')
     with pytest.raises(B.Error, match="bad unicode escape"):
         B.parse_gltf(str(p))
+
+
+def test_node_hierarchy_must_be_a_forest(tmp_path):
+    """A node listed as the child of two nodes, or parent links that loop, fail
+    the load (cgltf rejects both while parsing and validating).  A diamond
+    chain 40 levels deep, each node naming the next one twice, would otherwise
+    have 2^40 paths from the root."""
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32).tobytes()
+    view = [{"buffer": 0, "byteOffset": 16, "byteLength": 36}]
+    dense = {"bufferView": 2, "componentType": 5126, "count": 3, "type": "VEC3"}
+    doc = _one_triangle_doc(dense, view, pos)
+    doc["nodes"] = [{"mesh": 0, "children": [k + 1, k + 1]} for k in range(40)] + [{"mesh": 0}]
+    with pytest.raises(B.Error, match="has two parents"):
+        _load(tmp_path, doc)
+    doc["nodes"] = [{"mesh": 0}, {"children": [2]}, {"children": [1]}]
+    with pytest.raises(B.Error, match="cycle"):
+        _load(tmp_path, doc)
+    doc["nodes"] = [{"mesh": 0, "children": [0]}]
+    with pytest.raises(B.Error, match="cycle"):
+        _load(tmp_path, doc)
+    # a proper tree still loads: one instance per node that holds the mesh
+    doc["nodes"] = [{"mesh": 0, "children": [1, 2]}, {"mesh": 0}, {"mesh": 0, "children": [3]},
+                    {"mesh": 0}]
+    assert len(_load(tmp_path, doc).instances) == 4
