@@ -376,6 +376,56 @@ def ViewSplit(scene: Scene, camera: Camera | _abi.CgCamera | None = None, group=
     UpdateRgba8()
 
 
+def partition_views(views, world: int) -> list[list[int]]:
+    """Indices of the views each of `world` GPUs renders: longest first, each
+    view to the rank with the fewest samples (width * height * spp) so far,
+    the lower rank on ties.  Deterministic, so every rank computes the same
+    assignment from the same view list with no communication; a view's film
+    does not depend on the views it is batched with (its sample streams are
+    keyed by its seed, pixel and sample), so each rank's films equal a one-GPU
+    batch's."""
+    arr = views if isinstance(views, C.Array) else make_views(views)
+    work = [int(arr[k].width) * int(arr[k].height) * int(arr[k].spp) for k in range(len(arr))]
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in sorted(range(len(work)), key=lambda k: (-work[k], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(k)
+        load[r] += work[k]
+    return [sorted(p) for p in parts]
+
+
+def BatchSplit(scene: Scene, views, group=None):
+    """A batch of views spread over the ranks of a torch.distributed group, one
+    GPU per rank, with no collective: this rank renders its share
+    (partition_views) in one wavefront.  Returns (view indices, films) of this
+    rank's share; the shares of all ranks cover every view exactly once."""
+    import torch.distributed as dist
+    arr = views if isinstance(views, C.Array) else make_views(views)
+    mine = partition_views(arr, dist.get_world_size(group))[dist.get_rank(group)]
+    if not mine:
+        return [], []
+    sub = (_abi.CgViewDesc * len(mine))(*[arr[k] for k in mine])
+    return mine, batch_render(scene, sub)
+
+
+class RequestRouter:
+    """Routes a request stream over `world` GPUs, each running its own Server,
+    with no communication: every rank sees the same stream and routes request
+    k to the rank with the fewest samples routed so far (the lower rank on
+    ties), so all ranks agree on every request's owner and the work stays
+    balanced to within one request."""
+
+    def __init__(self, world: int):
+        self.world = world
+        self.load = [0] * world
+
+    def route(self, width: int, height: int, spp: int) -> int:
+        r = min(range(self.world), key=lambda r: (self.load[r], r))
+        self.load[r] += int(width) * int(height) * int(spp)
+        return r
+
+
 def ReadFilm(fmt: int = _abi.CG_FILM_XYZ32F, out: np.ndarray | None = None) -> np.ndarray:
     conf = _abi.CgConf()
     _check(lib.cg_get_conf(C.byref(conf)))

@@ -1,14 +1,17 @@
 // cg_server.cu — the served form: render requests over resident scenes.
 //
 // A worker thread owns two pipelines ("lanes", each a Renderer with its own
-// stream and ray queues).  Requests wait in a FIFO until their film plus
-// their share of path state fits the HBM budget, then join the active set.
-// Each idle lane gets one wavefront chunk for one scene, made of slices of
-// all that scene's active requests (each gets an equal share of the chunk,
-// the rest is filled first-come first-served), so requests that arrive while
-// others are on the GPU start with the next chunk and share the device with
-// them (continuous batching); with two chunks in flight the host builds and
-// retires chunks while the GPU stays busy.  A request finishes
+// stream and ray queues).  Requests wait until their film plus their share of
+// path state fits the HBM budget, then join the active set; both admission
+// and dispatch go shortest first (fewest samples left), except that a request
+// waiting longer than kAgingSeconds goes before every younger one, oldest
+// first, so large requests are not starved.  Each idle lane gets one
+// wavefront chunk for one scene: the scene of the first request in that
+// order, filled with slices of that scene's active requests in the same
+// order, so requests that arrive while others are on the GPU start with the
+// next chunk and share the device with them (continuous batching); with two
+// chunks in flight the host builds and retires chunks while the GPU stays
+// busy.  A request finishes
 // when its last pixel is resolved: the worker enqueues the film's copy into a
 // pinned staging buffer (a copy-engine transfer, so it does not wait for SMs
 // that the other lane's kernels hold) and goes on dispatching; a copy-out
@@ -108,8 +111,6 @@ struct cg_server_s {
   std::string fatal_msg;
   uint64_t next_id = 1;
   cg_server_stats st{};
-  uint32_t cur_scene = 0;  // scene of the current run of chunks
-  uint32_t run = 0;        // chunks dispatched in that run
   // copy-out thread and its queue; staging buffers and events are reused
   std::thread copier;
   std::mutex copy_mu;
@@ -153,43 +154,44 @@ void finishRequest(cg_server_s& sv, ServerReq* r, int status) {
     ++sv.st.cancelled;
 }
 
-// Chunks of one scene dispatched in a row before the server moves on to the
-// next scene with work.  Both lanes then mostly run chunks of the same scene,
-// whose trees share the L2 (two scenes' trees at once overflow it).
-constexpr uint32_t kSceneRun = 4;
+// Scheduling order (admission and dispatch): a request that has waited
+// longer than this since its submit goes before every younger one, the oldest
+// first; the others go shortest first (fewest samples left to schedule), the
+// older first among equals.  Shortest first finishes the many small requests
+// of a mixed stream early (lower median latency than first come, first
+// served, at the same throughput); the aging bound keeps the tail finite when
+// small requests keep arriving.
+constexpr double kAgingSeconds = 1.0;
 
-// Builds one chunk for one scene in `lane`: the current scene while its run
-// lasts and it has work, else the next scene with work (round robin); an
-// equal share of the chunk for each of the scene's active requests, the rest
-// first come first served.  Returns false when no request has pixels left to
-// schedule.
+uint64_t samplesLeft(const ServerReq* r) {
+  return uint64_t(r->npx - r->next_pixel) * r->req.view.spp;
+}
+
+// True when a goes before b.
+bool schedulesBefore(const ServerReq* a, const ServerReq* b, double now) {
+  const bool aged_a = now - a->submit_s > kAgingSeconds, aged_b = now - b->submit_s > kAgingSeconds;
+  if (aged_a != aged_b) return aged_a;
+  if (aged_a) return a->id < b->id;
+  const uint64_t la = samplesLeft(a), lb = samplesLeft(b);
+  if (la != lb) return la < lb;
+  return a->id < b->id;
+}
+
+// Builds one chunk in `lane` for the scene of the first request in
+// scheduling order, filled with that scene's requests in the same order.
+// Returns false when no request has pixels left to schedule.
 bool buildChunk(cg_server_s* sv, ServerLane& lane, const Caps& caps, SceneDev*& scene_out,
                 ChunkDesc& ch) {
-  const uint32_t nscenes = static_cast<uint32_t>(sv->scenes.size());
-  auto hasWork = [&](uint32_t s) {
-    for (ServerReq* r : sv->active)
-      if (r->req.scene == s && !r->cancelled && r->next_pixel < r->npx) return true;
-    return false;
-  };
-  uint32_t scene_idx = UINT32_MAX;
-  if (sv->run < kSceneRun && hasWork(sv->cur_scene)) {
-    scene_idx = sv->cur_scene;
-  } else {
-    for (uint32_t k = 1; k <= nscenes && scene_idx == UINT32_MAX; ++k) {
-      const uint32_t s = (sv->cur_scene + k) % nscenes;
-      if (hasWork(s)) scene_idx = s;
-    }
-    if (scene_idx == UINT32_MAX) return false;
-    sv->cur_scene = scene_idx;
-    sv->run = 0;
-  }
-  ++sv->run;
+  std::vector<ServerReq*> order;
+  for (ServerReq* r : sv->active)
+    if (!r->cancelled && r->next_pixel < r->npx) order.push_back(r);
+  if (order.empty()) return false;
+  const double now = nowSeconds();
+  std::sort(order.begin(), order.end(),
+            [now](const ServerReq* a, const ServerReq* b) { return schedulesBefore(a, b, now); });
+  const uint32_t scene_idx = order.front()->req.scene;
   SceneDev& scene = *sv->scenes[scene_idx];
   const uint32_t cap = lane.rend.chunkSamples(scene, caps);
-  std::vector<ServerReq*> mine;
-  for (ServerReq* r : sv->active)
-    if (r->req.scene == scene_idx && !r->cancelled && r->next_pixel < r->npx) mine.push_back(r);
-  const uint32_t share = std::max<uint32_t>(1u, cap / static_cast<uint32_t>(mine.size()));
   lane.slices.clear();
   lane.slice_req.clear();
   uint32_t used = 0;
@@ -216,8 +218,8 @@ bool buildChunk(cg_server_s* sv, ServerLane& lane, const Caps& caps, SceneDev*& 
     r->next_pixel += px;
     used += px * spp;
   };
-  for (ServerReq* r : mine) take(r, share);
-  for (ServerReq* r : mine) take(r, cap);
+  for (ServerReq* r : order)
+    if (r->req.scene == scene_idx) take(r, cap);
   layoutViews(lane.slices);
   ch = ChunkDesc{0, 0, used, 0};
   for (const ViewDev& v : lane.slices) ch.pixel_count += v.pixel_count;
@@ -423,11 +425,18 @@ void serverLoop(cg_server_s* sv) {
   double all_since = 0.0;   // start of the current stretch with every lane busy
   std::unique_lock<std::mutex> lk(sv->mu);
   while (true) {
-    // ---- admission (FIFO under the HBM budget) ----
+    // ---- admission under the HBM budget, in scheduling order ----
     while (!sv->pending.empty()) {
-      ServerReq* r = sv->pending.front();
+      auto pick = sv->pending.begin();
+      const double now = nowSeconds();
+      for (auto it = sv->pending.begin(); it != sv->pending.end(); ++it)
+        if ((*it)->cancelled || schedulesBefore(*it, *pick, now)) {
+          pick = it;
+          if ((*it)->cancelled) break;
+        }
+      ServerReq* r = *pick;
       if (r->cancelled) {
-        sv->pending.pop_front();
+        sv->pending.erase(pick);
         r->bytes = 0;
         finishRequest(*sv, r, CG_E_CANCELLED);
         sv->done_cv.notify_all();
@@ -435,15 +444,17 @@ void serverLoop(cg_server_s* sv) {
       }
       if (sv->st.bytes_in_use + r->bytes > sv->budget) {
         // wait for memory held by active requests or films being copied out
+        // (the first request in order keeps its place, so it is not passed
+        // over for ever by smaller ones)
         if (r->bytes <= sv->budget && sv->st.bytes_in_use > 0) break;
-        sv->pending.pop_front();  // can never fit
+        sv->pending.erase(pick);  // can never fit
         r->bytes = 0;
         ++sv->st.rejected;
         finishRequest(*sv, r, CG_E_OOM);
         sv->done_cv.notify_all();
         continue;
       }
-      sv->pending.pop_front();
+      sv->pending.erase(pick);
       const size_t fb = size_t(r->npx) * 16;
       void* film = nullptr;
       if (cudaMallocAsync(&film, fb, sv->alloc_stream) != cudaSuccess ||
@@ -684,6 +695,8 @@ CG_API int cg_server_submit(cg_server_t server, const cg_request* request, float
     SceneDev& scene = *server->scenes[request->scene];
     if (v.spp > server->lanes[0].rend.chunkSamples(scene, capsOf(server->conf)))
       return fail(CG_E_INVALID, "spp exceeds the wavefront chunk");
+    if (uint64_t(v.width) * v.height > 0xffffffffull)
+      return fail(CG_E_INVALID, "view has more than 2^32 - 1 pixels");
     auto r = std::make_unique<ServerReq>();
     r->req = *request;
     r->out = film_xyz;

@@ -446,11 +446,14 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views,
  * their film plus path-state bytes fit the HBM budget, batched with the work
  * already on the GPU at chunk granularity (continuous batching), and
  * completed independently: a copy-out thread writes each finished film into
- * the caller's buffer while the GPU goes on with other requests.  Chunks of
- * one scene run in short runs (both lanes on the same scene's trees) before
- * the next scene with work gets its turn.  Per-request sample streams are keyed by
- * (request seed, pixel, sample), so a request's result does not depend on
- * what it was batched with. */
+ * the caller's buffer while the GPU goes on with other requests.  Admission
+ * and dispatch go shortest first (fewest samples left), except that a request
+ * that has waited more than one second since its submit goes before every
+ * younger one (oldest first), so a stream of small requests cannot starve a
+ * large one.  A chunk holds one scene: that of the first request in this
+ * order, filled with the scene's requests in the same order.  Per-request
+ * sample streams are keyed by (request seed, pixel, sample), so a request's
+ * result does not depend on what it was batched with or when it ran. */
 typedef struct cg_server_s* cg_server_t;
 typedef struct cg_request {
   uint32_t scene;       /* index into the server's scene list */

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <chrono>
 #include <thread>
 #include <vector>
 
@@ -94,6 +95,9 @@ struct oracle_scene_s {
   float total_weight = 0.0f;
   uint32_t env_w = 0, env_h = 0;
   std::vector<float> env;
+  // single-threaded seconds of each host packing stage of the create call:
+  // BLAS builds, TLAS build, emissive buffer, alias table
+  double pack_s[4] = {0, 0, 0, 0};
 };
 
 namespace oracle {
@@ -941,11 +945,12 @@ float lightPdf(const oracle_scene_s& s, V3 next, const SurfacePos& sp) {
 struct EmissionDraw {
   V3 next;
   float prob, radiance, expected_dist;
+  uint32_t prim;  // the emissive primitive drawn
 };
 // sample (pdf/emission.wesl:32-82) with sampleEmissivePrim (:181-191); a bin
 // of u32(1.0 * N) is clamped to N - 1 (WGSL robust access).
 EmissionDraw emissionSample(const oracle_scene_s& s, float w, const SurfacePos& sp, Rng& rng) {
-  if (s.alias.empty()) return {V3{0, 0, 0}, 0.0f, 0.0f, 0.0f};
+  if (s.alias.empty()) return {V3{0, 0, 0}, 0.0f, 0.0f, 0.0f, 0u};
   uint32_t n = static_cast<uint32_t>(s.alias.size());
   uint32_t bin = static_cast<uint32_t>(randFloat(rng) * static_cast<float>(n));
   if (bin >= n) bin = n - 1u;
@@ -965,7 +970,7 @@ EmissionDraw emissionSample(const oracle_scene_s& s, float w, const SurfacePos& 
   float lp = std::fabs(dot(ln, -next));
   float area_pdf = wmax(prim.weight / prim.area, EPDF_EPS);
   float sapdf = area_pdf * dsq / wmax(lp, EPDF_EPS);
-  return {next, sapdf, rgbToWavelengthRadiance(ev(prim.emission), w), std::sqrt(dsq)};
+  return {next, sapdf, rgbToWavelengthRadiance(ev(prim.emission), w), std::sqrt(dsq), pi};
 }
 
 // ---- sample counts (shading/sample.wesl:151-299, lod.wesl) -------------------------
@@ -1049,10 +1054,14 @@ float balanceDenominator(const oracle_scene_s& s, V3 curr, V3 next, const Surfac
 struct TransportSample {
   V3 dir;
   float coeff;
+  int model;    // the lobe that drew it
+  float denom;  // its balance-heuristic denominator
 };
 struct EmissionSampleOut {
   V3 dir;
   float radiance, expected_dist;
+  uint32_t prim;      // the emissive primitive drawn
+  float sproj, denom; // |cos| at the surface, balance-heuristic denominator
 };
 struct Sample {
   uint32_t transport_count = 0, emission_count = 0;
@@ -1065,8 +1074,8 @@ Sample sampleModels(const oracle_scene_s& s, V3 curr, float w, const SurfacePos&
                     const MatEval& m, const Counts& c, Rng& rng) {
   Sample res;
   auto add = [&](V3 dir, int model, float prob, float dist) {
-    float coeff = dist / balanceDenominator(s, curr, dir, sp, m, c, model, prob, -1.0f);
-    res.ts[res.transport_count++] = TransportSample{dir, coeff};
+    float denom = balanceDenominator(s, curr, dir, sp, m, c, model, prob, -1.0f);
+    res.ts[res.transport_count++] = TransportSample{dir, dist / denom, model, denom};
   };
   for (uint32_t i = 0; i < c.diffuse; ++i) {  // pdf/diffuse.wesl:7-36
     V3 macro = orientedNormal(curr, sp.shading_norm);
@@ -1114,9 +1123,10 @@ Sample sampleModels(const oracle_scene_s& s, V3 curr, float w, const SurfacePos&
     float sproj = std::fabs(dot(sp.shading_norm, d.next));
     float ec = diffuseDist(curr, d.next, sp, m) + roughReflectDist(curr, d.next, sp, m) +
                roughTransmitDist(curr, d.next, sp, m);
-    float rad = d.radiance * ec * sproj /
-                balanceDenominator(s, curr, d.next, sp, m, c, M_NONE, -1.0f, d.prob);
-    res.es[res.emission_count++] = EmissionSampleOut{d.next, rad, d.expected_dist};
+    float denom = balanceDenominator(s, curr, d.next, sp, m, c, M_NONE, -1.0f, d.prob);
+    float rad = d.radiance * ec * sproj / denom;
+    res.es[res.emission_count++] =
+        EmissionSampleOut{d.next, rad, d.expected_dist, d.prim, sproj, denom};
   }
   return res;
 }
@@ -1184,6 +1194,109 @@ float trace(TraceCtx& tc, const Ray& ray, float w, int depth, uint32_t key) {
   for (uint32_t i = 0; i < smp.transport_count; ++i) rad += smp.ts[i].coeff * child_l[i];
   for (uint32_t i = 0; i < smp.emission_count; ++i) rad += smp.es[i].radiance;
   return emission + rad;
+}
+
+// ---- hero-wavelength mode -------------------------------------------------------
+// The same sample tree, drawn at the hero wavelength w[0] (material, sample
+// counts, directions and balance-heuristic denominators), carries the
+// radiance of all four wavelengths: a child's coefficient for wavelength j is
+// the lobe's value at w[j] over the hero's denominator.  The reference's
+// estimator weighs each lobe's sample by that lobe alone over the balance
+// denominator (sample.wesl:452-501), so its expected value depends on the
+// sample counts and pdfs at the wavelength; where they are the same at all
+// four wavelengths, the hero's tree gives each wavelength the reference's
+// expectation.  At a hit where they are not (a lobe whose heuristic vanishes
+// at some of the four, e.g. a reflectance of 0 in the Smits table's deep-red
+// gap, or a transmission whose refraction index varies with the wavelength),
+// the light sample and the subtree carry the hero alone with weight 4: over
+// the four equally likely heroes of the same wavelength set that is the
+// reference's estimator at each of them.  Emission is exact per wavelength.
+struct L4 {
+  float v[HERO_COUNT];
+};
+
+float lobeDist(int model, V3 curr, V3 next, const SurfacePos& sp, const MatEval& m) {
+  switch (model) {
+    case M_DIFFUSE: return diffuseDist(curr, next, sp, m);
+    case M_SREFL: return specularReflectDist(curr, next, sp, m);
+    case M_RREFL: return roughReflectDist(curr, next, sp, m);
+    case M_STRANS: return specularTransmitDist(curr, next, sp, m);
+    case M_RTRANS: return roughTransmitDist(curr, next, sp, m);
+  }
+  return 0.0f;
+}
+
+bool sameCounts(const Counts& a, const Counts& b) {
+  return a.diffuse == b.diffuse && a.specular_reflect == b.specular_reflect &&
+         a.rough_reflect == b.rough_reflect && a.specular_transmit == b.specular_transmit &&
+         a.rough_transmit == b.rough_transmit && a.light == b.light;
+}
+
+L4 traceHero(TraceCtx& tc, const Ray& ray, const float (&w)[HERO_COUNT], int depth, uint32_t key,
+             bool hero_only) {
+  const oracle_scene_s& s = *tc.s;
+  L4 out{};
+  ++tc.cnt.extend;
+  HitInfo hi = rayHit(s, ray, tc.prune, tc.cnt);
+  if (!hi.hit) {
+    for (int j = 0; j < HERO_COUNT; ++j)
+      out.v[j] = (j == 0 || !hero_only) ? envRadiance(s, ray.dir, w[j]) : 0.0f;
+    return out;
+  }
+  uint32_t trace_depth = std::max(1u, std::min(tc.conf.trace_depth, 64u));
+  if (depth >= static_cast<int>(tc.conf.trace_depth) ||
+      static_cast<uint32_t>(depth) >= trace_depth - 1u)
+    return out;
+  Rng node_rng;
+  Rng* rng = tc.seq;
+  if (tc.keyed) {
+    seedRng(node_rng, key);
+    rng = &node_rng;
+  }
+  const Material& mat = s.materials[hi.sp.material_idx];
+  MatEval m[HERO_COUNT];
+  for (int j = 0; j < HERO_COUNT; ++j) m[j] = decode(s, mat, hi.sp.uv, w[j]);
+  Counts c = counts(m[0], !s.alias.empty(), depth, tc.conf);
+  Sample smp = sampleModels(s, ray.dir, w[0], hi.sp, m[0], c, *rng);
+  // the four wavelengths share the hero's counts and pdfs here
+  bool uniform = !hero_only;
+  for (int j = 1; j < HERO_COUNT && uniform; ++j) {
+    uniform = sameCounts(counts(m[j], !s.alias.empty(), depth, tc.conf), c);
+    if ((c.specular_transmit || c.rough_transmit) && m[j].ior.re != m[0].ior.re) uniform = false;
+  }
+  const float k = (uniform || hero_only) ? 1.0f : static_cast<float>(HERO_COUNT);
+  for (int j = 0; j < HERO_COUNT; ++j)
+    out.v[j] = (j == 0 || !hero_only) ? m[j].emission : 0.0f;
+  for (uint32_t i = 0; i < smp.emission_count; ++i) {
+    const auto& es = smp.es[i];
+    V3 light_pos = hi.sp.pos + es.dir * es.expected_dist;
+    Ray shadow = spawnSurfaceRay(hi.sp, es.dir);
+    float expected = distance(shadow.pos, light_pos);
+    ++tc.cnt.shadow;
+    HitInfo sh = rayHit(s, shadow, tc.prune, tc.cnt);
+    if (sh.hit && sh.dist < (expected - 1e-3f)) continue;
+    // es.radiance is the hero's whole light-sample term already
+    out.v[0] += k * es.radiance;
+    if (!uniform) continue;
+    const cg_emissive_prim& prim = s.eprims[es.prim];
+    for (int j = 1; j < HERO_COUNT; ++j) {
+      float radiance = rgbToWavelengthRadiance(ev(prim.emission), w[j]);
+      float ec = diffuseDist(ray.dir, es.dir, hi.sp, m[j]) +
+                 roughReflectDist(ray.dir, es.dir, hi.sp, m[j]) +
+                 roughTransmitDist(ray.dir, es.dir, hi.sp, m[j]);
+      out.v[j] += radiance * ec * es.sproj / es.denom;
+    }
+  }
+  for (uint32_t i = 0; i < smp.transport_count; ++i) {
+    const TransportSample& t = smp.ts[i];
+    Ray child = spawnSurfaceRay(hi.sp, t.dir);
+    L4 cl = traceHero(tc, child, w, depth + 1, tc.keyed ? childKey(key, i) : 0u, !uniform);
+    out.v[0] += t.coeff * k * cl.v[0];
+    if (!uniform) continue;
+    for (int j = 1; j < HERO_COUNT; ++j)
+      out.v[j] += lobeDist(t.model, ray.dir, t.dir, hi.sp, m[j]) / t.denom * cl.v[j];
+  }
+  return out;
 }
 
 // cameraRay (compute.wesl:64-79)
@@ -1287,7 +1400,14 @@ oracle_scene_t oracle_scene_create(const cg_scene_desc* d) {
       }
     }
   }
+  using Clock = std::chrono::steady_clock;
+  auto seconds = [](Clock::time_point a) {
+    return std::chrono::duration<double>(Clock::now() - a).count();
+  };
+  auto t0 = Clock::now();
   for (const auto& mesh : s->meshes) blasBuildMesh(*s, mesh);
+  s->pack_s[0] = seconds(t0);
+  t0 = Clock::now();
   // TLAS over instances in scene order (tlas.h:34-77)
   std::vector<BoundedPrimitive> bp;
   for (size_t i = 0; i < s->inst_desc.size(); ++i) {
@@ -1312,11 +1432,16 @@ oracle_scene_t oracle_scene_create(const cg_scene_desc* d) {
     s->tnodes.emplace_back();
     tlasBuild(*s, 0, 0, static_cast<uint32_t>(bp.size()), bp);
   }
+  s->pack_s[1] = seconds(t0);
+  t0 = Clock::now();
   buildEmissive(*s);
+  s->pack_s[2] = seconds(t0);
+  t0 = Clock::now();
   std::vector<double> w;
   for (const auto& e : s->eprims) w.push_back(static_cast<double>(e.weight));
   s->alias.resize(w.size());
   aliasBuild(w.data(), static_cast<uint32_t>(w.size()), s->alias.data());
+  s->pack_s[3] = seconds(t0);
   // environment (scene_data.h:57-98)
   if (d->env_rgba32f && d->env_width && d->env_height) {
     s->env_w = d->env_width;
@@ -1342,6 +1467,12 @@ oracle_scene_t oracle_scene_create(const cg_scene_desc* d) {
 }
 
 void oracle_scene_destroy(oracle_scene_t s) { delete s; }
+
+int oracle_scene_pack_seconds(oracle_scene_t s, double* out) {
+  if (!s || !out) return -1;
+  std::memcpy(out, s->pack_s, sizeof(s->pack_s));
+  return 0;
+}
 
 uint32_t oracle_emissive_count(oracle_scene_t s) {
   return s ? static_cast<uint32_t>(s->eprims.size()) : 0u;
@@ -1430,18 +1561,29 @@ int oracle_render(oracle_scene_t s, const oracle_render_args* a, float* film, ui
     // render (render.wesl:7-18)
     V3 acc{0.0f, 0.0f, 0.0f};
     for (uint32_t i = 0; i < spp; ++i) {
-      WavelengthSample ws;
+      float u = 0.0f;
       uint32_t key = 0;
       if (tc.keyed) {
         key = sampleKey(a->seed, a->iter_count, pix, i);
         Rng wr;
         seedRng(wr, wavelengthKey(key));
-        ws = sampleWavelengthCdf(randFloat(wr));
+        u = randFloat(wr);
       } else {
-        ws = sampleWavelengthCdf(randFloat(seq));
+        u = randFloat(seq);
       }
-      float L = trace(tc, ray, ws.wavelength, 0, key);
-      const V3 term = illuminate(ws.wavelength, L) / ws.prob / static_cast<float>(spp);
+      V3 term;
+      if (a->spectral == ORACLE_SPECTRAL_HERO) {
+        float w[HERO_COUNT];
+        heroWavelengths(u, w);
+        const L4 L = traceHero(tc, ray, w, 0, key, false);
+        V3 est{0.0f, 0.0f, 0.0f};
+        for (int j = 0; j < HERO_COUNT; ++j) est = est + illuminate(w[j], L.v[j]);
+        term = est * (HERO_SPAN / HERO_COUNT) / static_cast<float>(spp);
+      } else {
+        const WavelengthSample ws = sampleWavelengthCdf(u);
+        float L = trace(tc, ray, ws.wavelength, 0, key);
+        term = illuminate(ws.wavelength, L) / ws.prob / static_cast<float>(spp);
+      }
       // the library's film policy: a sample whose estimate is not finite adds
       // nothing (the reference's running mean would keep the NaN for good)
       if (std::isfinite(term.x) && std::isfinite(term.y) && std::isfinite(term.z))

@@ -36,6 +36,12 @@ typedef struct oracle_scene_s* oracle_scene_t;
  * alias table (alias_table.h), environment (scene_data.h:57-98). */
 oracle_scene_t oracle_scene_create(const cg_scene_desc* desc);
 void oracle_scene_destroy(oracle_scene_t scene);
+/* Single-threaded seconds the create call spent in each host packing stage,
+ * as the reference runs them on the host (src/environment.cpp:69-74): [0] the
+ * median-split BLAS builds (blas.h:112-194, one per mesh), [1] the TLAS build
+ * (tlas.h:98-140), [2] the emissive buffer (emissive_buffer.h:44-100), [3]
+ * the alias table (alias_table.h:26-70). */
+int oracle_scene_pack_seconds(oracle_scene_t scene, double* out);
 
 uint32_t oracle_emissive_count(oracle_scene_t scene);
 /* Copies the emissive prims, alias entries and the float total weight. */
@@ -63,6 +69,18 @@ enum {
                                streams the CUDA kernels use */
 };
 
+enum {
+  ORACLE_SPECTRAL_REFERENCE = 0, /* one wavelength per sample, importance-sampled
+                                    by bisection of the CIE-sum CDF on
+                                    [380, 720] (physics/wavelength.wesl:20-45) */
+  ORACLE_SPECTRAL_HERO = 1       /* four wavelengths per sample: a hero uniform
+                                    on [380, 780] and three rotated by 100 nm;
+                                    directions follow the hero, the others
+                                    weigh the same paths, and a refraction
+                                    whose index varies across the four keeps
+                                    the hero alone (weight x 4) below it     */
+};
+
 typedef struct oracle_render_args {
   cg_conf conf;            /* render size, spp, depth, sample caps          */
   cg_camera camera;
@@ -74,7 +92,7 @@ typedef struct oracle_render_args {
                               except exact ties; faster), 0 = as reference  */
   uint32_t pixel_begin, pixel_end;  /* render only this pixel range
                               (end 0 = all); other pixels are left as is  */
-  uint32_t _pad;
+  uint32_t spectral;       /* ORACLE_SPECTRAL_*                             */
 } oracle_render_args;
 
 /* One View() frame: for every pixel, render() + film update + rng seed

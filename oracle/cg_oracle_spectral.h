@@ -101,6 +101,23 @@ inline WavelengthSample sampleWavelengthCdf(float cdf_sample) {
   return {wavelength, wmax(xyzMatchSum(wavelength) / total_match, 1e-6f)};
 }
 
+// ---- hero-wavelength sampling (an option beside the reference's sampler) -----
+// Four wavelengths per sample: the hero uniform on [380, 780] nm from one
+// random number, the others rotated by a quarter of the range each (Wilkie et
+// al. 2014, "Hero Wavelength Spectral Sampling").  Each is uniform on the
+// range, so a sample's estimate is (1/4) sum_j illuminate(w_j, L_j) / (1/400).
+constexpr int HERO_COUNT = 4;
+constexpr float HERO_MIN = 380.0f;
+constexpr float HERO_SPAN = 400.0f;
+inline void heroWavelengths(float u, float (&w)[HERO_COUNT]) {
+  const float x0 = HERO_SPAN * u;  // offset of the hero in the range
+  for (int j = 0; j < HERO_COUNT; ++j) {
+    float x = x0 + (HERO_SPAN / HERO_COUNT) * static_cast<float>(j);
+    if (x >= HERO_SPAN) x = x - HERO_SPAN;
+    w[j] = HERO_MIN + x;
+  }
+}
+
 // ---- physics/luminance.wesl:13-16 ------------------------------------------
 inline V3 illuminate(float wavelength, float radiance) {
   float average_integral = xyzMatchSumIntegral(380.0f, 720.0f) / 3.0f;

@@ -17,6 +17,8 @@ REF_ALIAS_PATH = os.path.join(HERE, "_ref", "libref_alias.so")
 
 RNG_REFERENCE = 0
 RNG_KEYED = 1
+SPECTRAL_REFERENCE = 0
+SPECTRAL_HERO = 1
 
 
 def reference_dir() -> str | None:
@@ -66,11 +68,12 @@ def lib():
                            ("iter_count", C.c_uint32), ("rng_mode", C.c_uint32),
                            ("seed", C.c_uint32), ("threads", C.c_uint32), ("prune", C.c_uint32),
                            ("pixel_begin", C.c_uint32), ("pixel_end", C.c_uint32),
-                           ("_pad", C.c_uint32)]
+                           ("spectral", C.c_uint32)]
     L = C.CDLL(LIB_PATH)
     L.oracle_scene_create.restype = C.c_void_p
     L.oracle_scene_create.argtypes = [C.POINTER(abi.CgSceneDesc)]
     L.oracle_scene_destroy.argtypes = [C.c_void_p]
+    L.oracle_scene_pack_seconds.argtypes = [C.c_void_p, C.c_void_p]
     L.oracle_emissive_count.restype = C.c_uint32
     L.oracle_emissive_count.argtypes = [C.c_void_p]
     L.oracle_emissive.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]
@@ -114,6 +117,14 @@ class OracleScene:
         except Exception:
             pass
 
+    def pack_seconds(self) -> dict:
+        """Single-threaded seconds of the host packing stages the create call
+        ran, as the reference runs them on the host: median-split BLAS builds,
+        TLAS build, emissive buffer, alias table."""
+        out = np.zeros(4, np.float64)
+        assert lib().oracle_scene_pack_seconds(self.h, out.ctypes.data) == 0
+        return dict(zip(("blas", "tlas", "emissive", "alias"), map(float, out)))
+
     def emissive(self):
         abi = _abi()
         n = lib().oracle_emissive_count(self.h)
@@ -134,7 +145,7 @@ class OracleScene:
         return hits, t2
 
     def render(self, conf, camera, film=None, seeds=None, iter_count=0, rng=RNG_KEYED, seed=0,
-               threads=0, prune=False, pixel_range=None):
+               threads=0, prune=False, pixel_range=None, spectral=SPECTRAL_REFERENCE):
         W, H = conf.render_width, conf.render_height
         if film is None:
             film = np.zeros((H, W, 3), np.float32)
@@ -148,6 +159,7 @@ class OracleScene:
         a.seed = seed
         a.threads = threads
         a.prune = 1 if prune else 0
+        a.spectral = spectral
         if pixel_range is not None:
             a.pixel_begin, a.pixel_end = pixel_range
         stats = np.zeros(5, np.uint64)

@@ -99,3 +99,44 @@ def test_view_split_in_a_one_rank_nccl_group(scene_pair):
         assert _close(B.ReadFilm(), full) < RTOL
     finally:
         dist.destroy_process_group()
+
+
+def test_batch_shares_render_the_films_of_the_whole_batch(scene_pair):
+    """The views of a batch split over two ranks (partition_views), each share
+    rendered as its own batch one after the other on this GPU, give every
+    view the film the whole batch gives it."""
+    _, g = scene_pair[1]
+    views = [(p, d, max(8, w // 16), max(8, h // 16), spp, seed)
+             for p, d, w, h, spp, seed in scenes.batch_views(24, seed=12)]
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=4))
+    whole = B.batch_render(g, views)
+    parts = B.partition_views(views, 2)
+    assert sorted(parts[0] + parts[1]) == list(range(len(views))) and parts[0] and parts[1]
+    for part in parts:
+        films = B.batch_render(g, [views[k] for k in part])
+        for k, f in zip(part, films):
+            assert _close(f, whole[k]) < RTOL, k
+
+
+def test_routed_requests_render_the_films_of_one_server(scene_pair):
+    """A request stream routed over two ranks (RequestRouter), each rank's
+    requests served by its own server (one after the other on this GPU),
+    gives every request the film one server gives it."""
+    gs = [g for _, g in scene_pair]
+    stream = [(t, si % 2, p, d, w // 8, h // 8, spp, seed)
+              for t, si, p, d, w, h, spp, seed in scenes.request_stream(12, 100.0, seed=13)]
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=16, trace_depth=4))
+
+    def serve(reqs):
+        with B.Server(gs, 8 << 30) as sv:
+            ids = [sv.submit(si, p, d, w, h, spp, seed) for _, si, p, d, w, h, spp, seed in reqs]
+            return [sv.wait(i)[0] for i in ids]
+
+    one = serve(stream)
+    router = B.RequestRouter(2)
+    owner = [router.route(w, h, spp) for _, _, _, _, w, h, spp, _ in stream]
+    assert set(owner) == {0, 1}
+    for rank in (0, 1):
+        ks = [k for k in range(len(stream)) if owner[k] == rank]
+        for k, f in zip(ks, serve([stream[k] for k in ks])):
+            assert _close(f, one[k]) < RTOL, k
