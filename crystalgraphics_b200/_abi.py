@@ -17,6 +17,7 @@ CG_E_DEVICE = -6
 CG_E_CANCELLED = -7
 CG_E_BUSY = -8
 
+CG_SPECTRAL_REFERENCE, CG_SPECTRAL_HERO = 0, 1
 CG_FILM_XYZ32F = 0
 CG_FILM_RGBA8 = 1
 CG_FILM_RGB32F = 2

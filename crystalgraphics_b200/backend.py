@@ -68,6 +68,8 @@ def _load():
         "cg_last_stats": (i, [C.POINTER(_abi.CgStats)]),
         "cg_set_counting": (i, [i]),
         "cg_set_seed": (i, [u32]),
+        "cg_set_spectral": (i, [i]),
+        "cg_get_spectral": (i, [C.POINTER(C.c_int)]),
         "cg_set_profiling": (i, [i]),
         "cg_profile_read": (i, [C.POINTER(_abi.CgProfile)]),
         "cg_trace_closest": (i, [vp, vp, u32, vp]),
@@ -471,6 +473,18 @@ def ReadProfile() -> dict:
 
 def SetSeed(seed: int) -> None:
     _check(lib.cg_set_seed(seed))
+
+
+def SetSpectral(mode: int) -> None:
+    """_abi.CG_SPECTRAL_REFERENCE (the reference's one wavelength per sample)
+    or _abi.CG_SPECTRAL_HERO (four wavelengths per sample)."""
+    _check(lib.cg_set_spectral(mode))
+
+
+def GetSpectral() -> int:
+    m = C.c_int()
+    _check(lib.cg_get_spectral(C.byref(m)))
+    return m.value
 
 
 def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_width=0,

@@ -271,10 +271,15 @@ void Renderer::adoptBuffers(Renderer& prev) {
   std::swap(wl_const, prev.wl_const);
   std::swap(wave_arena.base, prev.wave_arena.base);
   std::swap(wave_arena.size, prev.wave_arena.size);
+  std::swap(hero_arena.base, prev.hero_arena.base);
+  std::swap(hero_arena.size, prev.hero_arena.size);
   std::swap(wave, prev.wave);
+  std::swap(hero, prev.hero);
   for (int k = 0; k < kMaxPipelines - 1; ++k) {
     std::swap(xwave_arena[k].base, prev.xwave_arena[k].base);
     std::swap(xwave_arena[k].size, prev.xwave_arena[k].size);
+    std::swap(xhero_arena[k].base, prev.xhero_arena[k].base);
+    std::swap(xhero_arena[k].size, prev.xhero_arena[k].size);
     std::swap(xwave[k], prev.xwave[k]);
   }
 }
@@ -285,8 +290,10 @@ Renderer::~Renderer() {
     if (x) cudaStreamSynchronize(x);
   for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
   wave_arena.release();
+  hero_arena.release();
   for (int k = 0; k < kMaxPipelines - 1; ++k) {
     xwave_arena[k].release();
+    xhero_arena[k].release();
     if (xjoin_ev[k]) cudaEventDestroy(xjoin_ev[k]);
     if (xstream[k]) cudaStreamDestroy(xstream[k]);
   }
@@ -350,15 +357,59 @@ int allocWave(DeviceArena& arena, WaveBuffers& w, uint32_t capacity) {
 }
 }  // namespace
 
+// The hero-wavelength buffers of one queue set: per queued ray (both queues)
+// and per shadow ray a float4, per sample slot a float4.
+int attachHero(DeviceArena& arena, WaveBuffers& w) {
+  const size_t Q = w.capacity, S = w.sample_capacity;
+  const size_t q16 = align256(Q * 16);
+  int rc = arena.alloc(3 * q16 + align256(S * 16));
+  if (rc != CG_OK) return rc;
+  char* p = static_cast<char*>(arena.base);
+  w.ray_w[0] = reinterpret_cast<float4*>(p);
+  w.ray_w[1] = reinterpret_cast<float4*>(p + q16);
+  w.sh_w = reinterpret_cast<float4*>(p + 2 * q16);
+  w.s_L4 = reinterpret_cast<float4*>(p + 3 * q16);
+  w.hero = 1u;
+  return CG_OK;
+}
+
+void detachHero(DeviceArena& arena, WaveBuffers& w) {
+  arena.release();
+  w.ray_w[0] = w.ray_w[1] = w.sh_w = w.s_L4 = nullptr;
+  w.hero = 0u;
+}
+
+int Renderer::syncHero() {
+  auto one = [&](DeviceArena& queues, DeviceArena& extra, WaveBuffers& w) -> int {
+    if (!queues.base) return CG_OK;
+    if (hero && !w.hero) return attachHero(extra, w);
+    if (!hero && w.hero) detachHero(extra, w);
+    return CG_OK;
+  };
+  if (!hero) {  // buffers in use by queued work stay until it is done
+    if (stream) CG_CUDA(cudaStreamSynchronize(stream));
+    for (cudaStream_t x : xstream)
+      if (x) CG_CUDA(cudaStreamSynchronize(x));
+  }
+  int rc = one(wave_arena, hero_arena, wave);
+  for (int k = 0; k < kMaxPipelines - 1 && rc == CG_OK; ++k)
+    rc = one(xwave_arena[k], xhero_arena[k], xwave[k]);
+  return rc;
+}
+
 int Renderer::ensureWave(uint32_t capacity) {
-  if (wave_arena.base && wave.capacity == capacity) return CG_OK;
+  if (wave_arena.base && wave.capacity == capacity) return syncHero();
   if (stream) CG_CUDA(cudaStreamSynchronize(stream));
   for (int k = 0; k < kMaxPipelines - 1; ++k) {  // the extra sets follow the first one's capacity
     if (xstream[k]) CG_CUDA(cudaStreamSynchronize(xstream[k]));
     xwave_arena[k].release();
+    xhero_arena[k].release();
     xwave[k] = WaveBuffers{};
   }
-  return allocWave(wave_arena, wave, capacity);
+  hero_arena.release();
+  const int rc = allocWave(wave_arena, wave, capacity);
+  if (rc != CG_OK) return rc;
+  return syncHero();
 }
 
 int Renderer::ensurePipelines(int count) {
@@ -369,8 +420,13 @@ int Renderer::ensurePipelines(int count) {
       CG_CUDA(cudaEventCreateWithFlags(&xjoin_ev[k], cudaEventDisableTiming));
     }
     if (!(xwave_arena[k].base && xwave[k].capacity == wave.capacity)) {
-      const int rc = allocWave(xwave_arena[k], xwave[k], wave.capacity);
+      xhero_arena[k].release();
+      int rc = allocWave(xwave_arena[k], xwave[k], wave.capacity);
       if (rc != CG_OK) return rc;
+      if (hero) {
+        rc = attachHero(xhero_arena[k], xwave[k]);
+        if (rc != CG_OK) return rc;
+      }
     }
   }
   return CG_OK;
@@ -402,6 +458,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.shade_sort = tuning.shade_sort == 2u   ? kShadeSortNone
                   : tuning.shade_sort == 3u ? kShadeSortBlock
                                             : kShadeSortGlobal;
+  if (wb.hero) ls.shade_sort = kShadeSortGlobal;  // the hero kernels take the level-wide order
   profBegin(CG_K_GEN, s);
   launchGen(fc, wb, ch, s);
   profEnd(s);
@@ -628,6 +685,9 @@ static int createEnv(const cg_conf& conf_in, int device, std::unique_ptr<Env>& o
     env->adoptBuffers(*prev);
   }
   int rc = env->init(device);
+  if (rc != CG_OK) return rc;
+  env->hero = false;  // a new environment samples like the reference until told otherwise
+  rc = env->syncHero();
   if (rc != CG_OK) return rc;
   const size_t npx = size_t(env->conf.render_width) * env->conf.render_height;
   CG_CUDA(cudaMalloc(&env->film, npx * sizeof(float4)));
@@ -1106,6 +1166,35 @@ CG_API int cg_set_seed(uint32_t seed) {
     std::lock_guard<std::mutex> lk(g_env_mu);
     if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
     g_env->seed = seed;
+    return CG_OK;
+  });
+}
+
+CG_API int cg_set_spectral(int mode) {
+  return guarded([&]() -> int {
+    if (mode != CG_SPECTRAL_REFERENCE && mode != CG_SPECTRAL_HERO)
+      return fail(CG_E_INVALID, "unknown spectral sampling mode");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    if (env.spectral == mode) return CG_OK;
+    CG_CUDA(cudaSetDevice(env.device));
+    CG_CUDA(cudaStreamSynchronize(env.stream));
+    env.dropAllGraphs();  // captured launch sequences use the other mode's kernels
+    env.dropViewGraph();
+    env.spectral = mode;
+    env.hero = mode == CG_SPECTRAL_HERO;
+    env.has_prev = false;  // the film's running mean restarts
+    return env.syncHero();
+  });
+}
+
+CG_API int cg_get_spectral(int* mode) {
+  return guarded([&]() -> int {
+    if (!mode) return fail(CG_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    *mode = g_env->spectral;
     return CG_OK;
   });
 }

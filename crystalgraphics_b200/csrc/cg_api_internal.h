@@ -136,6 +136,14 @@ struct Renderer {
   static constexpr int kMaxPipelines = 4;
   DeviceArena xwave_arena[kMaxPipelines - 1];
   WaveBuffers xwave[kMaxPipelines - 1]{};
+  // hero-wavelength mode: the extra per-ray and per-sample buffers of every
+  // allocated queue set (WaveBuffers::ray_w, sh_w, s_L4), attached while
+  // `hero` is set
+  bool hero = false;
+  DeviceArena hero_arena, xhero_arena[kMaxPipelines - 1];
+  // (Re)attaches or releases the hero buffers of the allocated queue sets to
+  // match `hero` (never inside a stream capture)
+  int syncHero();
   cudaStream_t xstream[kMaxPipelines - 1] = {};
   cudaEvent_t fork_ev = nullptr, xjoin_ev[kMaxPipelines - 1] = {};
   // allocates pipelines 1 .. count - 1 (never inside a stream capture:
@@ -194,6 +202,7 @@ struct BatchGraph {
 // src/global.h:14): the View() film and its frame history.
 struct Env : Renderer {
   cg_conf conf{};
+  int spectral = CG_SPECTRAL_REFERENCE;  // cg_set_spectral
   void* film = nullptr;   // float4 per pixel
   void* rgba = nullptr;   // uchar4 per pixel
   float* film_pack = nullptr;  // three floats per pixel: the XYZ / RGB readback

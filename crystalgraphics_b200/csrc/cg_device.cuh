@@ -605,6 +605,26 @@ __device__ __forceinline__ Counts counts(const Mat& m, bool can_sample_light, in
   return out;
 }
 
+__device__ __forceinline__ bool sameCounts(const Counts& a, const Counts& b) {
+  return a.diffuse == b.diffuse && a.specular_reflect == b.specular_reflect &&
+         a.rough_reflect == b.rough_reflect && a.specular_transmit == b.specular_transmit &&
+         a.rough_transmit == b.rough_transmit && a.light == b.light;
+}
+
+// ---- hero-wavelength sampling (an option beside the reference's sampler) -------------
+// Four wavelengths per sample (Wilkie et al. 2014): the hero at offset x0 in
+// [0, 400] nm above 380 (x0 = 400 u from the sample's wavelength stream), the
+// others rotated by 100 nm each, wrapped into the range; each is uniform on
+// [380, 780].  The offset is what the sample slot keeps; every kernel derives
+// the four wavelengths from it with these same rounded operations.
+constexpr int kHeroCount = 4;
+__device__ __forceinline__ float heroOffset(float u) { return __fmul_rn(400.0f, u); }
+__device__ __forceinline__ float heroWavelength(float x0, int j) {
+  float x = __fadd_rn(x0, 100.0f * static_cast<float>(j));
+  if (x >= 400.0f) x = __fsub_rn(x, 400.0f);
+  return __fadd_rn(380.0f, x);
+}
+
 }  // namespace dev
 }  // namespace cg
 

@@ -104,12 +104,18 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   const uint32_t key = sampleKey(v.seed, v.frame, pixel, k + v.sample_base);
   Rng wr;
   seedRng(wr, wavelengthKey(key));
-  const float lambda = sampleWavelengthTree(fc.wl_tree, randFloat(wr));
-  const V3 xyz = xyzMatch(lambda);
-  const float prob = fmaxf((xyz.x + xyz.y + xyz.z) / fc.wl_const[0], 1e-6f);
-  wb.s_L[i] = 0.0f;
-  wb.s_lambda[i] = lambda;
-  wb.s_prob[i] = prob;
+  if (wb.hero) {  // the hero's offset; the four wavelengths follow from it
+    wb.s_lambda[i] = heroOffset(randFloat(wr));
+    wb.s_L4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    wb.ray_w[0][i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  } else {
+    const float lambda = sampleWavelengthTree(fc.wl_tree, randFloat(wr));
+    const V3 xyz = xyzMatch(lambda);
+    const float prob = fmaxf((xyz.x + xyz.y + xyz.z) / fc.wl_const[0], 1e-6f);
+    wb.s_L[i] = 0.0f;
+    wb.s_lambda[i] = lambda;
+    wb.s_prob[i] = prob;
+  }
   // cameraRay, rounded per operation like the host restatement
   const float cx = XS(XM(__fdiv_rn(static_cast<float>(px), static_cast<float>(v.width)), 2.0f), 1.0f);
   const float cy = XS(XM(__fdiv_rn(static_cast<float>(py), static_cast<float>(v.height)), 2.0f), 1.0f);
@@ -253,6 +259,18 @@ __global__ void __launch_bounds__(256, 4) k_extend(SceneView sc, WaveBuffers wb,
 // the queue: lanes advance their ray a bounded number of steps, and once at
 // least kRefill lanes are idle the warp takes that many new rays from a
 // per-launch work counter (one atomicAdd per refill).  kAny: shadow rays.
+// An unoccluded shadow ray adds its light-sample term to its sample's slot
+// (all four wavelengths' terms in hero-wavelength mode).
+__device__ __forceinline__ void addShadowTerm(const WaveBuffers& wb, uint32_t i) {
+  const uint32_t slot = wb.sh_slot[i];
+  if (wb.hero) {
+    const float4 x = wb.sh_w[i];
+    atomicAdd(wb.s_L4 + slot, make_float4(wb.sh_o[i].w, x.x, x.y, x.z));
+  } else {
+    atomicAdd(&wb.s_L[slot], wb.sh_o[i].w);
+  }
+}
+
 constexpr int kStepBudget = 16;
 constexpr int kRefill = 8;
 // Closest-hit traversal stack entries per thread kept in shared memory
@@ -303,7 +321,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
     }
     if (ray >= 0 && travSteps<kAny, kCount, kNodes>(sc, st, stack, kStepBudget, cnt, wb.status)) {
       if (kAny) {
-        if (st.best.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[ray]], wb.sh_o[ray].w);
+        if (st.best.inst < 0) addShadowTerm(wb, static_cast<uint32_t>(ray));
       } else {
         wb.hit[ray] = make_float4(st.best.t, st.best.u, st.best.v, __uint_as_float(st.best.tri));
         wb.hit_inst[ray] = st.best.inst;
@@ -366,7 +384,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(SceneView sc, WaveBuffers wb)
     // occluded iff the closest hit (< 1e6) is nearer than expected - 1e-3
     const float tmax = fminf(d.w, MAXD);
     HitRec h = trace<true, kCount, kNodes>(sc, o, d, tmax, cnt, wb.status);
-    if (h.inst < 0) atomicAdd(&wb.s_L[wb.sh_slot[i]], o.w);
+    if (h.inst < 0) addShadowTerm(wb, i);
   }
   if (kCount) {
     unsigned long long a = cnt.nodes, b = cnt.tris, c = cnt.insts;
@@ -518,6 +536,18 @@ struct Child {
   uint32_t key;
 };
 
+// A lobe's value at a direction (the dist functions of shading/dist/*.wesl).
+__device__ __forceinline__ float lobeDist(int model, V3 curr, V3 next, const Surf& s, const Mat& m) {
+  switch (model) {
+    case M_DIFFUSE: return diffuseDist(curr, next, s, m);
+    case M_SREFL: return specularReflectDist(curr, next, s, m);
+    case M_RREFL: return roughReflectDist(curr, next, s, m);
+    case M_STRANS: return specularTransmitDist(curr, next, s, m);
+    case M_RTRANS: return roughTransmitDist(curr, next, s, m);
+  }
+  return 0.0f;
+}
+
 // ---- shade: one tree node per ray ------------------------------------------------
 // Places every ray at its key's cursor: shade_perm lists the level's rays
 // grouped by key.  A block takes tiles of kScatterTile rays: each warp ranks
@@ -587,11 +617,23 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 // kShadeSortGlobal — the level was sorted (keys from the closest-hit kernel,
 // permutation from k_shade_scatter) and the kernel takes rays in that order.  Either way a warp shades misses,
 // cut hits or one material kind rather than a mix of code paths.
-// At most 96 registers: five blocks of 128 threads per SM (the lobe groups
-// need 90-93 without spills; uncapped they took 98, which left room for four).
-template <int kSort, int kLobes = kLobesAll>
-__global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb,
-                                               int depth, int parity) {
+//
+// kHero: hero-wavelength mode.  The tree is drawn at the hero wavelength (the
+// material, sample counts, directions and balance denominators at it), and
+// each ray also carries the path weights of the three other wavelengths: a
+// child's weight for wavelength j is the lobe's value at that wavelength over
+// the hero's denominator.  The reference's estimator weighs each lobe's
+// sample by that lobe alone over the balance denominator (sample.wesl:
+// 452-501), so its expectation depends on the counts and pdfs at the
+// wavelength; at a hit where they differ across the four wavelengths (a lobe
+// heuristic that vanishes at some of them, or a transmission whose refraction
+// index varies with the wavelength) the light sample and the subtree carry
+// the hero alone with weight 4 — over the four equally likely heroes of one
+// wavelength set that is the reference's estimator at each of them.
+// Emission is exact per wavelength.
+template <int kSort, int kLobes, bool kHero>
+__device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst& fc,
+                                           const WaveBuffers& wb, int depth, int parity) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
   // [lo, hi): the queue slice (or, in global order, the permutation range of
   // this launch's keys) the launch takes
@@ -638,9 +680,13 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
       __syncthreads();  // s_order / s_cnt are rewritten by the next slice
     }
     Child ch[4];
+    // hero mode: per child the other wavelengths' weights and the flags (bit 0:
+    // the hero alone below)
+    float4 chw[kHero ? 4 : 1];
     uint32_t nch = 0;
     bool shadow = false;
     float4 sh_o = make_float4(0, 0, 0, 0), sh_d = make_float4(0, 0, 0, 0);
+    float4 sh_x = make_float4(0, 0, 0, 0);  // hero mode: the other wavelengths' terms
     uint32_t slot = 0;
     if (i < n) {
       const float4 o4 = wb.ray_o[parity][i];
@@ -651,11 +697,28 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
       const uint32_t key = __float_as_uint(d4.w);
       const float4 h4 = wb.hit[i];
       const int32_t hinst = wb.hit_inst[i];
-      const float lambda = wb.s_lambda[slot];
+      // hero mode: the other wavelengths' weights, and whether the hero goes alone
+      float4 Wx = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      bool alone = false;
+      float x0 = 0.0f;
+      if constexpr (kHero) {
+        Wx = wb.ray_w[parity][i];
+        alone = (__float_as_uint(Wx.w) & 1u) != 0u;
+        x0 = wb.s_lambda[slot];
+      }
+      const float lambda = kHero ? heroWavelength(x0, 0) : wb.s_lambda[slot];
       const SmitsPos spos = smitsPos(lambda);
       float addL = 0.0f;
+      float4 addX = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // hero mode: wavelengths 1..3
       if (hinst < 0) {
         addL = W * envRadiance(sc, rd, spos);
+        if constexpr (kHero) {
+          if (!alone) {
+            addX.x = Wx.x * envRadiance(sc, rd, smitsPos(heroWavelength(x0, 1)));
+            addX.y = Wx.y * envRadiance(sc, rd, smitsPos(heroWavelength(x0, 2)));
+            addX.z = Wx.z * envRadiance(sc, rd, smitsPos(heroWavelength(x0, 3)));
+          }
+        }
       } else if ((kLobes & kLobeHit) && static_cast<uint32_t>(depth) < cut_depth) {
         // surface frame of the closest hit (bvh.wesl:102-129, 167-179)
         const uint32_t tri = __float_as_uint(h4.w);
@@ -681,26 +744,66 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
         s.sn = dot(wsn, wgn) >= 0.0f ? wsn : -wsn;
         const DevMaterial& dmat = sc.mat[meta.y];
         Mat m;
+        float4 uv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (dmat.volume & kTexturedBit) {
           // the hit's texture coordinates (bvh.wesl:172-179)
           const float4 a = __ldg(sc.vuv + vi.x), b = __ldg(sc.vuv + vi.y), cc = __ldg(sc.vuv + vi.z);
-          const float4 uv = make_float4(w0 * a.x + u * b.x + v * cc.x, w0 * a.y + u * b.y + v * cc.y,
-                                        w0 * a.z + u * b.z + v * cc.z, w0 * a.w + u * b.w + v * cc.w);
+          uv = make_float4(w0 * a.x + u * b.x + v * cc.x, w0 * a.y + u * b.y + v * cc.y,
+                           w0 * a.z + u * b.z + v * cc.z, w0 * a.w + u * b.w + v * cc.w);
           m = decodeTextured(sc, dmat, sc.mattex[meta.y], uv, lambda, spos);
         } else {
           m = decode(dmat, lambda, spos);
         }
         const Counts c = counts(m, sc.has_lights != 0u, depth, caps);
+        // hero mode: the other wavelengths' materials, and whether all four
+        // sample alike here (same counts; the same refraction index where a
+        // transmission lobe is sampled)
+        Mat mx[kHero ? 3 : 1];
+        bool uniform = false;
+        float kw = 1.0f;
+        if constexpr (kHero) {
+          uniform = !alone;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const float lj = heroWavelength(x0, j + 1);
+            mx[j] = (dmat.volume & kTexturedBit)
+                        ? decodeTextured(sc, dmat, sc.mattex[meta.y], uv, lj, smitsPos(lj))
+                        : decode(dmat, lj, smitsPos(lj));
+            if (!sameCounts(counts(mx[j], sc.has_lights != 0u, depth, caps), c)) uniform = false;
+            if ((c.specular_transmit || c.rough_transmit) && mx[j].ior.re != m.ior.re) uniform = false;
+          }
+          kw = (uniform || alone) ? 1.0f : static_cast<float>(kHeroCount);
+          if (!alone) {
+            addX.x = Wx.x * mx[0].emission;
+            addX.y = Wx.y * mx[1].emission;
+            addX.z = Wx.z * mx[2].emission;
+          }
+        }
         Rng rng;
         seedRng(rng, key);
         addL = W * m.emission;
         const V3 curr = rd;
         uint32_t ti = 0;  // transport sample index (child key)
         auto push = [&](V3 next, int model, float prob, float dist) {
-          const float coeff =
-              dist / balanceDenom<kLobes>(sc, curr, next, s, m, c, model, prob, -1.0f, wb.status);
-          const float cw = W * coeff;
-          if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
+          const float denom = balanceDenom<kLobes>(sc, curr, next, s, m, c, model, prob, -1.0f,
+                                                   wb.status);
+          const float coeff = dist / denom;
+          if constexpr (kHero) {
+            const float cw = W * coeff * kw;
+            float c1 = 0.0f, c2 = 0.0f, c3 = 0.0f;
+            if (uniform) {
+              c1 = Wx.x * (lobeDist(model, curr, next, s, mx[0]) / denom);
+              c2 = Wx.y * (lobeDist(model, curr, next, s, mx[1]) / denom);
+              c3 = Wx.z * (lobeDist(model, curr, next, s, mx[2]) / denom);
+            }
+            if (cw != 0.0f || c1 != 0.0f || c2 != 0.0f || c3 != 0.0f) {
+              chw[nch] = make_float4(c1, c2, c3, __uint_as_float(uniform ? 0u : 1u));
+              ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
+            }
+          } else {
+            const float cw = W * coeff;
+            if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
+          }
           ++ti;
         };
         // sampleModels (sample.wesl:301-425) in its lobe order
@@ -771,11 +874,25 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
             const float sproj = fabsf(dot(s.sn, next));
             float ec = diffuseDist(curr, next, s, m) + roughReflectDist(curr, next, s, m);
             if (m.transmission != 0.0f) ec = ec + roughTransmitDist(curr, next, s, m);
-            const float rad = radiance * ec * sproj /
-                              balanceDenom<kLobes>(sc, curr, next, s, m, c, M_NONE, -1.0f, sapdf,
-                                                   wb.status);
-            const float contrib = W * rad;
-            if (contrib != 0.0f) {
+            const float denom = balanceDenom<kLobes>(sc, curr, next, s, m, c, M_NONE, -1.0f, sapdf,
+                                                     wb.status);
+            const float rad = radiance * ec * sproj / denom;
+            const float contrib = W * rad * kw;
+            float4 cx = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if constexpr (kHero) {
+              if (uniform) {
+                float cj[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                  const float lj = heroWavelength(x0, j + 1);
+                  float ecj = diffuseDist(curr, next, s, mx[j]) + roughReflectDist(curr, next, s, mx[j]);
+                  if (mx[j].transmission != 0.0f) ecj = ecj + roughTransmitDist(curr, next, s, mx[j]);
+                  cj[j] = rgbToRadiance(ld3(P.emission), smitsPos(lj)) * ecj * sproj / denom;
+                }
+                cx = make_float4(Wx.x * cj[0], Wx.y * cj[1], Wx.z * cj[2], 0.0f);
+              }
+            }
+            if (contrib != 0.0f || cx.x != 0.0f || cx.y != 0.0f || cx.z != 0.0f) {
               const float expected_dist = sqrtf(dsq);
               const V3 light_pos = s.pos + next * expected_dist;
               const V3 so = spawnOrigin(s, next);
@@ -783,11 +900,17 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
               shadow = true;
               sh_o = make_float4(so.x, so.y, so.z, contrib);
               sh_d = make_float4(next.x, next.y, next.z, tmax);
+              sh_x = cx;
             }
           }
         }
       }
-      if (addL != 0.0f) atomicAdd(&wb.s_L[slot], addL);
+      if constexpr (kHero) {
+        if (addL != 0.0f || addX.x != 0.0f || addX.y != 0.0f || addX.z != 0.0f)
+          atomicAdd(wb.s_L4 + slot, make_float4(addL, addX.x, addX.y, addX.z));
+      } else {
+        if (addL != 0.0f) atomicAdd(&wb.s_L[slot], addL);
+      }
     }
     // ---- warp-aggregated queue appends ----
     uint32_t incl = nch;
@@ -809,6 +932,7 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
           wb.ray_o[out][pos] = make_float4(ch[k].o.x, ch[k].o.y, ch[k].o.z, ch[k].w);
           wb.ray_d[out][pos] = make_float4(ch[k].d.x, ch[k].d.y, ch[k].d.z, __uint_as_float(ch[k].key));
           wb.ray_slot[out][pos] = slot;
+          if constexpr (kHero) wb.ray_w[out][pos] = chw[k];
         }
       }
     }
@@ -824,9 +948,25 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
         wb.sh_o[pos] = sh_o;
         wb.sh_d[pos] = sh_d;
         wb.sh_slot[pos] = slot;
+        if constexpr (kHero) wb.sh_w[pos] = sh_x;
       }
     }
   }
+}
+
+// At most 96 registers: five blocks of 128 threads per SM (the lobe groups
+// need 90-93 without spills; uncapped they took 98, which left room for four).
+template <int kSort, int kLobes = kLobesAll>
+__global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb, int depth,
+                                        int parity) {
+  shadeLevel<kSort, kLobes, false>(sc, fc, wb, depth, parity);
+}
+
+// Hero-wavelength mode (level-wide shading order only).
+template <int kLobes>
+__global__ void __launch_bounds__(128) k_shade_hero(SceneView sc, FrameConst fc, WaveBuffers wb,
+                                                    int depth, int parity) {
+  shadeLevel<kShadeSortGlobal, kLobes, true>(sc, fc, wb, depth, parity);
 }
 
 // ---- resolve: spp loop sum + running mean + sRGB (compute.wesl:41-61) -----------
@@ -845,11 +985,23 @@ __global__ void k_resolve(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
   V3 acc{0.0f, 0.0f, 0.0f};
   uint32_t dropped = 0;
   for (uint32_t k = 0; k < v.spp; ++k) {
-    const float L = wb.s_L[first + k];
-    const float lambda = wb.s_lambda[first + k];
-    const float prob = wb.s_prob[first + k];
-    const V3 il = xyzMatch(lambda) * L / avg;
-    const V3 term = il / prob / spp;
+    V3 term;
+    if (wb.hero) {
+      // four wavelengths, each uniform on [380, 780]: (1/4) sum_j f_j / (1/400)
+      const float4 L = wb.s_L4[first + k];
+      const float x0 = wb.s_lambda[first + k];
+      const float Ls[kHeroCount] = {L.x, L.y, L.z, L.w};
+      V3 est{0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int j = 0; j < kHeroCount; ++j) est = est + xyzMatch(heroWavelength(x0, j)) * Ls[j] / avg;
+      term = est * 100.0f / spp;
+    } else {
+      const float L = wb.s_L[first + k];
+      const float lambda = wb.s_lambda[first + k];
+      const float prob = wb.s_prob[first + k];
+      const V3 il = xyzMatch(lambda) * L / avg;
+      term = il / prob / spp;
+    }
     // a sample whose estimate is not finite adds nothing (and is counted):
     // one NaN would otherwise stay in the pixel's running mean for good
     if (isfinite(term.x) && isfinite(term.y) && isfinite(term.z))
@@ -952,6 +1104,13 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
                 int parity, const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
+  if (wb.hero) {  // hero-wavelength mode: level-wide order, one launch per lobe group
+    k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
+    k_shade_hero<0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade_hero<kLobeHit | kLobeDiffuse | kLobeReflect><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade_hero<kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    return 4;
+  }
   if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
     // one launch per lobe group, each over its keys' range of the permutation

@@ -62,6 +62,15 @@ struct WaveBuffers {
   uint32_t* status;      // bit 0: traversal stack overflow, bit 1: queue overflow
   uint32_t capacity;     // rays per queue (and shadow rays)
   uint32_t sample_capacity;
+  // hero-wavelength mode (hero != 0): per queued ray the path weights of the
+  // three other wavelengths (x, y, z) and flags (w: bit 0 = the hero alone
+  // below a hit where the four wavelengths sample differently); per shadow ray
+  // the other wavelengths' light-sample terms; per sample slot the four
+  // wavelengths' radiance (s_lambda then holds the hero's offset above 380 nm)
+  float4* ray_w[2];
+  float4* sh_w;
+  float4* s_L4;
+  uint32_t hero;
 };
 
 struct FrameConst {

@@ -619,12 +619,14 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
     cg_conf conf;
     cg_tuning tuning;
     int device = 0;
+    bool hero = false;
     {
       std::lock_guard<std::mutex> lk(g_env_mu);
       if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
       conf = g_env->conf;
       tuning = g_env->tuning;
       device = g_env->device;
+      hero = g_env->spectral == CG_SPECTRAL_HERO;
     }
     for (uint32_t i = 0; i < scene_count; ++i)
       if (!scenes[i]) return fail(CG_E_INVALID, "null scene");
@@ -634,6 +636,7 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
     sv->conf = conf;
     for (ServerLane& lane : sv->lanes) {
       lane.rend.tuning = tuning;
+      lane.rend.hero = hero;
       int rc = lane.rend.init(device);
       if (rc != CG_OK) return rc;
       rc = lane.rend.ensureWave(tuning.queue_capacity);

@@ -356,6 +356,29 @@ CG_API int cg_set_counting(int enable);
 /* Selects the RNG seed of the keyed sample streams (default 0). */
 CG_API int cg_set_seed(uint32_t seed);
 
+/* ---- spectral sampling --------------------------------------------------------
+ * CG_SPECTRAL_REFERENCE (the default after cg_init): one wavelength per
+ * sample, importance-sampled on [380, 720] nm by the 16-step bisection of
+ * physics/wavelength.wesl:20-45, weighted as render.wesl:7-18 does.
+ * CG_SPECTRAL_HERO: hero-wavelength sampling (no counterpart in the
+ * reference): four wavelengths per sample, a hero uniform on [380, 780] nm
+ * from the same random number and three more 100 nm apart (wrapped), all
+ * carried by one sample tree drawn at the hero; a sample's XYZ is the mean of
+ * the four wavelengths' terms over their uniform pdf.  Where the four would
+ * draw the tree differently (a lobe whose heuristic vanishes at some of
+ * them, a transmission whose refraction index varies with the wavelength)
+ * the subtree carries the hero alone, weighted by 4, so the estimate keeps the
+ * reference estimator's expectation at every wavelength; the images of the
+ * two modes agree up to the reference's wavelength range (720-780 nm adds a
+ * little X and Y) and the hero mode's lower colour noise.  Applies to cg_view,
+ * cg_view_samples, cg_batch_render and servers created afterwards (each keeps
+ * the mode it was created with); cg_render_noalloc always uses the reference
+ * sampler.  A change restarts the film's running mean.  cg_init resets the
+ * mode to CG_SPECTRAL_REFERENCE. */
+enum { CG_SPECTRAL_REFERENCE = 0, CG_SPECTRAL_HERO = 1 };
+CG_API int cg_set_spectral(int mode);
+CG_API int cg_get_spectral(int* mode);
+
 /* Per-kernel device time of the environment's View() / batch launches,
  * recorded with CUDA events on the launching stream while profiling is on
  * (batches then run without graph capture).  Index: CG_K_* */

@@ -127,6 +127,66 @@ def test_keyed_streams_match_oracle(case):
         assert bias < 0.5, bias
 
 
+@pytest.mark.parametrize("case", [k for k in KEYED if k[0] != "cornell_d2"],
+                         ids=[k[0] for k in KEYED if k[0] != "cornell_d2"])
+def test_hero_keyed_streams_match_oracle(case):
+    """Hero-wavelength mode on the GPU against the oracle's hero mode with the
+    same keyed streams, X, Y and Z.  Besides the branch flips of the reference
+    mode, a hit's 'do the four wavelengths sample alike' decision compares
+    sample counts computed with fused multiply-adds on the GPU and without on
+    the CPU, which can differ at a threshold, so the bar is 99 %."""
+    name, mk, W, H, spp, D, _ = case
+    s = mk()
+    g = B.LoadScene(s)
+    conf = B.PathTraceConf(render_width=W, render_height=H, sample_count=spp, trace_depth=D)
+    B.EnvInit(conf)
+    B.SetSpectral(_abi.CG_SPECTRAL_HERO)
+    assert B.GetSpectral() == _abi.CG_SPECTRAL_HERO
+    B.View(g, B.Camera.from_c(s.camera))
+    gpu = B.ReadFilm(_abi.CG_FILM_XYZ32F)
+    o = O.OracleScene(s)
+    ora, _, _ = o.render(conf.to_c(), s.camera, rng=O.RNG_KEYED, prune=True,
+                         spectral=O.SPECTRAL_HERO)
+    assert np.all(np.isfinite(gpu))
+    keep = ~primary_tie_mask(o, s.camera, W, H)
+    close, rel_mean, far = keyed_compare(gpu, ora, keep)
+    bias = abs(float(far.mean())) / max(float(np.abs(far).mean()), 1e-12) if len(far) else 0.0
+    print(f"hero {name}: {close:.4%} of X/Y/Z values within 1e-3, channel means within "
+          f"{rel_mean:.2e}, diverged {len(far)} (bias {bias:.3f})")
+    assert close >= 0.99, close
+    assert rel_mean < 0.005, rel_mean
+    if len(far) >= 50:
+        assert bias < 0.5, bias
+    g.close()
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
+
+
+def test_hero_mode_lowers_colour_noise_at_equal_samples():
+    """At the same samples per pixel, hero-wavelength frames of the icosphere
+    scatter less than reference-sampler frames around the same mean."""
+    W, H, D, spp, frames = 48, 24, 8, 64, 16
+    s = scenes.icosphere_scene(subdiv=4, width=W, height=H)
+    g = B.LoadScene(s)
+    views = [(s.camera.position[:], s.camera.direction[:], W, H, spp, 77 + k,
+              tuple(s.camera.viewport[:])) for k in range(frames)]
+    stacks = []
+    for mode in (_abi.CG_SPECTRAL_REFERENCE, _abi.CG_SPECTRAL_HERO):
+        B.EnvInit(B.PathTraceConf(render_width=W, render_height=H, sample_count=spp, trace_depth=D))
+        B.SetSpectral(mode)
+        stacks.append(np.stack([pooled_masked(f, np.ones((H, W), bool), 8)
+                                for f in B.batch_render(g, views)]))
+    ref, hero = stacks
+    var_ratio = float(hero.var(0, ddof=1).mean() / ref.var(0, ddof=1).mean())
+    se = np.sqrt(ref.var(0, ddof=1) / frames + hero.var(0, ddof=1) / frames) + 1e-12
+    z = np.abs(ref.mean(0) - hero.mean(0)) / se
+    print(f"hero/reference variance of 8x8-block means at {spp} spp: {var_ratio:.3f}; "
+          f"|z|>3 in {int((z > 3).sum())} of {z.size}")
+    assert var_ratio < 0.7, var_ratio
+    assert (z > 3.5).sum() <= 2
+    g.close()
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
+
+
 def _empty_scene():
     """No geometry at all: every camera ray misses and sees the environment."""
     b = scenes._Builder()
@@ -240,8 +300,10 @@ CONVERGED = [
 ]
 
 
+@pytest.mark.parametrize("spectral", [_abi.CG_SPECTRAL_REFERENCE, _abi.CG_SPECTRAL_HERO],
+                         ids=["reference_lambda", "hero_lambda"])
 @pytest.mark.parametrize("case", CONVERGED, ids=[c[0] for c in CONVERGED])
-def test_converged_image_matches_reference_order_oracle(case):
+def test_converged_image_matches_reference_order_oracle(case, spectral):
     """GPU (keyed streams) vs the oracle in the reference's own RNG order
     (per-pixel PCG-hash streams consumed depth first, trace.wesl:22-89,
     render.wesl:7-18), both converged, on X, Y and Z: relative RMSE of the
@@ -250,7 +312,9 @@ def test_converged_image_matches_reference_order_oracle(case):
     cover the reference's depth cut at 2, the rough dispersive dielectric of
     the icosphere configuration at depth 8 (tree fan-out 3, 2, 1, ...), and
     the instanced material mix at depth 12.  Primary-ray tie pixels are left
-    out of the blocks."""
+    out of the blocks.  Both spectral modes: the reference's one wavelength
+    per sample, and hero-wavelength sampling (four per sample) against the
+    oracle in the same mode."""
     name, mk, W, H, D, (fo, so), (fg, sg) = case
     s = mk()
     g = B.LoadScene(s)
@@ -262,12 +326,14 @@ def test_converged_image_matches_reference_order_oracle(case):
     of = []
     for k in range(fo):
         film, seeds, _ = o.render(conf_o.to_c(), s.camera, film=np.zeros((H, W, 3), np.float32),
-                                  seeds=seeds, iter_count=k, rng=O.RNG_REFERENCE, prune=True)
+                                  seeds=seeds, iter_count=k, rng=O.RNG_REFERENCE, prune=True,
+                                  spectral=spectral)
         of.append(film * (k + 1))
     # GPU: independent frames (different stream seeds)
     views = [(s.camera.position[:], s.camera.direction[:], W, H, sg, 1000 + k,
               tuple(s.camera.viewport[:])) for k in range(fg)]
     B.EnvInit(B.PathTraceConf(render_width=W, render_height=H, sample_count=sg, trace_depth=D))
+    B.SetSpectral(spectral)
     gf = B.batch_render(g, views)
     of, gf = np.stack(of), np.stack(gf)
     assert np.all(np.isfinite(gf)) and np.all(np.isfinite(of))
@@ -280,7 +346,8 @@ def test_converged_image_matches_reference_order_oracle(case):
     floor = np.sqrt(np.mean(se ** 2)) / np.sqrt(np.mean(mo ** 2))
     per_channel = [float(np.sqrt(np.mean((mo[..., c] - mg[..., c]) ** 2)) /
                    np.sqrt(np.mean(mo[..., c] ** 2))) for c in range(3)]
-    print(f"{name}: {int((~keep).sum())} tie pixels excluded; relative RMSE {rmse:.4%} "
+    print(f"{name} ({'hero' if spectral else 'reference'} wavelengths): {int((~keep).sum())} "
+          f"tie pixels excluded; relative RMSE {rmse:.4%} "
           f"(X/Y/Z {per_channel[0]:.3%}/{per_channel[1]:.3%}/{per_channel[2]:.3%}, noise floor "
           f"{floor:.3%}), |z|>3 in {int((z > 3).sum())} of {z.size} block-channels")
     assert rmse <= 0.01, rmse
