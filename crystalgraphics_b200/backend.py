@@ -69,6 +69,7 @@ def _load():
         "cg_set_counting": (i, [i]),
         "cg_set_seed": (i, [u32]),
         "cg_set_spectral": (i, [i]),
+        "cg_set_roulette": (i, [u32]),
         "cg_get_spectral": (i, [C.POINTER(C.c_int)]),
         "cg_set_profiling": (i, [i]),
         "cg_profile_read": (i, [C.POINTER(_abi.CgProfile)]),
@@ -479,6 +480,12 @@ def SetSpectral(mode: int) -> None:
     """_abi.CG_SPECTRAL_REFERENCE (the reference's one wavelength per sample)
     or _abi.CG_SPECTRAL_HERO (four wavelengths per sample)."""
     _check(lib.cg_set_spectral(mode))
+
+
+def SetRoulette(start_depth: int) -> None:
+    """Russian roulette for child rays spawned at hits of depth >= start_depth
+    (0 = off, as the reference)."""
+    _check(lib.cg_set_roulette(start_depth))
 
 
 def GetSpectral() -> int:

@@ -386,7 +386,9 @@ int Renderer::syncHero() {
     if (!hero && w.hero) detachHero(extra, w);
     return CG_OK;
   };
-  if (!hero) {  // buffers in use by queued work stay until it is done
+  bool detach = !hero && wave.hero;
+  for (int k = 0; k < kMaxPipelines - 1; ++k) detach = detach || (!hero && xwave[k].hero);
+  if (detach) {  // buffers in use by queued work stay until it is done
     if (stream) CG_CUDA(cudaStreamSynchronize(stream));
     for (cudaStream_t x : xstream)
       if (x) CG_CUDA(cudaStreamSynchronize(x));
@@ -449,6 +451,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   fc.caps = caps;
   fc.wl_tree = wl_tree;
   fc.wl_const = wl_const;
+  fc.roulette = roulette;
   LaunchShape ls;
   ls.extend_block = tuning.extend_block;
   ls.shade_block = tuning.shade_block;
@@ -1186,6 +1189,23 @@ CG_API int cg_set_spectral(int mode) {
     env.hero = mode == CG_SPECTRAL_HERO;
     env.has_prev = false;  // the film's running mean restarts
     return env.syncHero();
+  });
+}
+
+CG_API int cg_set_roulette(uint32_t start_depth) {
+  return guarded([&]() -> int {
+    if (start_depth > 64u) return fail(CG_E_INVALID, "roulette start depth beyond the trace depth cap");
+    std::lock_guard<std::mutex> lk(g_env_mu);
+    if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
+    Env& env = *g_env;
+    if (env.roulette == start_depth) return CG_OK;
+    CG_CUDA(cudaSetDevice(env.device));
+    CG_CUDA(cudaStreamSynchronize(env.stream));
+    env.dropAllGraphs();  // captured launches hold the old setting
+    env.dropViewGraph();
+    env.roulette = start_depth;
+    env.has_prev = false;  // the film's running mean restarts
+    return CG_OK;
   });
 }
 

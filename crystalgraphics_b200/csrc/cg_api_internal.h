@@ -141,6 +141,8 @@ struct Renderer {
   // `hero` is set
   bool hero = false;
   DeviceArena hero_arena, xhero_arena[kMaxPipelines - 1];
+  // Russian roulette from this hit depth on (0 = off, as the reference)
+  uint32_t roulette = 0;
   // (Re)attaches or releases the hero buffers of the allocated queue sets to
   // match `hero` (never inside a stream capture)
   int syncHero();

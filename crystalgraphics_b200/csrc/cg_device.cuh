@@ -103,6 +103,11 @@ __device__ __forceinline__ uint32_t sampleKey(uint32_t seed, uint32_t frame, uin
 }
 __device__ __forceinline__ uint32_t childKey(uint32_t key, uint32_t i) { return combine(key, i + 1u); }
 __device__ __forceinline__ uint32_t wavelengthKey(uint32_t key) { return combine(key, 0u); }
+// The Russian-roulette decision of a child (an option beyond the reference):
+// one number from this stream.
+__device__ __forceinline__ uint32_t rouletteKey(uint32_t child_key) {
+  return combine(child_key, 0xfffffffeu);
+}
 
 // ---- CIE (physics/cie.wesl) ----------------------------------------------------------
 constexpr float SQRT_HALF_PI = 1.2533141373155001f;

@@ -536,6 +536,19 @@ struct Child {
   uint32_t key;
 };
 
+// Russian roulette (an option beyond the reference, which has none): a child
+// spawned at a hit of depth >= FrameConst::roulette survives with
+// q = min(1, its path weight t) and then carries t / q.  Returns the factor
+// 1 / q, or 0 when the child is dropped; one number from the child's
+// roulette stream decides.
+__device__ __forceinline__ float rouletteFactor(float t, uint32_t child_key) {
+  const float q = fminf(1.0f, t);
+  if (!(q < 1.0f)) return 1.0f;
+  Rng r;
+  seedRng(r, rouletteKey(child_key));
+  return randFloat(r) < q ? 1.0f / q : 0.0f;
+}
+
 // A lobe's value at a direction (the dist functions of shading/dist/*.wesl).
 __device__ __forceinline__ float lobeDist(int model, V3 curr, V3 next, const Surf& s, const Mat& m) {
   switch (model) {
@@ -784,27 +797,39 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
         addL = W * m.emission;
         const V3 curr = rd;
         uint32_t ti = 0;  // transport sample index (child key)
+        const bool roulette = fc.roulette != 0u && static_cast<uint32_t>(depth) >= fc.roulette;
         auto push = [&](V3 next, int model, float prob, float dist) {
           const float denom = balanceDenom<kLobes>(sc, curr, next, s, m, c, model, prob, -1.0f,
                                                    wb.status);
           const float coeff = dist / denom;
+          const uint32_t ck = childKey(key, ti++);
           if constexpr (kHero) {
-            const float cw = W * coeff * kw;
+            float cw = W * coeff * kw;
             float c1 = 0.0f, c2 = 0.0f, c3 = 0.0f;
             if (uniform) {
               c1 = Wx.x * (lobeDist(model, curr, next, s, mx[0]) / denom);
               c2 = Wx.y * (lobeDist(model, curr, next, s, mx[1]) / denom);
               c3 = Wx.z * (lobeDist(model, curr, next, s, mx[2]) / denom);
             }
+            if (roulette) {
+              const float tmax = fmaxf(fmaxf(cw, 0.0f), fmaxf(fmaxf(c1, c2), c3));
+              if (tmax == 0.0f) return;
+              const float rr = rouletteFactor(tmax, ck);
+              if (rr == 0.0f) return;
+              cw = cw * rr;
+              c1 = c1 * rr;
+              c2 = c2 * rr;
+              c3 = c3 * rr;
+            }
             if (cw != 0.0f || c1 != 0.0f || c2 != 0.0f || c3 != 0.0f) {
               chw[nch] = make_float4(c1, c2, c3, __uint_as_float(uniform ? 0u : 1u));
-              ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
+              ch[nch++] = Child{spawnOrigin(s, next), next, cw, ck};
             }
           } else {
-            const float cw = W * coeff;
-            if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, childKey(key, ti)};
+            float cw = W * coeff;
+            if (roulette && cw != 0.0f) cw = cw * rouletteFactor(cw, ck);
+            if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, ck};
           }
-          ++ti;
         };
         // sampleModels (sample.wesl:301-425) in its lobe order
         if ((kLobes & kLobeDiffuse) && c.diffuse) {  // pdf/diffuse.wesl:7-36

@@ -79,6 +79,7 @@ struct FrameConst {
   Caps caps;
   const float* wl_tree;  // 65535 cdf values (sampleWavelengthCdf bisection)
   const float* wl_const; // [0] total integral, [1] total / 3
+  uint32_t roulette = 0; // Russian roulette from this hit depth on (0 = off, as the reference)
 };
 
 struct ChunkDesc {

@@ -620,6 +620,7 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
     cg_tuning tuning;
     int device = 0;
     bool hero = false;
+    uint32_t roulette = 0;
     {
       std::lock_guard<std::mutex> lk(g_env_mu);
       if (!g_env) return fail(CG_E_NOT_INIT, "Environment not initialized.");
@@ -627,6 +628,7 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
       tuning = g_env->tuning;
       device = g_env->device;
       hero = g_env->spectral == CG_SPECTRAL_HERO;
+      roulette = g_env->roulette;
     }
     for (uint32_t i = 0; i < scene_count; ++i)
       if (!scenes[i]) return fail(CG_E_INVALID, "null scene");
@@ -637,6 +639,7 @@ CG_API int cg_server_create(const cg_scene_t* scenes, uint32_t scene_count, uint
     for (ServerLane& lane : sv->lanes) {
       lane.rend.tuning = tuning;
       lane.rend.hero = hero;
+      lane.rend.roulette = roulette;
       int rc = lane.rend.init(device);
       if (rc != CG_OK) return rc;
       rc = lane.rend.ensureWave(tuning.queue_capacity);

@@ -379,6 +379,18 @@ enum { CG_SPECTRAL_REFERENCE = 0, CG_SPECTRAL_HERO = 1 };
 CG_API int cg_set_spectral(int mode);
 CG_API int cg_get_spectral(int* mode);
 
+/* ---- Russian roulette ------------------------------------------------------------
+ * No counterpart in the reference, whose sample trees end only at the depth
+ * cut (trace.wesl:41-49).  With start_depth S > 0, every child ray spawned at
+ * a hit of depth >= S (depth 0 = the camera ray's hit; S = 3 is "after the
+ * third bounce") survives with probability q = min(1, its path weight t, the
+ * largest over the wavelengths it carries) and then carries t / q; one
+ * number from a stream keyed by the child decides.  The estimate keeps its
+ * expectation and traces fewer rays.  0 (the default after cg_init) turns it
+ * off.  Applies like cg_set_spectral; a change restarts the film's running
+ * mean; cg_render_noalloc never uses it. */
+CG_API int cg_set_roulette(uint32_t start_depth);
+
 /* Per-kernel device time of the environment's View() / batch launches,
  * recorded with CUDA events on the launching stream while profiling is on
  * (batches then run without graph capture).  Index: CG_K_* */

@@ -1152,9 +1152,30 @@ struct TraceCtx {
   bool keyed;
   Rng* seq;  // reference mode: the pixel stream
   Counters cnt;
+  uint32_t roulette = 0;  // Russian roulette from this hit depth on (0 = off, as the reference)
 };
 
-float trace(TraceCtx& tc, const Ray& ray, float w, int depth, uint32_t key) {
+// Russian roulette (an option beyond the reference, which has none): a child
+// spawned at a hit of depth >= the start survives with q = min(1, its path
+// weight t) and then carries t / q; one uniform number decides, from the
+// child's roulette stream (keyed) or the pixel stream right before the child
+// is traced (reference order).  Returns the factor 1 / q, or 0 if the child
+// is dropped.
+float roulette(TraceCtx& tc, float t, uint32_t child_key) {
+  const float q = wmin(1.0f, t);
+  if (!(q < 1.0f)) return 1.0f;
+  float u;
+  if (tc.keyed) {
+    Rng r;
+    seedRng(r, rouletteKey(child_key));
+    u = randFloat(r);
+  } else {
+    u = randFloat(*tc.seq);
+  }
+  return u < q ? 1.0f / q : 0.0f;
+}
+
+float trace(TraceCtx& tc, const Ray& ray, float w, int depth, uint32_t key, float thr) {
   const oracle_scene_s& s = *tc.s;
   ++tc.cnt.extend;
   HitInfo hi = rayHit(s, ray, tc.prune, tc.cnt);
@@ -1186,8 +1207,16 @@ float trace(TraceCtx& tc, const Ray& ray, float w, int depth, uint32_t key) {
   }
   float child_l[4] = {0, 0, 0, 0};
   for (uint32_t i = 0; i < smp.transport_count; ++i) {
+    const float t = thr * smp.ts[i].coeff;
+    const uint32_t ck = tc.keyed ? childKey(key, i) : 0u;
+    float rr = 1.0f;
+    if (tc.roulette != 0u && static_cast<uint32_t>(depth) >= tc.roulette) {
+      if (t == 0.0f) continue;  // adds exactly 0: not traced, no number drawn (as the kernels)
+      rr = roulette(tc, t, ck);
+      if (rr == 0.0f) continue;
+    }
     Ray child = spawnSurfaceRay(hi.sp, smp.ts[i].dir);
-    child_l[i] = trace(tc, child, w, depth + 1, tc.keyed ? childKey(key, i) : 0u);
+    child_l[i] = rr * trace(tc, child, w, depth + 1, ck, t * rr);
   }
   // backwardPass = emission + collect (collect.wesl:4-17)
   float rad = 0.0f;
@@ -1233,7 +1262,7 @@ bool sameCounts(const Counts& a, const Counts& b) {
 }
 
 L4 traceHero(TraceCtx& tc, const Ray& ray, const float (&w)[HERO_COUNT], int depth, uint32_t key,
-             bool hero_only) {
+             bool hero_only, const float (&thr)[HERO_COUNT]) {
   const oracle_scene_s& s = *tc.s;
   L4 out{};
   ++tc.cnt.extend;
@@ -1289,12 +1318,29 @@ L4 traceHero(TraceCtx& tc, const Ray& ray, const float (&w)[HERO_COUNT], int dep
   }
   for (uint32_t i = 0; i < smp.transport_count; ++i) {
     const TransportSample& t = smp.ts[i];
+    float cj[HERO_COUNT] = {t.coeff * k, 0.0f, 0.0f, 0.0f};  // the child's coefficients
+    if (uniform)
+      for (int j = 1; j < HERO_COUNT; ++j)
+        cj[j] = lobeDist(t.model, ray.dir, t.dir, hi.sp, m[j]) / t.denom;
+    float ct[HERO_COUNT];  // the child's path weights
+    float tmax = 0.0f;
+    for (int j = 0; j < HERO_COUNT; ++j) {
+      ct[j] = j == 0 ? thr[0] * t.coeff * k : thr[j] * cj[j];
+      tmax = wmax(tmax, ct[j]);
+    }
+    const uint32_t ck = tc.keyed ? childKey(key, i) : 0u;
+    float rr = 1.0f;
+    if (tc.roulette != 0u && static_cast<uint32_t>(depth) >= tc.roulette) {
+      if (tmax == 0.0f) continue;
+      rr = roulette(tc, tmax, ck);
+      if (rr == 0.0f) continue;
+    }
+    for (int j = 0; j < HERO_COUNT; ++j) ct[j] = ct[j] * rr;
     Ray child = spawnSurfaceRay(hi.sp, t.dir);
-    L4 cl = traceHero(tc, child, w, depth + 1, tc.keyed ? childKey(key, i) : 0u, !uniform);
-    out.v[0] += t.coeff * k * cl.v[0];
+    L4 cl = traceHero(tc, child, w, depth + 1, ck, !uniform, ct);
+    out.v[0] += cj[0] * rr * cl.v[0];
     if (!uniform) continue;
-    for (int j = 1; j < HERO_COUNT; ++j)
-      out.v[j] += lobeDist(t.model, ray.dir, t.dir, hi.sp, m[j]) / t.denom * cl.v[j];
+    for (int j = 1; j < HERO_COUNT; ++j) out.v[j] += cj[j] * rr * cl.v[j];
   }
   return out;
 }
@@ -1555,6 +1601,7 @@ int oracle_render(oracle_scene_t s, const oracle_render_args* a, float* film, ui
     tc.conf = conf;
     tc.prune = a->prune != 0;
     tc.keyed = a->rng_mode == ORACLE_RNG_KEYED;
+    tc.roulette = a->roulette;
     Rng seq;
     seedRng(seq, rand_seed);
     tc.seq = &seq;
@@ -1575,13 +1622,14 @@ int oracle_render(oracle_scene_t s, const oracle_render_args* a, float* film, ui
       if (a->spectral == ORACLE_SPECTRAL_HERO) {
         float w[HERO_COUNT];
         heroWavelengths(u, w);
-        const L4 L = traceHero(tc, ray, w, 0, key, false);
+        const float one[HERO_COUNT] = {1.0f, 1.0f, 1.0f, 1.0f};
+        const L4 L = traceHero(tc, ray, w, 0, key, false, one);
         V3 est{0.0f, 0.0f, 0.0f};
         for (int j = 0; j < HERO_COUNT; ++j) est = est + illuminate(w[j], L.v[j]);
         term = est * (HERO_SPAN / HERO_COUNT) / static_cast<float>(spp);
       } else {
         const WavelengthSample ws = sampleWavelengthCdf(u);
-        float L = trace(tc, ray, ws.wavelength, 0, key);
+        float L = trace(tc, ray, ws.wavelength, 0, key, 1.0f);
         term = illuminate(ws.wavelength, L) / ws.prob / static_cast<float>(spp);
       }
       // the library's film policy: a sample whose estimate is not finite adds

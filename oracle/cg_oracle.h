@@ -93,6 +93,10 @@ typedef struct oracle_render_args {
   uint32_t pixel_begin, pixel_end;  /* render only this pixel range
                               (end 0 = all); other pixels are left as is  */
   uint32_t spectral;       /* ORACLE_SPECTRAL_*                             */
+  uint32_t roulette;       /* Russian roulette from this hit depth on (0 = off,
+                              as the reference): a child survives with
+                              q = min(1, its path weight) and carries weight / q */
+  uint32_t _pad;
 } oracle_render_args;
 
 /* One View() frame: for every pixel, render() + film update + rng seed

@@ -127,6 +127,9 @@ inline uint32_t sampleKey(uint32_t seed, uint32_t frame, uint32_t pixel, uint32_
 }
 // Child i (0-based transport sample index) of a node.
 inline uint32_t childKey(uint32_t node_key, uint32_t i) { return combine(node_key, i + 1u); }
+// The Russian-roulette decision of a child (an option beyond the reference):
+// one number from this stream.
+inline uint32_t rouletteKey(uint32_t child_key) { return combine(child_key, 0xfffffffeu); }
 // The wavelength stream of a sample.
 inline uint32_t wavelengthKey(uint32_t sample_key) { return combine(sample_key, 0u); }
 

@@ -68,7 +68,8 @@ def lib():
                            ("iter_count", C.c_uint32), ("rng_mode", C.c_uint32),
                            ("seed", C.c_uint32), ("threads", C.c_uint32), ("prune", C.c_uint32),
                            ("pixel_begin", C.c_uint32), ("pixel_end", C.c_uint32),
-                           ("spectral", C.c_uint32)]
+                           ("spectral", C.c_uint32), ("roulette", C.c_uint32),
+                           ("_pad", C.c_uint32)]
     L = C.CDLL(LIB_PATH)
     L.oracle_scene_create.restype = C.c_void_p
     L.oracle_scene_create.argtypes = [C.POINTER(abi.CgSceneDesc)]
@@ -145,7 +146,8 @@ class OracleScene:
         return hits, t2
 
     def render(self, conf, camera, film=None, seeds=None, iter_count=0, rng=RNG_KEYED, seed=0,
-               threads=0, prune=False, pixel_range=None, spectral=SPECTRAL_REFERENCE):
+               threads=0, prune=False, pixel_range=None, spectral=SPECTRAL_REFERENCE,
+               roulette=0):
         W, H = conf.render_width, conf.render_height
         if film is None:
             film = np.zeros((H, W, 3), np.float32)
@@ -160,6 +162,7 @@ class OracleScene:
         a.threads = threads
         a.prune = 1 if prune else 0
         a.spectral = spectral
+        a.roulette = roulette
         if pixel_range is not None:
             a.pixel_begin, a.pixel_end = pixel_range
         stats = np.zeros(5, np.uint64)

@@ -161,6 +161,70 @@ def test_hero_keyed_streams_match_oracle(case):
     B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
 
 
+ROULETTE = [("cornell_d6_rr2", lambda: scenes.cornell(), 96, 96, 4, 6, 2),
+            ("icosphere_d8_rr3", lambda: scenes.icosphere_scene(subdiv=4), 96, 54, 4, 8, 3)]
+
+
+@pytest.mark.parametrize("spectral", [_abi.CG_SPECTRAL_REFERENCE, _abi.CG_SPECTRAL_HERO],
+                         ids=["reference_lambda", "hero_lambda"])
+@pytest.mark.parametrize("case", ROULETTE, ids=[r[0] for r in ROULETTE])
+def test_roulette_keyed_streams_match_oracle(case, spectral):
+    """Russian roulette (cg_set_roulette, not in the reference) on the GPU
+    against the oracle's roulette with the same keyed streams, in both
+    spectral modes; it traces fewer rays than the same frame without it."""
+    name, mk, W, H, spp, D, start = case
+    s = mk()
+    g = B.LoadScene(s)
+    conf = B.PathTraceConf(render_width=W, render_height=H, sample_count=spp, trace_depth=D)
+    B.EnvInit(conf)
+    B.SetSpectral(spectral)
+    B.SetRoulette(start)
+    B.View(g, B.Camera.from_c(s.camera))
+    gpu = B.ReadFilm(_abi.CG_FILM_XYZ32F)
+    rays_rr = B.LastStats().extend_rays
+    B.SetRoulette(0)
+    B.View(g, B.Camera.from_c(s.camera))
+    rays = B.LastStats().extend_rays
+    o = O.OracleScene(s)
+    ora, _, _ = o.render(conf.to_c(), s.camera, rng=O.RNG_KEYED, prune=True, spectral=spectral,
+                         roulette=start)
+    keep = ~primary_tie_mask(o, s.camera, W, H)
+    close, rel_mean, _ = keyed_compare(gpu, ora, keep)
+    print(f"roulette {name} ({'hero' if spectral else 'reference'}): {close:.4%} of X/Y/Z values "
+          f"within 1e-3, channel means within {rel_mean:.2e}; extend rays {rays_rr} vs {rays} "
+          f"without")
+    assert np.all(np.isfinite(gpu))
+    assert close >= 0.99, close
+    assert rel_mean < 0.005, rel_mean
+    assert rays_rr < rays
+    g.close()
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
+
+
+def test_roulette_keeps_the_expectation():
+    """Frames with Russian roulette after the third bounce converge to the
+    frames without it (icosphere configuration, depth 8, 8x8-block means
+    within 3 sigma on X, Y and Z)."""
+    W, H, D, spp, frames = 48, 24, 8, 64, 16
+    s = scenes.icosphere_scene(subdiv=4, width=W, height=H)
+    g = B.LoadScene(s)
+    views = [(s.camera.position[:], s.camera.direction[:], W, H, spp, 300 + k,
+              tuple(s.camera.viewport[:])) for k in range(frames)]
+    stacks = []
+    for start in (0, 3):
+        B.EnvInit(B.PathTraceConf(render_width=W, render_height=H, sample_count=spp, trace_depth=D))
+        B.SetRoulette(start)
+        stacks.append(np.stack([pooled_masked(f, np.ones((H, W), bool), 8)
+                                for f in B.batch_render(g, views)]))
+    a, b = stacks
+    se = np.sqrt(a.var(0, ddof=1) / frames + b.var(0, ddof=1) / frames) + 1e-12
+    z = np.abs(a.mean(0) - b.mean(0)) / se
+    print(f"roulette vs none: |z|>3 in {int((z > 3).sum())} of {z.size}, max {z.max():.2f}")
+    assert (z > 3.5).sum() <= 2
+    g.close()
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
+
+
 def test_hero_mode_lowers_colour_noise_at_equal_samples():
     """At the same samples per pixel, hero-wavelength frames of the icosphere
     scatter less than reference-sampler frames around the same mean."""
