@@ -598,7 +598,8 @@ def run_ours(args):
     if (args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort != "default" or
             args.box_bits or args.pipelines):
         B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width,
-                    persistent=None if args.persistent < 0 else bool(args.persistent),
+                    persistent=None if args.persistent < 0 else
+                    ("postponed" if args.persistent == 3 else bool(args.persistent)),
                     shade_sort=None if args.shade_sort == "default" else args.shade_sort,
                     box_bits=args.box_bits, pipelines=args.pipelines)
     clocks = ClockSampler(local).__enter__()
@@ -770,8 +771,9 @@ def main():
     ap.add_argument("--queue", type=int, default=0, help="ray queue capacity (0 = default)")
     ap.add_argument("--bvh-width", type=int, default=0, choices=[0, 2, 4],
                     help="node width of the traversal (0 = library default, 4)")
-    ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
-                    help="persistent lane-refill traversal (-1 = library default)")
+    ap.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1, 3],
+                    help="persistent lane-refill traversal (-1 = library default; 3 = with "
+                         "postponed leaves)")
     ap.add_argument("--pipelines", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="chunk pipelines of View() (0 = library default, 2)")
     ap.add_argument("--box-bits", type=int, default=0, choices=[0, 8, 32],

@@ -498,7 +498,8 @@ def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_
               persistent=None, shade_sort=None, box_bits=0, pipelines=0) -> None:
     """0 (or None for the two switches) keeps the current value.  shade_sort:
     True / "global" (level-wide sort by material kind), "block" (per block),
-    False / "none"."""
+    False / "none".  persistent: True (persistent warps), False (one ray per
+    thread) or "postponed" (persistent, with postponed leaves)."""
     if shade_sort is None:
         sort = 0
     elif isinstance(shade_sort, str):
@@ -506,7 +507,8 @@ def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_
     else:
         sort = 1 if shade_sort else 2
     t = _abi.CgTuning(queue_capacity, extend_block, shade_block, use_graph, bvh_width,
-                      0 if persistent is None else (1 if persistent else 2), sort, box_bits,
+                      0 if persistent is None else
+                      (3 if persistent == "postponed" else 1 if persistent else 2), sort, box_bits,
                       pipelines)
     _check(lib.cg_set_tuning(C.byref(t)))
 

@@ -457,6 +457,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.shade_block = tuning.shade_block;
   ls.nodes = nodeFormatOf(tuning);
   ls.persistent = tuning.persistent != 2u;
+  ls.spec = tuning.persistent == 3u;
   const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
   ls.shade_sort = tuning.shade_sort == 2u   ? kShadeSortNone
                   : tuning.shade_sort == 3u ? kShadeSortBlock
@@ -1246,7 +1247,7 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
     if (t->extend_block) g.extend_block = t->extend_block;
     if (t->shade_block) g.shade_block = t->shade_block;
     if (t->bvh_width) g.bvh_width = t->bvh_width;
-    if (t->persistent) g.persistent = t->persistent == 2u ? 2u : 1u;
+    if (t->persistent) g.persistent = t->persistent == 2u || t->persistent == 3u ? t->persistent : 1u;
     if (t->shade_sort) g.shade_sort = t->shade_sort;
     g_env->tuning.use_graph = t->use_graph;
     g_env->dropAllGraphs();

@@ -281,7 +281,8 @@ constexpr int kRefill = 8;
 // shared carve-out costs them L1), so shadow rays keep a local stack.
 constexpr int kShortStack = 16;
 
-template <bool kAny, bool kCount, int kNodes>
+// kSpec: closest hits over four-wide trees with postponed leaves (travStepsSpec).
+template <bool kAny, bool kCount, int kNodes, bool kSpec = false>
 __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuffers& wb, uint32_t n,
                                                    uint32_t* work, int parity, int keys) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -294,6 +295,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
   }
   TravState st;
   int32_t ray = -1;
+  int32_t leaf = kNoLeaf;  // kSpec: the parked BLAS leaf
   bool exhausted = false;
   while (true) {
     const unsigned idle = __ballot_sync(kFull, ray < 0);
@@ -319,7 +321,14 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
       if (exhausted) break;
       continue;
     }
-    if (ray >= 0 && travSteps<kAny, kCount, kNodes>(sc, st, stack, kStepBudget, cnt, wb.status)) {
+    bool fin;
+    if constexpr (kSpec) {  // every lane of the warp takes part in the leaf votes
+      fin = travStepsSpec<kCount, kNodes == kNodesWide4Q>(sc, st, leaf, stack, kStepBudget, cnt,
+                                                          wb.status, ray >= 0);
+    } else {
+      fin = ray >= 0 && travSteps<kAny, kCount, kNodes>(sc, st, stack, kStepBudget, cnt, wb.status);
+    }
+    if (ray >= 0 && fin) {
       if (kAny) {
         if (st.best.inst < 0) addShadowTerm(wb, static_cast<uint32_t>(ray));
       } else {
@@ -348,7 +357,7 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
 // counts[3] (extend) and counts[4] (shadow) are the work counters; each is
 // zeroed by the kernel before its user in stream order (k_gen for depth 0,
 // k_shade for the next extend, k_extend for the shadow launch after it).
-template <bool kCount, int kNodes>
+template <bool kCount, int kNodes, bool kSpec = false>
 __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, WaveBuffers wb,
                                                               int parity, int keys) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
@@ -359,7 +368,7 @@ __global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, Wave
     atomicAdd(&wb.stats[0], static_cast<unsigned long long>(n));
   }
   if (keys) beginShadeKeys();
-  persistentTraverse<false, kCount, kNodes>(sc, wb, n, &wb.counts[3], parity, keys);
+  persistentTraverse<false, kCount, kNodes, kSpec>(sc, wb, n, &wb.counts[3], parity, keys);
   if (keys) finishShadeKeys(wb);
 }
 
@@ -1104,6 +1113,17 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
   if (ls.persistent) {  // one resident grid: 64 registers -> 65536 / (64 * block) blocks per SM
     const uint32_t g = gridFor(1024u / block);
     const size_t smem = size_t(kShortStack) * block * sizeof(int32_t);
+    if (ls.spec && ls.nodes != kNodesBinary) {  // postponed leaves
+      const bool q = ls.nodes == kNodesWide4Q;
+      if (counting) {
+        if (q) k_extend_persistent<true, kNodesWide4Q, true><<<g, block, smem, s>>>(sc, wb, parity, keys);
+        else k_extend_persistent<true, kNodesWide4, true><<<g, block, smem, s>>>(sc, wb, parity, keys);
+      } else {
+        if (q) k_extend_persistent<false, kNodesWide4Q, true><<<g, block, smem, s>>>(sc, wb, parity, keys);
+        else k_extend_persistent<false, kNodesWide4, true><<<g, block, smem, s>>>(sc, wb, parity, keys);
+      }
+      return;
+    }
     switch (ls.nodes * 2 + (counting ? 1 : 0)) {
       case kNodesBinary * 2: k_extend_persistent<false, kNodesBinary><<<g, block, smem, s>>>(sc, wb, parity, keys); break;
       case kNodesBinary * 2 + 1: k_extend_persistent<true, kNodesBinary><<<g, block, smem, s>>>(sc, wb, parity, keys); break;

@@ -102,6 +102,7 @@ struct LaunchShape {
   uint32_t grid_shade = 0;
   int nodes = kNodesWide4;   // NodeFormat of the traversal
   bool persistent = true;    // persistent warps with lane refill
+  bool spec = false;         // with persistent four-wide closest hits: postponed leaves
   int shade_sort = kShadeSortGlobal;  // ShadeSort: order of the rays the shading kernel takes
 };
 

@@ -476,6 +476,142 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, Sta
   return false;
 }
 
+// The closest-hit walk of travSteps over four-wide trees with postponed
+// leaves ("speculative traversal", Aila & Laine 2009): a lane that reaches a
+// BLAS leaf parks it and goes on with its next inner node; the parked
+// triangles are tested when no lane of the warp still walks inner nodes
+// without a parked leaf, so the node visits and the triangle tests each run
+// with most lanes of the warp instead of alternating between lanes.  A lane
+// that reaches a second leaf, the end of its instance (return to the TLAS) or
+// the end of its walk while a leaf is parked waits for the flush.  Every lane
+// of the warp calls it together (`active` false for idle lanes); returns true
+// when the lane's ray is finished.  Hits are those of travSteps: every
+// overlapping node is still visited or bounded by a closest hit found so far
+// (the bound is only looser while a leaf is parked).
+constexpr int32_t kNoLeaf = INT_MIN + 2;
+
+template <bool kCount, bool kQuant, class Stack>
+__device__ __forceinline__ bool travStepsSpec(const SceneView& sc, TravState& s, int32_t& leaf,
+                                              Stack& stack, int budget, TravCounters& cnt,
+                                              uint32_t* status, bool active) {
+  using W = Wide<kQuant>;
+  bool finished = false;
+  for (int step = 0; step < budget; ++step) {
+    if (active && !finished) {
+      int32_t node = s.node;
+      if (node >= 0) {  // one inner node visit
+        const typename W::Node* nodes = s.cur_inst < 0 ? W::tlas(sc) : W::blas(sc);
+        float nxs[4], fxs[4], nys[4], fys[4], nzs[4], fzs[4];
+        const int4 ch = W::fetch(nodes + node, s.idx < 0.0f, s.idy < 0.0f, s.idz < 0.0f, nxs, fxs,
+                                 nys, fys, nzs, fzs);
+        if (kCount) ++cnt.nodes;
+        float k[4];
+        const int32_t links[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float a0 = fmaf(nxs[c], s.idx, -s.oix), a1 = fmaf(fxs[c], s.idx, -s.oix);
+          const float b0 = fmaf(nys[c], s.idy, -s.oiy), b1 = fmaf(fys[c], s.idy, -s.oiy);
+          const float c0 = fmaf(nzs[c], s.idz, -s.oiz), c1 = fmaf(fzs[c], s.idz, -s.oiz);
+          const float tmin = fmaxf(fmaxf(a0, b0), fmaxf(c0, 0.0f));
+          const float tmx = fminf(fminf(a1, b1), fminf(c1, s.best.t));
+          const bool hit = kQuant ? (tmin <= tmx && links[c] != kEmptyLink) : tmin <= tmx;
+          k[c] = hit ? tmin : INFINITY;
+        }
+        int32_t l0 = ch.x, l1 = ch.y, l2 = ch.z, l3 = ch.w;
+        float k0 = k[0], k1 = k[1], k2 = k[2], k3 = k[3];
+        cswap(k0, l0, k1, l1);
+        cswap(k2, l2, k3, l3);
+        cswap(k0, l0, k2, l2);
+        cswap(k1, l1, k3, l3);
+        cswap(k1, l1, k2, l2);
+        if (k0 == INFINITY) {
+          s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
+        } else {
+          const int pushes = (k1 != INFINITY) + (k2 != INFINITY) + (k3 != INFINITY);
+          if (s.sp + pushes > kStackSize) {
+            atomicOr(status, 1u);
+            s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
+            s.node = kDone;
+            leaf = kNoLeaf;
+            finished = true;
+          } else {
+            if (k3 != INFINITY) stack.set(s.sp++, l3);
+            if (k2 != INFINITY) stack.set(s.sp++, l2);
+            if (k1 != INFINITY) stack.set(s.sp++, l1);
+            s.node = l0;
+          }
+        }
+      } else if (node != kDone && node != kToTlas) {
+        const uint32_t first = static_cast<uint32_t>(~node) >> 3;
+        const uint32_t count = static_cast<uint32_t>(~node) & 7u;
+        if (s.cur_inst >= 0) {  // a BLAS leaf: park it if the slot is free
+          if (leaf == kNoLeaf) {
+            leaf = node;
+            s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
+          }
+        } else if (count == 0u) {
+          s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
+        } else {  // a TLAS leaf: enter the instance's BLAS in its space
+          const float4* ipf = reinterpret_cast<const float4*>(sc.inst + first);
+          const float4 r0 = __ldg(ipf), r1 = __ldg(ipf + 1), r2 = __ldg(ipf + 2);
+          const uint4 meta = __ldg(reinterpret_cast<const uint4*>(ipf + 3));
+          const float m[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+          if (kCount) ++cnt.insts;
+          toLocal(m, s.wox, s.woy, s.woz, s.wdx, s.wdy, s.wdz, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz);
+          s.idx = safeInv(s.dx); s.idy = safeInv(s.dy); s.idz = safeInv(s.dz);
+          s.oix = s.ox * s.idx; s.oiy = s.oy * s.idy; s.oiz = s.oz * s.idz;
+          if (s.sp >= kStackSize) {
+            atomicOr(status, 1u);
+            s.best = HitRec{s.best.t, 0.0f, 0.0f, -1, 0u};
+            s.node = kDone;
+            finished = true;
+          } else {
+            stack.set(s.sp++, kToTlas);
+            s.cur_inst = static_cast<int32_t>(first);
+            s.node = static_cast<int32_t>(meta.w);  // blas4_root
+          }
+        }
+      } else if (leaf == kNoLeaf) {  // the end of an instance or of the walk
+        if (node == kDone) {
+          finished = true;
+        } else {
+          s.cur_inst = -1;
+          s.ox = s.wox; s.oy = s.woy; s.oz = s.woz;
+          s.dx = s.wdx; s.dy = s.wdy; s.dz = s.wdz;
+          s.idx = safeInv(s.dx); s.idy = safeInv(s.dy); s.idz = safeInv(s.dz);
+          s.oix = s.ox * s.idx; s.oiy = s.oy * s.idy; s.oiz = s.oz * s.idz;
+          s.node = s.sp > 0 ? stack.get(--s.sp) : kDone;
+        }
+      }
+    }
+    // flush the parked leaves once no lane walks inner nodes without one
+    const bool parked = active && leaf != kNoLeaf;
+    const bool walking = active && !finished && leaf == kNoLeaf && s.node >= 0;
+    const unsigned want = __ballot_sync(0xffffffffu, parked);
+    if (want && !__any_sync(0xffffffffu, walking) && parked) {
+      const uint32_t first = static_cast<uint32_t>(~leaf) >> 3;
+      const uint32_t count = static_cast<uint32_t>(~leaf) & 7u;
+      for (uint32_t kk = 0; kk < count; ++kk) {
+        const float4* tp = sc.tris + 3u * (first + kk);
+        const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
+        if (kCount) ++cnt.tris;
+        float t, u, v;
+        if (intersectTri(s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, ta, tb, tc, t, u, v) &&
+            t < s.best.t) {
+          s.best.t = t;
+          s.best.u = u;
+          s.best.v = v;
+          s.best.inst = s.cur_inst;
+          s.best.tri = first + kk;
+        }
+      }
+      leaf = kNoLeaf;
+    }
+    if (__all_sync(0xffffffffu, !active || finished)) break;
+  }
+  return active && finished;
+}
+
 // The same closest / any hit over Bvh4Node trees: one node visit tests four
 // boxes (six independent 128-bit slab loads), the hit children are ordered
 // by entry distance, the nearest is visited next and the others pushed.

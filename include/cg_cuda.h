@@ -452,7 +452,11 @@ typedef struct cg_tuning {
                            always written (0 = launch directly) */
   uint32_t bvh_width;   /* 4 (default) or 2: node width the traversal walks */
   uint32_t persistent;  /* 1 (default) = persistent traversal warps that refill
-                           idle lanes, 2 = one ray per thread, 0 = keep */
+                           idle lanes, 2 = one ray per thread, 3 = persistent
+                           with postponed leaves on four-wide trees (a lane
+                           parks a BLAS leaf and goes on with inner nodes;
+                           the warp tests the parked triangles together),
+                           0 = keep */
   uint32_t shade_sort;  /* order of the rays the shading kernel takes: 1 (default)
                            = grouped by material kind with a level-wide counting
                            sort, 3 = sorted within each block's slice, 2 = as

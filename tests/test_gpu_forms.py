@@ -251,7 +251,9 @@ def test_server_cancel_and_timeout(cornell):
                                      dict(bvh_width=4, persistent=False),
                                      dict(bvh_width=4, persistent=False, shade_sort=False),
                                      dict(bvh_width=4, persistent=True, shade_sort="block"),
-                                     dict(bvh_width=4, persistent=False, box_bits=8)])
+                                     dict(bvh_width=4, persistent=False, box_bits=8),
+                                     dict(bvh_width=4, persistent="postponed"),
+                                     dict(bvh_width=4, persistent="postponed", box_bits=8)])
 def test_traversal_variants_render_the_same_samples(variant):
     """Binary or four-wide trees, one ray per thread or persistent warps, rays
     grouped by material before shading or not: the closest hits and the keyed
