@@ -56,13 +56,37 @@ NODE_B = {4: 128, "4q": 64, 2: 64}
 TRI_B, INST_B, RAY_B = 48, 64, 52
 # non-tensor FP32 peak (nominal; no measured figure exists for it)
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
-# DRAM bytes (read + write) per closest-hit launch of this workload, mean of the
-# seven launches of one chunk in profiles/dram_traffic_icosphere_1280x720_16spp_d8.md
-# (ncu, cold caches: an upper bound), captured with 14 closest-hit launches per
-# frame (64M-ray queues); with another chunking the frame's traffic is spread
-# over its launches
-EXTEND_TRAFFIC_B = 718.7e6
-EXTEND_TRAFFIC_LAUNCHES = 14
+# Memory traffic of the closest-hit kernel (k_extend_persistent, four-wide
+# float-box trees) per extend ray, from ncu on the medium icosphere case
+# (640x360, 16 spp, 16M-ray queues): DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) over the closest-hit launches of one frame divided by
+# the frame's extend rays, and L2 bytes (lts__t_bytes.sum) per extend ray over
+# two of those launches; with the active lanes per issued instruction
+# (smsp__thread_inst_executed_per_inst_executed.ratio) of the same two.  A
+# launch's traffic is taken as proportional to its rays (the trees stay
+# L2-resident at both sizes).  None where no capture of the variant exists.
+EXTEND_COUNTERS = {
+    "dram_bytes_per_ray": None,
+    "l2_bytes_per_ray": None,
+    "lanes_active": None,
+}
+
+
+def l2_copy_gbs(torch):
+    """Bandwidth of a copy whose buffers stay in L2 (2 x 24 MiB, torch copy_,
+    CUDA events over 200 copies, read + write bytes): the denominator of the
+    closest-hit kernel's L2-side fraction."""
+    a = torch.empty(24 << 20, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(200):
+        b.copy_(a)
+    e1.record()
+    torch.cuda.synchronize()
+    return 2 * a.numel() * 200 / (e0.elapsed_time(e1) / 1e3) / 1e9
 
 
 def dist_env():
@@ -663,7 +687,6 @@ def run_ours(args):
     sh_ms, sh_n = prof["shadow"]
     # counting pass totals cover extend + shadow; split the node/tri work by ray count
     per_frame_launch = max(ext_n // max(args.steps, 1), 1)
-    extend_scale = EXTEND_TRAFFIC_LAUNCHES / per_frame_launch
     tun = B.GetTuning()
     width = int(tun.bvh_width) or 4
     node_b = NODE_B["4q"] if width == 4 and int(tun.box_bits) == 8 else NODE_B[width]
@@ -684,6 +707,24 @@ def run_ours(args):
         peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
+    # the kernel's real memory traffic, from the medium-case counters scaled by
+    # this launch's rays (default kernel variant on the icosphere workload only)
+    counters_apply = (WORKLOAD_NAME == "icosphere" and width == 4 and node_b == NODE_B[4] and
+                      int(tun.persistent) == 1)
+    rays_per_launch = cst.extend_rays / per_frame_launch
+    traffic = dram_side = l2_side = None
+    if counters_apply and EXTEND_COUNTERS["dram_bytes_per_ray"]:
+        traffic = EXTEND_COUNTERS["dram_bytes_per_ray"] * rays_per_launch
+        gbs = traffic / avg_launch_s / 1e9
+        dram_side = {"bytes_per_launch": traffic, "achieved": gbs, "peak": peak, "unit": "GB/s",
+                     "frac": gbs / peak}
+    if counters_apply and EXTEND_COUNTERS["l2_bytes_per_ray"]:
+        l2b = EXTEND_COUNTERS["l2_bytes_per_ray"] * rays_per_launch
+        l2_peak = l2_copy_gbs(torch)
+        gbs = l2b / avg_launch_s / 1e9
+        l2_side = {"bytes_per_launch": l2b, "achieved": gbs, "peak": l2_peak, "unit": "GB/s",
+                   "frac": gbs / l2_peak,
+                   "peak_source": "measured here: torch copy of an L2-resident 24 MiB buffer"}
 
     cpu = cpu_rate(scene, budget_s=12.0) if (rank == 0 and ws == 1 and not args.no_cpu) else None
     packing = host_packing_baseline(B) if (rank == 0 and ws == 1 and not args.no_cpu and
@@ -714,13 +755,14 @@ def run_ours(args):
             "roofline": {"kernel": "k_extend (closest-hit traversal)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": (EXTEND_TRAFFIC_B * extend_scale if (
-                                         args.case == "full" and width == 4 and
-                                         node_b == NODE_B[4] and WORKLOAD_NAME == "icosphere")
-                                     else None),
-                         "traffic_source": "ncu dram__bytes_read+write per launch, cold "
-                                           "caches (profiles/dram_traffic_icosphere_"
-                                           "1280x720_16spp_d8.md)",
+                         "traffic": traffic,
+                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                            "of k_extend_persistent per extend ray on the "
+                                            "640x360 icosphere frame, times this launch's rays"
+                                            if traffic else None),
+                         "dram": dram_side, "l2": l2_side,
+                         "lanes_active_per_instruction": EXTEND_COUNTERS["lanes_active"]
+                         if counters_apply else None,
                          "bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": avg_launch_s * 1e3,
                          "fp32": {"achieved": fp32_achieved, "peak": FP32_PEAK_TFLOPS,

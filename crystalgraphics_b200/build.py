@@ -18,7 +18,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
+# CG_NVCC_DEFINES (e.g. "CG_SMITS_SHARED"): preprocessor switches of a kernel
+# variant; such builds keep their objects apart
+DEFINES = os.environ.get("CG_NVCC_DEFINES", "").split()
+BUILD = os.path.join(HERE, "_build" + ("_" + "_".join(DEFINES) if DEFINES else ""))
 LIB = os.path.join(HERE, "libcg_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -33,7 +36,8 @@ def nvcc() -> str:
 def _flags(extra_device: list[str] | None = None) -> list[str]:
     return ARCH + ["-O3", "-lineinfo", "-std=c++20", "--expt-relaxed-constexpr",
                    "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
-                   "-I", os.path.join(HERE, "..", "include")] + (extra_device or [])
+                   "-I", os.path.join(HERE, "..", "include")] + ["-D" + d for d in DEFINES] + \
+        (extra_device or [])
 
 
 def sources() -> list[str]:
@@ -99,7 +103,11 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose, ptxas_v), srcs))
-    if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
+    stamp = LIB + ".variant"  # the switches the library was linked with
+    variant = " ".join(DEFINES)
+    same = os.path.exists(stamp) and open(stamp).read() == variant
+    if not same or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB)
+                                                  for o in objs):
         tmp = LIB + ".tmp"
         cmd = [nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-lcudart", "-Xcompiler", "-fPIC"]
         if verbose:
@@ -108,6 +116,8 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+        with open(stamp, "w") as f:
+            f.write(variant)
     build_cxx(verbose)
     return LIB
 

@@ -195,6 +195,26 @@ __device__ const float kSmits[7][10] = {
     {0.0001f, 0.0f, 0.1088f, 0.6651f, 1.0f, 1.0f, 0.9996f, 0.9586f, 0.9685f, 0.984f}};        // yellow
 enum { SM_WHITE = 0, SM_RED, SM_GREEN, SM_BLUE, SM_MAGENTA, SM_CYAN, SM_YELLOW };
 
+// Built with CG_SMITS_SHARED, the shading kernels copy the bins and curves
+// into shared memory at their start (stageSmitsTables) and read them there;
+// otherwise they read the global copies above through the read-only cache.
+#ifdef CG_SMITS_SHARED
+__shared__ float s_smits_tables[80];  // 10 bins, then the 7 curves
+__device__ __forceinline__ void stageSmitsTables() {
+  for (int i = threadIdx.x; i < 80; i += blockDim.x)
+    s_smits_tables[i] = i < 10 ? kBins[i] : kSmits[(i - 10) / 10][(i - 10) % 10];
+  __syncthreads();
+}
+__device__ __forceinline__ float smitsBin(uint32_t i) { return s_smits_tables[i]; }
+__device__ __forceinline__ float smitsCurve(int curve, uint32_t i) {
+  return s_smits_tables[10 + curve * 10 + i];
+}
+#else
+__device__ __forceinline__ void stageSmitsTables() {}
+__device__ __forceinline__ float smitsBin(uint32_t i) { return __ldg(&kBins[i]); }
+__device__ __forceinline__ float smitsCurve(int curve, uint32_t i) { return __ldg(&kSmits[curve][i]); }
+#endif
+
 // Per-wavelength lookup position shared by all seven curves.
 struct SmitsPos {
   int mode;  // 0: below 380, 1: above 720, 2: interpolate
@@ -214,15 +234,14 @@ __device__ __forceinline__ SmitsPos smitsPos(float w) {
   uint32_t bin = static_cast<uint32_t>(10.0f * (w - 380.0f) / 340.0f);
   p.b0 = bin > 9u ? 9u : bin;
   p.b1 = (bin + 1u) > 9u ? 9u : bin + 1u;  // WGSL robust access clamps index 10 to 9
-  const float lo = __ldg(&kBins[p.b0]), hi = __ldg(&kBins[p.b1]);
+  const float lo = smitsBin(p.b0), hi = smitsBin(p.b1);
   p.mixv = (w - lo) / (hi - lo);
   return p;
 }
 __device__ __forceinline__ float smits(const SmitsPos& p, int curve) {
-  const float* X = kSmits[curve];
-  if (p.mode == 0) return __ldg(&X[0]);
-  if (p.mode == 1) return __ldg(&X[9]);
-  return (1.0f - p.mixv) * __ldg(&X[p.b0]) + p.mixv * __ldg(&X[p.b1]);
+  if (p.mode == 0) return smitsCurve(curve, 0);
+  if (p.mode == 1) return smitsCurve(curve, 9);
+  return (1.0f - p.mixv) * smitsCurve(curve, p.b0) + p.mixv * smitsCurve(curve, p.b1);
 }
 __device__ __forceinline__ float rgbToSpectrum(V3 rgb, const SmitsPos& sp) {
   float s = 0.0f;

@@ -656,6 +656,7 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 template <int kSort, int kLobes, bool kHero>
 __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst& fc,
                                            const WaveBuffers& wb, int depth, int parity) {
+  stageSmitsTables();
   const uint32_t n = min(wb.counts[parity], wb.capacity);
   // [lo, hi): the queue slice (or, in global order, the permutation range of
   // this launch's keys) the launch takes
