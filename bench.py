@@ -66,9 +66,9 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # launch's traffic is taken as proportional to its rays (the trees stay
 # L2-resident at both sizes).  None where no capture of the variant exists.
 EXTEND_COUNTERS = {
-    "dram_bytes_per_ray": None,
-    "l2_bytes_per_ray": None,
-    "lanes_active": None,
+    "dram_bytes_per_ray": 145.0,   # 2162 MB over the 14 launches of a frame of 14,915,514 rays
+    "l2_bytes_per_ray": 962.3,     # L2 / DRAM bytes 6.64 on two of those launches
+    "lanes_active": 10.4,          # 11.58 and 9.17 of 32 on the same two
 }
 
 
@@ -626,6 +626,10 @@ def run_ours(args):
                     ("postponed" if args.persistent == 3 else bool(args.persistent)),
                     shade_sort=None if args.shade_sort == "default" else args.shade_sort,
                     box_bits=args.box_bits, pipelines=args.pipelines)
+    if args.spectral == "hero":
+        B.SetSpectral(_abi.CG_SPECTRAL_HERO)
+    if args.roulette:
+        B.SetRoulette(args.roulette)
     clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         B.View(g, cam)
@@ -746,6 +750,7 @@ def run_ours(args):
             "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "samples_per_step": samples_per_step,
+                       "spectral": args.spectral, "roulette_from_depth": args.roulette,
                        "l2": "flushed between steps (256 MiB write)",
                        "queue_capacity": queue_capacity,
                        "parallelism": f"replicas x{ws}"},
@@ -822,6 +827,12 @@ def main():
                     help="four-wide child box precision (0 = library default, 32)")
     ap.add_argument("--forms", default="auto", choices=["auto", "on", "off"],
                     help="batched and served forms vs plain (auto: on at one GPU)")
+    ap.add_argument("--spectral", default="reference", choices=["reference", "hero"],
+                    help="wavelength sampling: the reference's one per sample (default) or hero "
+                         "(four per sample)")
+    ap.add_argument("--roulette", type=int, default=0,
+                    help="Russian roulette from this hit depth on (0 = off, as the reference; 3 = "
+                         "after the third bounce)")
     ap.add_argument("--shade-sort", default="default", choices=["default", "global", "block", "none"],
                     help="order of the rays the shading kernel takes (default: the library's, global)")
     args = ap.parse_args()
