@@ -18,10 +18,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-# CG_NVCC_DEFINES (e.g. "CG_SMITS_SHARED"): preprocessor switches of a kernel
-# variant; such builds keep their objects apart
+# CG_NVCC_DEFINES (e.g. "CG_SMITS_SHARED" or "CG_STEP_BUDGET=8"): preprocessor
+# switches of a kernel variant for measurements; such builds keep their objects
+# apart
 DEFINES = os.environ.get("CG_NVCC_DEFINES", "").split()
-BUILD = os.path.join(HERE, "_build" + ("_" + "_".join(DEFINES) if DEFINES else ""))
+BUILD = os.path.join(HERE, "_build" + ("_" + "_".join(DEFINES).replace("=", "-") if DEFINES else ""))
 LIB = os.path.join(HERE, "libcg_cuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -271,8 +271,15 @@ __device__ __forceinline__ void addShadowTerm(const WaveBuffers& wb, uint32_t i)
   }
 }
 
-constexpr int kStepBudget = 16;
-constexpr int kRefill = 8;
+// (CG_STEP_BUDGET / CG_REFILL override them for measurements)
+#ifndef CG_STEP_BUDGET
+#define CG_STEP_BUDGET 16
+#endif
+#ifndef CG_REFILL
+#define CG_REFILL 8
+#endif
+constexpr int kStepBudget = CG_STEP_BUDGET;
+constexpr int kRefill = CG_REFILL;
 // Closest-hit traversal stack entries per thread kept in shared memory
 // (dynamic shared memory of the persistent closest-hit launch: kShortStack * 4
 // bytes per thread).  Measured on the 1280x720 icosphere frame and the
