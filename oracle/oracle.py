@@ -41,6 +41,24 @@ def build(reference: bool = True) -> None:
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
 
 
+def use_native() -> bool:
+    """Switches this process to the oracle built for its own CPU
+    (-march=native, `make native`), building it if needed; for the timed CPU
+    baselines.  Must come before the first oracle call.  Returns False (and
+    keeps the portable build) if the native build fails."""
+    global LIB_PATH, _lib
+    native = os.path.join(HERE, "_build", "libcg_oracle_native.so")
+    try:
+        subprocess.run(["make", "-s", "-C", HERE, "native"], check=True, timeout=300,
+                       capture_output=True)
+    except (subprocess.SubprocessError, OSError):
+        return False
+    if _lib is None and os.path.exists(native):
+        LIB_PATH = native
+        return True
+    return LIB_PATH == native
+
+
 def _abi():
     import sys
     root = os.path.dirname(HERE)
