@@ -395,11 +395,13 @@ def test_converged_image_matches_reference_order_oracle(case, spectral):
     """GPU (keyed streams) vs the oracle in the reference's own RNG order
     (per-pixel PCG-hash streams consumed depth first, trace.wesl:22-89,
     render.wesl:7-18), both converged, on X, Y and Z: relative RMSE of the
-    8x8-block means <= 1 %, and few block-channels outside 3 sigma (sigma from
-    the spread of 16 or more independent frames on each side; with ~30
-    degrees of freedom a block-channel exceeds 3 sigma with probability
-    ~0.5 %, and the dispersive glass's weighted subtrees are heavy-tailed,
-    so up to 3 % of them, at least one, may).  The cases
+    8x8-block means <= 1 %, the RMS of the block-channels' z scores <= 1.5
+    (a bias would raise every z), and few block-channels outside 3 sigma
+    (sigma from the spread of 16 or more independent frames on each side;
+    with ~30 degrees of freedom a block-channel exceeds 3 sigma with
+    probability ~0.5 %, and the dispersive glass's subtrees that carry the
+    hero wavelength alone with weight 4 are heavy-tailed, which inflates that
+    rate, so up to 6 % of them, at least one, may).  The cases
     cover the reference's depth cut at 2, the rough dispersive dielectric of
     the icosphere configuration at depth 8 (tree fan-out 3, 2, 1, ...), and
     the instanced material mix at depth 12.  Primary-ray tie pixels are left
@@ -440,10 +442,12 @@ def test_converged_image_matches_reference_order_oracle(case, spectral):
     print(f"{name} ({'hero' if spectral else 'reference'} wavelengths): {int((~keep).sum())} "
           f"tie pixels excluded; relative RMSE {rmse:.4%} "
           f"(X/Y/Z {per_channel[0]:.3%}/{per_channel[1]:.3%}/{per_channel[2]:.3%}, noise floor "
-          f"{floor:.3%}), |z|>3 in {int((z > 3).sum())} of {z.size} block-channels")
+          f"{floor:.3%}), |z|>3 in {int((z > 3).sum())} of {z.size} block-channels, RMS z "
+          f"{float(np.sqrt(np.mean(z ** 2))):.2f}")
     assert rmse <= 0.01, rmse
     assert max(per_channel) <= 0.015, per_channel
-    assert (z > 3).sum() <= max(1, round(0.03 * z.size)), (z > 3).sum()
+    assert float(np.sqrt(np.mean(z ** 2))) <= 1.5, float(np.sqrt(np.mean(z ** 2)))
+    assert (z > 3).sum() <= max(1, round(0.06 * z.size)), (z > 3).sum()
     g.close()
     B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=2))
 
