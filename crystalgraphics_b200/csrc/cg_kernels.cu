@@ -1004,9 +1004,11 @@ __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers
   shadeLevel<kSort, kLobes, false>(sc, fc, wb, depth, parity);
 }
 
-// Hero-wavelength mode (level-wide shading order only).
+// Hero-wavelength mode (level-wide shading order only).  At most 128
+// registers: the group with transmission needs 109 without spills (ptxas
+// chose 96 with spills when left free).
 template <int kLobes>
-__global__ void __launch_bounds__(128) k_shade_hero(SceneView sc, FrameConst fc, WaveBuffers wb,
+__global__ void __maxnreg__(128) k_shade_hero(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                     int depth, int parity) {
   shadeLevel<kShadeSortGlobal, kLobes, true>(sc, fc, wb, depth, parity);
 }

@@ -199,6 +199,29 @@ def test_server_results_same_alone_and_in_the_mix(cornell):
     assert _close(mixed[0], ref) < RTOL
 
 
+def test_server_in_hero_mode_matches_the_batched_form(cornell):
+    """A server created while hero-wavelength sampling is on keeps that mode:
+    its requests equal the same views rendered by the batched form in hero
+    mode, alone and in a mix, and differ from reference-mode frames."""
+    s, g = cornell
+    c = s.camera
+    reqs = [(48, 40, 4, 15), (32, 32, 8, 16), (80, 60, 2, 17)]
+    views = [(c.position[:], c.direction[:], w, h, spp, seed) for w, h, spp, seed in reqs]
+    B.SetSpectral(_abi.CG_SPECTRAL_HERO)
+    try:
+        ref = B.batch_render(g, views)
+        with B.Server([g], 1 << 30) as sv:
+            ids = [sv.submit(0, c.position[:], c.direction[:], w, h, spp, seed)
+                   for w, h, spp, seed in reqs]
+            served = [sv.wait(i)[0] for i in ids]
+    finally:
+        B.SetSpectral(_abi.CG_SPECTRAL_REFERENCE)
+    plain = B.batch_render(g, views)
+    for a, b, p in zip(served, ref, plain):
+        assert _close(a, b) < RTOL
+        assert _close(p, b) > 10 * RTOL
+
+
 def test_server_admission_under_budget(cornell):
     s, g = cornell
     c = s.camera
