@@ -142,3 +142,14 @@ def test_alias_build_matches_reference_golden():
 
 def test_version_string():
     assert b"sm_100a" in B.lib.cg_version()
+
+
+def test_spectral_and_roulette_settings_check_their_arguments():
+    """Hero-wavelength mode and Russian roulette are environment settings:
+    an unknown mode or a start depth beyond the depth cap is rejected, and
+    without an environment the calls report it (no device is needed)."""
+    assert B.lib.cg_set_spectral(7) == _abi.CG_E_INVALID
+    assert B.lib.cg_set_roulette(65) == _abi.CG_E_INVALID
+    if not B.EnvStatus():
+        assert B.lib.cg_set_spectral(_abi.CG_SPECTRAL_HERO) == _abi.CG_E_NOT_INIT
+        assert B.lib.cg_set_roulette(3) == _abi.CG_E_NOT_INIT
