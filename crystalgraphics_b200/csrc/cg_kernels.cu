@@ -138,15 +138,11 @@ __global__ void k_gen(FrameConst fc, WaveBuffers wb, ChunkDesc ch) {
 constexpr int kNumKeys = 19;
 constexpr int kTicket = 6, kKeyCount = 8, kKeyCursor = 32;
 
-// Kinds are ordered so that each lobe group is a contiguous key range:
-// [2, 6) neither diffuse nor transmission, [6, 10) diffuse, [10, 14)
-// transmission, [14, 18) both (within a range: the specular / rough bits).
 __device__ __forceinline__ int shadeKeyOf(const SceneView& sc, int32_t inst, bool cut) {
   if (inst < 0) return 0;
   if (cut) return 1;
   const uint4 meta = __ldg(reinterpret_cast<const uint4*>(sc.inst + inst) + 3);
-  const uint32_t kind = (sc.mat[meta.y].volume >> kKindShift) & 15u;
-  return 2 + static_cast<int>(((kind >> 3) & 1u) * 8u + (kind & 1u) * 4u + ((kind >> 1) & 3u));
+  return 2 + static_cast<int>((sc.mat[meta.y].volume >> kKindShift) & 15u);
 }
 
 // The block's key counts of a keyed closest-hit launch (one shared array per
@@ -643,8 +639,8 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 
 // kLobes: the lobe group (kLobesAll unless the level is in global shading
 // order, where one launch per group takes its keys' contiguous range of the
-// permutation: keys [0, 2) misses and hits beyond the depth cut, then one range
-// per combination of the diffuse and transmission lobes; see shadeKeyOf).
+// permutation: keys [0, 2) misses and hits beyond the depth cut, [2, 10) opaque
+// kinds, [10, 18) kinds with transmission; see shadeKeyOf).
 // kSort (ShadeSort): kShadeSortBlock — before shading, every block sorts its
 // slice of the queue by shading key in shared memory (counting sort);
 // kShadeSortGlobal — the level was sorted (keys from the closest-hit kernel,
@@ -674,10 +670,8 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
   uint32_t lo = 0, hi = n;
   if (kSort == kShadeSortGlobal) {
     // after k_shade_scatter every cursor is the end of its key's range
-    constexpr int k0 = kLobes == 0 ? 0
-                                   : 2 + ((kLobes & kLobeTransmit) ? 8 : 0) +
-                                         ((kLobes & kLobeDiffuse) ? 4 : 0);
-    constexpr int k1 = kLobes == 0 ? 2 : k0 + 4;
+    constexpr int k0 = kLobes == 0 ? 0 : (kLobes & kLobeTransmit) ? 10 : 2;
+    constexpr int k1 = kLobes == 0 ? 2 : (kLobes & kLobeTransmit) ? kNumKeys - 1 : 10;
     lo = k0 == 0 ? 0u : min(wb.counts[kKeyCursor + k0 - 1], n);
     hi = min(wb.counts[kKeyCursor + k1 - 1], n);
   }
@@ -1165,25 +1159,21 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
                 int parity, const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
-  constexpr int kR = kLobeHit | kLobeReflect, kDR = kR | kLobeDiffuse, kRT = kR | kLobeTransmit;
   if (wb.hero) {  // hero-wavelength mode: level-wide order, one launch per lobe group
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
     k_shade_hero<0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade_hero<kR><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade_hero<kDR><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade_hero<kRT><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade_hero<kLobeHit | kLobeDiffuse | kLobeReflect><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
     k_shade_hero<kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    return 6;
+    return 4;
   }
   if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
     // one launch per lobe group, each over its keys' range of the permutation
     k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade<kShadeSortGlobal, kR><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade<kShadeSortGlobal, kDR><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade<kShadeSortGlobal, kRT><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    k_shade<kShadeSortGlobal, kLobeHit | kLobeDiffuse | kLobeReflect>
+        <<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
     k_shade<kShadeSortGlobal, kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    return 6;
+    return 4;
   }
   if (ls.shade_sort == kShadeSortBlock)
     k_shade<kShadeSortBlock><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);

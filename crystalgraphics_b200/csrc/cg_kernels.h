@@ -114,7 +114,7 @@ void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
                   const LaunchShape& ls, bool cut, cudaStream_t s);
 // Returns the number of kernels launched (one, or with the global sort the
-// scatter and one shading launch per lobe group: six).
+// scatter and one shading launch per lobe group: four).
 int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
                 int parity, const LaunchShape& ls, cudaStream_t s);
 void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
