@@ -254,6 +254,7 @@ int Renderer::init(int dev) {
   CG_CUDA(cudaEventCreate(&ev0));
   CG_CUDA(cudaEventCreate(&ev1));
   CG_CUDA(cudaMallocHost(&stats_host, kMaxPipelines * kStatsHostStride));
+  configureKernels();
   if (wl_tree) return CG_OK;  // adopted from a previous renderer
   CG_CUDA(cudaMalloc(&wl_tree, 65535 * sizeof(float)));
   CG_CUDA(cudaMalloc(&wl_const, 4 * sizeof(float)));

@@ -1116,6 +1116,25 @@ void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
   k_gen<<<(n + 255) / 256, 256, 0, s>>>(fc, wb, ch);
 }
 
+// Kernel attributes set once per device before any launch (never inside a
+// stream capture).  CG_CARVEOUT (a measurement switch): the shared-memory
+// share of the unified L1 / shared memory, in percent, requested for the
+// traversal and shading kernels; without it the driver's default.
+void configureKernels() {
+#ifdef CG_CARVEOUT
+  const int pct = CG_CARVEOUT;
+  cudaFuncSetAttribute(k_extend_persistent<false, kNodesWide4>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  cudaFuncSetAttribute(k_shadow_persistent<false, kNodesWide4>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  cudaFuncSetAttribute(k_shade<kShadeSortGlobal, kLobeHit | kLobeDiffuse | kLobeReflect>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  cudaFuncSetAttribute(k_shade<kShadeSortGlobal, kLobesAll>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  cudaGetLastError();
+#endif
+}
+
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
                   const LaunchShape& ls, bool cut, cudaStream_t s) {
   const int keys = ls.shade_sort == kShadeSortGlobal ? (cut ? 2 : 1) : 0;

@@ -129,6 +129,9 @@ void launchTraceClosest(const SceneView& sc, const float4* rays, uint32_t n, flo
                         int4* out_ids, uint32_t* status, int nodes, cudaStream_t s);
 
 int smCount();
+// Sets kernel attributes on the current device (once per device, outside any
+// stream capture).
+void configureKernels();
 
 }  // namespace cg
 
