@@ -685,6 +685,33 @@ def run_ours(args):
     prof = B.ReadProfile()
     B.SetProfiling(False)
 
+    # ---- the options beyond the reference on the same frame: Russian roulette
+    # after the third bounce (as configs[1] states it) and hero-wavelength
+    # sampling (four wavelengths per sample, as configs[0] states it); device
+    # time of the same number of frames, L2 flushed between them ----
+    variants = None
+    if (rank == 0 and args.spectral == "reference" and not args.roulette and
+            WORKLOAD_NAME == "icosphere" and args.case == "full"):
+        variants = {}
+        for name, on, off in (("roulette_after_bounce_3", lambda: B.SetRoulette(3),
+                               lambda: B.SetRoulette(0)),
+                              ("hero_wavelengths", lambda: B.SetSpectral(_abi.CG_SPECTRAL_HERO),
+                               lambda: B.SetSpectral(_abi.CG_SPECTRAL_REFERENCE))):
+            on()
+            for _ in range(2):
+                B.View(g, cam)
+            ms = 0.0
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                B.View(g, cam)
+                ms += B.LastStats().device_ms
+            vst = B.LastStats()
+            off()
+            variants[name] = {"value": samples_per_step * args.steps / (ms / 1e3) / 1e6,
+                              "unit": "Msamples/s", "ms_per_step": ms / args.steps,
+                              "extend_rays_per_step": int(vst.extend_rays)}
+
     # ---- counting pass: algorithmic work of the traversal kernels ----
     B.SetCounting(True)
     B.View(g, cam)
@@ -797,6 +824,8 @@ def run_ours(args):
             out["cpu_baseline"] = cpu
         if packing:
             out["host_packing_baseline"] = packing
+        if variants:
+            out["options_beyond_the_reference"] = variants
         if forms:
             out["forms_summary"] = forms_summary(forms)
             out["forms"] = forms
