@@ -692,7 +692,24 @@ def run_ours(args):
     variants = None
     if (rank == 0 and args.spectral == "reference" and not args.roulette and
             WORKLOAD_NAME == "icosphere" and args.case == "full"):
-        variants = {}
+
+        def frame_noise():
+            """Relative variance of a pixel over independent frames (fresh
+            sample streams, frame 0 each): the noise one frame leaves."""
+            films = []
+            for k in range(6):
+                B.SetSeed(7000 + k)
+                B.ViewSamples(g, cam, 0, SPP_)
+                films.append(B.ReadFilm().copy())
+            B.SetSeed(1000 * rank)
+            f = np.stack(films).astype(np.float64)
+            return float(f.var(0, ddof=1).mean() / max(f.mean() ** 2, 1e-30))
+
+        base_ms = sum(dev_ms) / len(dev_ms)
+        base_noise = frame_noise()
+        variants = {"reference_frame_relative_variance": base_noise,
+                    "efficiency": "time x variance of the reference sampler without roulette over "
+                                  "the option's: how much sooner it reaches the same image RMSE"}
         for name, on, off in (("roulette_after_bounce_3", lambda: B.SetRoulette(3),
                                lambda: B.SetRoulette(0)),
                               ("hero_wavelengths", lambda: B.SetSpectral(_abi.CG_SPECTRAL_HERO),
@@ -707,10 +724,14 @@ def run_ours(args):
                 B.View(g, cam)
                 ms += B.LastStats().device_ms
             vst = B.LastStats()
+            noise = frame_noise()
             off()
             variants[name] = {"value": samples_per_step * args.steps / (ms / 1e3) / 1e6,
                               "unit": "Msamples/s", "ms_per_step": ms / args.steps,
-                              "extend_rays_per_step": int(vst.extend_rays)}
+                              "extend_rays_per_step": int(vst.extend_rays),
+                              "frame_relative_variance": noise,
+                              "efficiency_vs_reference": (base_ms * base_noise) /
+                                                         (ms / args.steps * noise)}
 
     # ---- counting pass: algorithmic work of the traversal kernels ----
     B.SetCounting(True)
