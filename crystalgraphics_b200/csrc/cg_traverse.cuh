@@ -37,28 +37,6 @@ struct HitRec {
   uint32_t tri;   // global triangle slot
 };
 
-// Three-input minimum / maximum (sm_100's min.f32 / max.f32 with three
-// operands; NaN operands are dropped as by fminf / fmaxf).  The slab test of a
-// child box takes one of each instead of two.
-__device__ __forceinline__ float fmax3(float a, float b, float c) {
-#ifdef CG_NO_MINMAX3
-  return fmaxf(fmaxf(a, b), c);
-#else
-  float d;
-  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
-  return d;
-#endif
-}
-__device__ __forceinline__ float fmin3(float a, float b, float c) {
-#ifdef CG_NO_MINMAX3
-  return fminf(fminf(a, b), c);
-#else
-  float d;
-  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
-  return d;
-#endif
-}
-
 __device__ __forceinline__ float safeInv(float d) {
   return 1.0f / (fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d));
 }
@@ -372,8 +350,8 @@ __device__ __forceinline__ bool travSteps(const SceneView& sc, TravState& s, Sta
         const float a0 = fmaf(nxs[c], s.idx, -s.oix), a1 = fmaf(fxs[c], s.idx, -s.oix);
         const float b0 = fmaf(nys[c], s.idy, -s.oiy), b1 = fmaf(fys[c], s.idy, -s.oiy);
         const float c0 = fmaf(nzs[c], s.idz, -s.oiz), c1 = fmaf(fzs[c], s.idz, -s.oiz);
-        const float tmin = fmax3(a0, b0, fmaxf(c0, 0.0f));
-        const float tmx = fmin3(a1, b1, fminf(c1, s.best.t));
+        const float tmin = fmaxf(fmaxf(a0, b0), fmaxf(c0, 0.0f));
+        const float tmx = fminf(fminf(a1, b1), fminf(c1, s.best.t));
         const bool hit = kNodes == kNodesWide4Q ? (tmin <= tmx && links[c] != kEmptyLink)
                                                 : tmin <= tmx;
         k[c] = hit ? tmin : INFINITY;
@@ -534,8 +512,8 @@ __device__ __forceinline__ bool travStepsSpec(const SceneView& sc, TravState& s,
           const float a0 = fmaf(nxs[c], s.idx, -s.oix), a1 = fmaf(fxs[c], s.idx, -s.oix);
           const float b0 = fmaf(nys[c], s.idy, -s.oiy), b1 = fmaf(fys[c], s.idy, -s.oiy);
           const float c0 = fmaf(nzs[c], s.idz, -s.oiz), c1 = fmaf(fzs[c], s.idz, -s.oiz);
-          const float tmin = fmax3(a0, b0, fmaxf(c0, 0.0f));
-          const float tmx = fmin3(a1, b1, fminf(c1, s.best.t));
+          const float tmin = fmaxf(fmaxf(a0, b0), fmaxf(c0, 0.0f));
+          const float tmx = fminf(fminf(a1, b1), fminf(c1, s.best.t));
           const bool hit = kQuant ? (tmin <= tmx && links[c] != kEmptyLink) : tmin <= tmx;
           k[c] = hit ? tmin : INFINITY;
         }
@@ -667,8 +645,8 @@ __device__ __forceinline__ HitRec traceRay4(const SceneView& sc, float wox, floa
         const float a0 = fmaf(nxs[c], idx, -oix), a1 = fmaf(fxs[c], idx, -oix);
         const float b0 = fmaf(nys[c], idy, -oiy), b1 = fmaf(fys[c], idy, -oiy);
         const float c0 = fmaf(nzs[c], idz, -oiz), c1 = fmaf(fzs[c], idz, -oiz);
-        const float tmin = fmax3(a0, b0, fmaxf(c0, 0.0f));
-        const float tmx = fmin3(a1, b1, fminf(c1, best.t));
+        const float tmin = fmaxf(fmaxf(a0, b0), fmaxf(c0, 0.0f));
+        const float tmx = fminf(fminf(a1, b1), fminf(c1, best.t));
         // absent children: a point box at 1e30 (full precision) or the link (quantised)
         const bool hit = kQuant ? (tmin <= tmx && links[c] != kEmptyLink) : tmin <= tmx;
         k[c] = hit ? tmin : INFINITY;
