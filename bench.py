@@ -396,9 +396,10 @@ def _rel_diff(a, b):
 def _tuning_kwargs(t):
     return dict(queue_capacity=int(t.queue_capacity), extend_block=int(t.extend_block),
                 shade_block=int(t.shade_block), use_graph=int(t.use_graph),
-                bvh_width=int(t.bvh_width), persistent=int(t.persistent) != 2,
+                bvh_width=int(t.bvh_width),
+                persistent={2: False, 3: "postponed"}.get(int(t.persistent), True),
                 shade_sort={1: "global", 2: "none", 3: "block"}.get(int(t.shade_sort), "global"),
-                pipelines=int(t.pipelines))
+                pipelines=int(t.pipelines), traversal_threads=int(t.traversal_threads))
 
 
 def _plain_render(B, g, pos, d, w, h, spp, seed, depth, tuning=None, out=None):
@@ -625,12 +626,13 @@ def run_ours(args):
     samples_per_step = W_ * H_ * SPP_
 
     if (args.queue or args.bvh_width or args.persistent >= 0 or args.shade_sort != "default" or
-            args.box_bits or args.pipelines):
+            args.box_bits or args.pipelines or args.traversal_threads):
         B.SetTuning(queue_capacity=args.queue, bvh_width=args.bvh_width,
                     persistent=None if args.persistent < 0 else
                     ("postponed" if args.persistent == 3 else bool(args.persistent)),
                     shade_sort=None if args.shade_sort == "default" else args.shade_sort,
-                    box_bits=args.box_bits, pipelines=args.pipelines)
+                    box_bits=args.box_bits, pipelines=args.pipelines,
+                    traversal_threads=args.traversal_threads)
     if args.spectral == "hero":
         B.SetSpectral(_abi.CG_SPECTRAL_HERO)
     if args.roulette:
@@ -878,6 +880,9 @@ def main():
                          "postponed leaves)")
     ap.add_argument("--pipelines", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="chunk pipelines of View() (0 = library default, 2)")
+    ap.add_argument("--traversal-threads", type=int, default=0,
+                    help="threads per SM of the persistent traversal grids (0 = library default, "
+                         "1024)")
     ap.add_argument("--box-bits", type=int, default=0, choices=[0, 8, 32],
                     help="four-wide child box precision (0 = library default, 32)")
     ap.add_argument("--forms", default="auto", choices=["auto", "on", "off"],

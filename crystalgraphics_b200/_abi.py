@@ -100,7 +100,7 @@ class CgViewDesc(C.Structure):
 class CgTuning(C.Structure):
     _fields_ = [("queue_capacity", u32), ("extend_block", u32), ("shade_block", u32),
                 ("use_graph", u32), ("bvh_width", u32), ("persistent", u32), ("shade_sort", u32),
-                ("box_bits", u32), ("pipelines", u32), ("_pad", u32)]
+                ("box_bits", u32), ("pipelines", u32), ("traversal_threads", u32)]
 
 
 class CgRequest(C.Structure):

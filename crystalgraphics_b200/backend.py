@@ -495,7 +495,8 @@ def GetSpectral() -> int:
 
 
 def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_width=0,
-              persistent=None, shade_sort=None, box_bits=0, pipelines=0) -> None:
+              persistent=None, shade_sort=None, box_bits=0, pipelines=0,
+              traversal_threads=0) -> None:
     """0 (or None for the two switches) keeps the current value.  shade_sort:
     True / "global" (level-wide sort by material kind), "block" (per block),
     False / "none".  persistent: True (persistent warps), False (one ray per
@@ -509,7 +510,7 @@ def SetTuning(queue_capacity=0, extend_block=0, shade_block=0, use_graph=1, bvh_
     t = _abi.CgTuning(queue_capacity, extend_block, shade_block, use_graph, bvh_width,
                       0 if persistent is None else
                       (3 if persistent == "postponed" else 1 if persistent else 2), sort, box_bits,
-                      pipelines)
+                      pipelines, traversal_threads)
     _check(lib.cg_set_tuning(C.byref(t)))
 
 

@@ -459,6 +459,7 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
   ls.nodes = nodeFormatOf(tuning);
   ls.persistent = tuning.persistent != 2u;
   ls.spec = tuning.persistent == 3u;
+  ls.traversal_threads = tuning.traversal_threads ? tuning.traversal_threads : 1024u;
   const uint32_t cut_depth = std::max(1u, std::min(caps.trace_depth, 64u)) - 1u;
   ls.shade_sort = tuning.shade_sort == 2u   ? kShadeSortNone
                   : tuning.shade_sort == 3u ? kShadeSortBlock
@@ -1241,6 +1242,13 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
     if (t->pipelines > static_cast<uint32_t>(Renderer::kMaxPipelines))
       return fail(CG_E_INVALID, "pipelines must be 1 to 4");
     if (t->shade_sort > 3u) return fail(CG_E_INVALID, "shade_sort must be 0..3");
+    {
+      const uint32_t eb = t->extend_block ? t->extend_block : g_env->tuning.extend_block;
+      if (t->traversal_threads &&
+          (t->traversal_threads > 1024u || t->traversal_threads < eb || t->traversal_threads % eb))
+        return fail(CG_E_INVALID,
+                    "traversal_threads must be a multiple of extend_block in [extend_block, 1024]");
+    }
     cg_tuning& g = g_env->tuning;
     if (t->queue_capacity) g.queue_capacity = t->queue_capacity;
     if (t->box_bits) g.box_bits = t->box_bits;
@@ -1250,6 +1258,8 @@ CG_API int cg_set_tuning(const cg_tuning* t) {
     if (t->bvh_width) g.bvh_width = t->bvh_width;
     if (t->persistent) g.persistent = t->persistent == 2u || t->persistent == 3u ? t->persistent : 1u;
     if (t->shade_sort) g.shade_sort = t->shade_sort;
+    if (t->traversal_threads) g.traversal_threads = t->traversal_threads;
+    if (g.traversal_threads % g.extend_block) g.traversal_threads = 1024u;  // a new block size
     g_env->tuning.use_graph = t->use_graph;
     g_env->dropAllGraphs();
     return CG_OK;

@@ -127,7 +127,7 @@ struct Renderer {
   bool counting = false;
   // 64M rays per level queue (~9.7 GB of path state): large chunks keep every
   // level's launch full
-  cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u, 2u, 0u};
+  cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u, 2u, 1024u};
   DeviceArena wave_arena;
   WaveBuffers wave{};
   // the extra chunk pipelines of enqueueViews (pipeline 0 is `stream` with

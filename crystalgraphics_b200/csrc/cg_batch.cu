@@ -268,13 +268,16 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32
         consider(t);
       }
     }
-    {
+    {  // pipelines together with the traversal grids' residency: fewer traversal
+       // threads per SM let one pipeline's shading run beside another's traversal
       const cg_tuning base = winner;
-      for (uint32_t pl : {1u, 2u, 3u, 4u}) {
-        cg_tuning t = base;
-        t.pipelines = pl;
-        consider(t);
-      }
+      for (uint32_t pl : {1u, 2u, 3u, 4u})
+        for (uint32_t tt : {1024u, 768u}) {
+          cg_tuning t = base;
+          t.pipelines = pl;
+          t.traversal_threads = tt % t.extend_block ? 1024u : tt;
+          consider(t);
+        }
     }
     {
       const cg_tuning base = winner;
@@ -289,6 +292,7 @@ CG_API int cg_autotune_views(cg_scene_t scene, const cg_view_desc* views, uint32
       for (uint32_t b : {64u, 128u, 256u}) {
         cg_tuning t = base;
         t.extend_block = b;
+        if (t.traversal_threads % b) t.traversal_threads = 1024u;
         consider(t);
       }
     }

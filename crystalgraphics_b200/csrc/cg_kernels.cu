@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <type_traits>
 
@@ -1135,19 +1136,12 @@ void configureKernels() {
 #endif
 }
 
-// Threads per SM of the persistent traversal grids (a measurement switch,
-// CG_TRAVERSAL_THREADS_PER_SM; 1024 = the register file's limit at 64
-// registers per thread).
-#ifndef CG_TRAVERSAL_THREADS_PER_SM
-#define CG_TRAVERSAL_THREADS_PER_SM 1024u
-#endif
-
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
                   const LaunchShape& ls, bool cut, cudaStream_t s) {
   const int keys = ls.shade_sort == kShadeSortGlobal ? (cut ? 2 : 1) : 0;
   const uint32_t block = ls.extend_block;
   if (ls.persistent) {  // one resident grid: 64 registers -> 65536 / (64 * block) blocks per SM
-    const uint32_t g = gridFor(CG_TRAVERSAL_THREADS_PER_SM / block);
+    const uint32_t g = gridFor(std::max(1u, ls.traversal_threads / block));
     const size_t smem = size_t(kShortStack) * block * sizeof(int32_t);
     if (ls.spec && ls.nodes != kNodesBinary) {  // postponed leaves
       const bool q = ls.nodes == kNodesWide4Q;
@@ -1212,7 +1206,7 @@ void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s) {
   const uint32_t block = ls.extend_block;
   if (ls.persistent) {
-    const uint32_t g = gridFor(CG_TRAVERSAL_THREADS_PER_SM / block);
+    const uint32_t g = gridFor(std::max(1u, ls.traversal_threads / block));
     switch (ls.nodes * 2 + (counting ? 1 : 0)) {
       case kNodesBinary * 2: k_shadow_persistent<false, kNodesBinary><<<g, block, 0, s>>>(sc, wb); break;
       case kNodesBinary * 2 + 1: k_shadow_persistent<true, kNodesBinary><<<g, block, 0, s>>>(sc, wb); break;

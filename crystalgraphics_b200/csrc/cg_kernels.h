@@ -103,6 +103,7 @@ struct LaunchShape {
   int nodes = kNodesWide4;   // NodeFormat of the traversal
   bool persistent = true;    // persistent warps with lane refill
   bool spec = false;         // with persistent four-wide closest hits: postponed leaves
+  uint32_t traversal_threads = 1024;  // threads per SM of the persistent traversal grids
   int shade_sort = kShadeSortGlobal;  // ShadeSort: order of the rays the shading kernel takes
 };
 

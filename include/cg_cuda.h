@@ -466,7 +466,12 @@ typedef struct cg_tuning {
   uint32_t pipelines;   /* chunk pipelines of View() and cg_batch_render, 1 to
                            4: chunk k runs on stream k mod pipelines with that
                            stream's own ray queues (2 = default); 0 = keep */
-  uint32_t _pad;
+  uint32_t traversal_threads;  /* threads per SM of the persistent traversal
+                           grids: a multiple of extend_block in [extend_block,
+                           1024] (1024 = default: the register file's limit at
+                           64 registers per thread); fewer leave SM room for
+                           another pipeline's shading launches to run beside
+                           them; 0 = keep */
 } cg_tuning;
 CG_API int cg_set_tuning(const cg_tuning* tuning);
 CG_API int cg_get_tuning(cg_tuning* out);

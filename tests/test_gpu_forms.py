@@ -276,6 +276,8 @@ def test_server_cancel_and_timeout(cornell):
                                      dict(bvh_width=4, persistent=True, shade_sort="block"),
                                      dict(bvh_width=4, persistent=False, box_bits=8),
                                      dict(bvh_width=4, persistent="postponed"),
+                                     dict(bvh_width=4, persistent=True, traversal_threads=768,
+                                          pipelines=3),
                                      dict(bvh_width=4, persistent="postponed", box_bits=8)])
 def test_traversal_variants_render_the_same_samples(variant):
     """Binary or four-wide trees, one ray per thread or persistent warps, rays
@@ -303,6 +305,7 @@ def test_autotune_returns_a_valid_tuning(cornell):
     t = B.autotune(g, (s.camera.position[:], s.camera.direction[:], 96, 96, 4, 1))
     assert t.queue_capacity >= 4096 and t.extend_block % 32 == 0 and t.shade_block % 32 == 0
     assert t.bvh_width in (2, 4) and t.box_bits in (8, 32) and t.shade_sort in (1, 2, 3)
+    assert 0 < t.traversal_threads <= 1024 and t.traversal_threads % t.extend_block == 0
     # a tuning found on probe views renders the batch like the default tuning
     views = _views(s)
     ref = B.batch_render(g, views)
@@ -311,12 +314,14 @@ def test_autotune_returns_a_valid_tuning(cornell):
     for x, y in zip(B.batch_render(g, views), ref):
         assert _close(x, y) < RTOL
     B.SetTuning(queue_capacity=64 << 20, extend_block=128, shade_block=128, use_graph=1,
-                bvh_width=4, persistent=True, shade_sort=True, box_bits=32, pipelines=2)
+                bvh_width=4, persistent=True, shade_sort=True, box_bits=32, pipelines=2,
+                traversal_threads=1024)
 
 
 def test_tuning_rejects_out_of_range_values(cornell):
     before = B.GetTuning()
     for bad in (dict(extend_block=512), dict(extend_block=48), dict(shade_block=2048),
+                dict(traversal_threads=1056), dict(traversal_threads=100),
                 dict(queue_capacity=1024), dict(pipelines=5), dict(bvh_width=3),
                 dict(box_bits=16)):
         with pytest.raises(B.Error) as e:
