@@ -475,7 +475,8 @@ void Renderer::enqueueChunk(const SceneDev& scene, uint32_t view_count, const Vi
     launchExtend(scene.view, wb, parity, counting, ls, d >= cut_depth, s);
     profEnd(s);
     profBegin(CG_K_SHADE, s);
-    const int shade_kernels = launchShade(scene.view, fc, wb, static_cast<int>(d), parity, ls, s);
+    const int shade_kernels =
+        launchShade(scene.view, fc, wb, static_cast<int>(d), parity, ls, s, plan.shadow[d]);
     profEnd(s);
     rec.launches += 1 + static_cast<uint32_t>(shade_kernels);
     if (plan.shadow[d]) {

@@ -661,7 +661,9 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 // the hero alone with weight 4 — over the four equally likely heroes of one
 // wavelength set that is the reference's estimator at each of them.
 // Emission is exact per wavelength.
-template <int kSort, int kLobes, bool kHero>
+// kLight: the level can draw light samples (false: no ray of the level has a
+// light-sample count, so the light sample and the light pdf's code are left out).
+template <int kSort, int kLobes, bool kHero, bool kLight = true>
 __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst& fc,
                                            const WaveBuffers& wb, int depth, int parity) {
   stageSmitsTables();
@@ -785,7 +787,7 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
         } else {
           m = decode(dmat, lambda, spos);
         }
-        const Counts c = counts(m, sc.has_lights != 0u, depth, caps);
+        const Counts c = counts(m, kLight && sc.has_lights != 0u, depth, caps);
         // hero mode: the other wavelengths' materials, and whether all four
         // sample alike here (same counts; the same refraction index where a
         // transmission lobe is sampled)
@@ -999,19 +1001,19 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
 
 // At most 96 registers: five blocks of 128 threads per SM (the lobe groups
 // need 90-93 without spills; uncapped they took 98, which left room for four).
-template <int kSort, int kLobes = kLobesAll>
+template <int kSort, int kLobes = kLobesAll, bool kLight = true>
 __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb, int depth,
                                         int parity) {
-  shadeLevel<kSort, kLobes, false>(sc, fc, wb, depth, parity);
+  shadeLevel<kSort, kLobes, false, kLight>(sc, fc, wb, depth, parity);
 }
 
 // Hero-wavelength mode (level-wide shading order only).  At most 128
 // registers: the group with transmission needs 109 without spills (ptxas
 // chose 96 with spills when left free).
-template <int kLobes>
+template <int kLobes, bool kLight = true>
 __global__ void __maxnreg__(128) k_shade_hero(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                     int depth, int parity) {
-  shadeLevel<kShadeSortGlobal, kLobes, true>(sc, fc, wb, depth, parity);
+  shadeLevel<kShadeSortGlobal, kLobes, true, kLight>(sc, fc, wb, depth, parity);
 }
 
 // ---- resolve: spp loop sum + running mean + sRGB (compute.wesl:41-61) -----------
@@ -1176,23 +1178,35 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
 }
 
 int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
-                int parity, const LaunchShape& ls, cudaStream_t s) {
+                int parity, const LaunchShape& ls, cudaStream_t s, bool light) {
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
+  constexpr int kOpaque = kLobeHit | kLobeDiffuse | kLobeReflect;
   if (wb.hero) {  // hero-wavelength mode: level-wide order, one launch per lobe group
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
-    k_shade_hero<0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade_hero<kLobeHit | kLobeDiffuse | kLobeReflect><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade_hero<kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    if (light) {
+      k_shade_hero<0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade_hero<kOpaque><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade_hero<kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    } else {
+      k_shade_hero<0, false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade_hero<kOpaque, false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade_hero<kLobesAll, false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    }
     return 4;
   }
   if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
     // one launch per lobe group, each over its keys' range of the permutation
-    k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade<kShadeSortGlobal, kLobeHit | kLobeDiffuse | kLobeReflect>
-        <<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
-    k_shade<kShadeSortGlobal, kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    if (light) {
+      k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade<kShadeSortGlobal, kOpaque><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade<kShadeSortGlobal, kLobesAll><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    } else {
+      k_shade<kShadeSortGlobal, 0, false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade<kShadeSortGlobal, kOpaque, false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade<kShadeSortGlobal, kLobesAll, false><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+    }
     return 4;
   }
   if (ls.shade_sort == kShadeSortBlock)

@@ -116,8 +116,10 @@ void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool c
                   const LaunchShape& ls, bool cut, cudaStream_t s);
 // Returns the number of kernels launched (one, or with the global sort the
 // scatter and one shading launch per lobe group: four).
+// `light`: the level can draw light samples (false leaves the light-sample code
+// out of the level's global-order shading launches).
 int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,
-                int parity, const LaunchShape& ls, cudaStream_t s);
+                int parity, const LaunchShape& ls, cudaStream_t s, bool light = true);
 void launchShadow(const SceneView& sc, const WaveBuffers& wb, bool counting,
                   const LaunchShape& ls, cudaStream_t s);
 void launchResolve(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
