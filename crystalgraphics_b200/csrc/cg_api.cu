@@ -317,7 +317,8 @@ int allocWave(DeviceArena& arena, WaveBuffers& w, uint32_t capacity) {
                           Q * 16, Q * 16, Q * 4,                         // shadow queue
                           Q * 4,  Q * 4,  Q * 4,                         // sample slots
                           Q,      Q * 4,                                 // shading key, order
-                          256,    256,    256};                          // counts, stats, status
+                          256,    256,    256,                           // counts, stats, status
+                          Q * 16, Q * 4};                                // light-pdf deferral
   size_t total = 0;
   for (size_t b : parts) total += align256(b);
   w = WaveBuffers{};
@@ -349,6 +350,8 @@ int allocWave(DeviceArena& arena, WaveBuffers& w, uint32_t capacity) {
   w.counts = reinterpret_cast<uint32_t*>(take(256));
   w.stats = reinterpret_cast<unsigned long long*>(take(256));
   w.status = reinterpret_cast<uint32_t*>(take(256));
+  w.defer = reinterpret_cast<float4*>(take(Q * 16));
+  w.defer_dist = reinterpret_cast<float*>(take(Q * 4));
   w.capacity = capacity;
   w.sample_capacity = capacity;
   CG_CUDA(cudaMemset(w.counts, 0, 256));

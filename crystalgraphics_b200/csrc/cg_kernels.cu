@@ -420,28 +420,42 @@ __global__ void __launch_bounds__(256, 4) k_shadow(SceneView sc, WaveBuffers wb)
 
 // ---- light pdf: sum over every emissive triangle the ray meets -------------------
 // (pdf/emission.wesl:120-179).  A BVH over the emissive triangles finds them;
-// the terms are added in traversal order rather than buffer order.
+// the terms are added in traversal order rather than buffer order.  Every
+// operation is rounded explicitly (no contraction to FMA), so each compiled
+// copy of the walk (inside a shading kernel, or in k_light_pdf) returns the
+// same bits for the same ray: whether a ray grazing a triangle edge counts
+// that triangle must not depend on which kernel asked.
+__device__ __forceinline__ float dotRn(V3 a, V3 b) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ V3 crossRn(V3 a, V3 b) {
+  return V3{__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+            __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+
 __device__ __forceinline__ float triangleHitDist(V3 rp, V3 rd, const DevLightTri& L) {
-  V3 e1 = ld3(L.e1), e2 = ld3(L.e2);
-  V3 pv = cross(rd, e2);
-  float det = dot(e1, pv);
+  const V3 e1 = ld3(L.e1), e2 = ld3(L.e2);
+  const V3 pv = crossRn(rd, e2);
+  const float det = dotRn(e1, pv);
   if (fabsf(det) <= 1e-3f) return -1.0f;
-  float inv_det = 1.0f / det;
-  V3 tv = rp - ld3(L.v0);
-  float bu = dot(tv, pv) * inv_det;
+  const float inv_det = __fdiv_rn(1.0f, det);
+  const V3 tv{__fsub_rn(rp.x, L.v0[0]), __fsub_rn(rp.y, L.v0[1]), __fsub_rn(rp.z, L.v0[2])};
+  const float bu = __fmul_rn(dotRn(tv, pv), inv_det);
   if (bu < 0.0f || bu > 1.0f) return -1.0f;
-  V3 qv = cross(tv, e1);
-  float bv = dot(rd, qv) * inv_det;
-  if (bv < 0.0f || bu + bv > 1.0f) return -1.0f;
-  float hd = dot(e2, qv) * inv_det;
+  const V3 qv = crossRn(tv, e1);
+  const float bv = __fmul_rn(dotRn(rd, qv), inv_det);
+  if (bv < 0.0f || __fadd_rn(bu, bv) > 1.0f) return -1.0f;
+  const float hd = __fmul_rn(dotRn(e2, qv), inv_det);
   return hd > 1e-3f ? hd : -1.0f;
 }
 
 __device__ float lightPdf(const SceneView& sc, V3 pos, V3 next, uint32_t* status) {
   if (!sc.has_lights) return 0.0f;
-  const V3 rd = normalize(next);
+  const float len = __fsqrt_rn(dotRn(next, next));
+  const V3 rd{__fdiv_rn(next.x, len), __fdiv_rn(next.y, len), __fdiv_rn(next.z, len)};
   const float idx = safeInv(rd.x), idy = safeInv(rd.y), idz = safeInv(rd.z);
-  const float oix = pos.x * idx, oiy = pos.y * idy, oiz = pos.z * idz;
+  const float oix = __fmul_rn(pos.x, idx), oiy = __fmul_rn(pos.y, idy), oiz = __fmul_rn(pos.z, idz);
   int32_t stack[32];
   int sp = 0;
   int32_t node = 0;
@@ -486,8 +500,8 @@ __device__ float lightPdf(const SceneView& sc, V3 pos, V3 next, uint32_t* status
       const DevLightTri L = sc.light_tri[first + k];
       const float hd = triangleHitDist(pos, rd, L);
       if (hd <= 0.0f) continue;
-      const float lp = fabsf(dot(ld3(L.n), -rd));
-      pdf += L.area_pdf * hd * hd / fmaxf(lp, 1e-3f);
+      const float lp = fabsf(dotRn(ld3(L.n), rd));
+      pdf = __fadd_rn(pdf, __fdiv_rn(__fmul_rn(__fmul_rn(L.area_pdf, hd), hd), fmaxf(lp, 1e-3f)));
     }
     node = sp > 0 ? stack[--sp] : kDone;
   }
@@ -516,12 +530,11 @@ enum { M_NONE = 0, M_DIFFUSE = 1, M_SREFL = 2, M_RREFL = 3, M_STRANS = 4, M_RTRA
 constexpr int kLobeHit = 1, kLobeDiffuse = 2, kLobeReflect = 4, kLobeTransmit = 8;
 constexpr int kLobesAll = kLobeHit | kLobeDiffuse | kLobeReflect | kLobeTransmit;
 
+// The lobes' part of the denominator: the sum before the light term is added.
 template <int kLobes = kLobesAll>
-__device__ __forceinline__ float balanceDenom(const SceneView& sc, V3 curr, V3 next, const Surf& s,
-                                              const Mat& m, const Counts& c, int model,
-                                              float model_pdf, float light_pdf_in,
-                                              uint32_t* status) {
-  float pd = 0.0f, psr = 0.0f, prr = 0.0f, pst = 0.0f, prt = 0.0f, pl = 0.0f;
+__device__ __forceinline__ float balanceSum(V3 curr, V3 next, const Surf& s, const Mat& m,
+                                            const Counts& c, int model, float model_pdf) {
+  float pd = 0.0f, psr = 0.0f, prr = 0.0f, pst = 0.0f, prt = 0.0f;
   if ((kLobes & kLobeDiffuse) && c.diffuse)
     pd = model == M_DIFFUSE ? model_pdf : diffusePdf(curr, next, s);
   if ((kLobes & kLobeReflect) && c.specular_reflect)
@@ -532,13 +545,24 @@ __device__ __forceinline__ float balanceDenom(const SceneView& sc, V3 curr, V3 n
     pst = model == M_STRANS ? model_pdf : specularTransmitPdf(curr, next, s, m);
   if ((kLobes & kLobeTransmit) && c.rough_transmit)
     prt = model == M_RTRANS ? model_pdf : roughTransmitPdf(curr, next, s, m);
+  // rounded explicitly: the deferred light term (k_light_pdf) is added to this
+  // value and must give the denominator balanceDenom gives
+  float sum = __fmul_rn(static_cast<float>(c.diffuse), pd);
+  sum = __fadd_rn(sum, __fmul_rn(static_cast<float>(c.specular_reflect), psr));
+  sum = __fadd_rn(sum, __fmul_rn(static_cast<float>(c.rough_reflect), prr));
+  sum = __fadd_rn(sum, __fmul_rn(static_cast<float>(c.specular_transmit), pst));
+  return __fadd_rn(sum, __fmul_rn(static_cast<float>(c.rough_transmit), prt));
+}
+
+template <int kLobes = kLobesAll>
+__device__ __forceinline__ float balanceDenom(const SceneView& sc, V3 curr, V3 next, const Surf& s,
+                                              const Mat& m, const Counts& c, int model,
+                                              float model_pdf, float light_pdf_in,
+                                              uint32_t* status) {
+  const float sum = balanceSum<kLobes>(curr, next, s, m, c, model, model_pdf);
+  float pl = 0.0f;
   if (c.light) pl = light_pdf_in >= 0.0f ? light_pdf_in : lightPdf(sc, s.pos, next, status);
-  return fmaxf(static_cast<float>(c.diffuse) * pd + static_cast<float>(c.specular_reflect) * psr +
-                   static_cast<float>(c.rough_reflect) * prr +
-                   static_cast<float>(c.specular_transmit) * pst +
-                   static_cast<float>(c.rough_transmit) * prt +
-                   static_cast<float>(c.light) * pl,
-               1e-6f);
+  return fmaxf(__fadd_rn(sum, __fmul_rn(static_cast<float>(c.light), pl)), 1e-6f);
 }
 
 // spawnSurfaceRay (spawn_surface_ray.wesl:4-15)
@@ -663,7 +687,9 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 // Emission is exact per wavelength.
 // kLight: the level can draw light samples (false: no ray of the level has a
 // light-sample count, so the light sample and the light pdf's code are left out).
-template <int kSort, int kLobes, bool kHero, bool kLight = true>
+// kDefer (with kLight, not in hero mode): children leave the light-pdf term of
+// their denominators to k_light_pdf (WaveBuffers::defer).
+template <int kSort, int kLobes, bool kHero, bool kLight = true, bool kDefer = false>
 __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst& fc,
                                            const WaveBuffers& wb, int depth, int parity) {
   stageSmitsTables();
@@ -716,10 +742,14 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
     // hero mode: per child the other wavelengths' weights and the flags (bit 0:
     // the hero alone below)
     float4 chw[kHero ? 4 : 1];
+    // kDefer: per child its denominator without the light-pdf term (x; -1:
+    // the weight is final) and its lobe value (y)
+    float2 cha[kDefer ? 4 : 1];
     uint32_t nch = 0;
     bool shadow = false;
     float4 sh_o = make_float4(0, 0, 0, 0), sh_d = make_float4(0, 0, 0, 0);
     float4 sh_x = make_float4(0, 0, 0, 0);  // hero mode: the other wavelengths' terms
+    V3 dpos{0.0f, 0.0f, 0.0f};  // the hit, for the children's deferred light-pdf terms
     uint32_t slot = 0;
     if (i < n) {
       const float4 o4 = wb.ray_o[parity][i];
@@ -817,10 +847,28 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
         addL = W * m.emission;
         const V3 curr = rd;
         uint32_t ti = 0;  // transport sample index (child key)
-        const bool roulette = fc.roulette != 0u && static_cast<uint32_t>(depth) >= fc.roulette;
+        // kDefer: a child whose denominator has a light term leaves it to
+        // k_light_pdf (the light-pdf walk then runs in a small kernel at full
+        // occupancy, not in this one): it carries the parent's weight, and its
+        // lobe value and denominator without the light term go beside it, so
+        // the weight is completed as W * (dist / denom) like the others.  The
+        // light count is 0
+        // or 1 (the emission budget is capped at 1), and roulette, which needs
+        // the final weight, is never active on a level launched with kDefer.
+        const bool roulette =
+            !kDefer && fc.roulette != 0u && static_cast<uint32_t>(depth) >= fc.roulette;
+        if constexpr (kDefer) dpos = s.pos;
         auto push = [&](V3 next, int model, float prob, float dist) {
-          const float denom = balanceDenom<kLobes>(sc, curr, next, s, m, c, model, prob, -1.0f,
-                                                   wb.status);
+          float denom = 1.0f, a = -1.0f;
+          if constexpr (kDefer) {
+            a = balanceSum<kLobes>(curr, next, s, m, c, model, prob);
+            if (c.light == 0u) {  // nothing to defer: balanceDenom's value
+              denom = fmaxf(a, 1e-6f);
+              a = -1.0f;
+            }
+          } else {
+            denom = balanceDenom<kLobes>(sc, curr, next, s, m, c, model, prob, -1.0f, wb.status);
+          }
           const float coeff = dist / denom;
           const uint32_t ck = childKey(key, ti++);
           if constexpr (kHero) {
@@ -848,7 +896,13 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
           } else {
             float cw = W * coeff;
             if (roulette && cw != 0.0f) cw = cw * rouletteFactor(cw, ck);
-            if (cw != 0.0f) ch[nch++] = Child{spawnOrigin(s, next), next, cw, ck};
+            if (cw != 0.0f) {
+              if constexpr (kDefer) {
+                cha[nch] = make_float2(a, dist);
+                if (a != -1.0f) cw = W;  // completed by k_light_pdf
+              }
+              ch[nch++] = Child{spawnOrigin(s, next), next, cw, ck};
+            }
           }
         };
         // sampleModels (sample.wesl:301-425) in its lobe order
@@ -978,6 +1032,10 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
           wb.ray_d[out][pos] = make_float4(ch[k].d.x, ch[k].d.y, ch[k].d.z, __uint_as_float(ch[k].key));
           wb.ray_slot[out][pos] = slot;
           if constexpr (kHero) wb.ray_w[out][pos] = chw[k];
+          if constexpr (kDefer) {
+            wb.defer[pos] = make_float4(dpos.x, dpos.y, dpos.z, cha[k].x);
+            wb.defer_dist[pos] = cha[k].y;
+          }
         }
       }
     }
@@ -1001,10 +1059,10 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
 
 // At most 96 registers: five blocks of 128 threads per SM (the lobe groups
 // need 90-93 without spills; uncapped they took 98, which left room for four).
-template <int kSort, int kLobes = kLobesAll, bool kLight = true>
+template <int kSort, int kLobes = kLobesAll, bool kLight = true, bool kDefer = false>
 __global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb, int depth,
                                         int parity) {
-  shadeLevel<kSort, kLobes, false, kLight>(sc, fc, wb, depth, parity);
+  shadeLevel<kSort, kLobes, false, kLight, kDefer>(sc, fc, wb, depth, parity);
 }
 
 // Hero-wavelength mode (level-wide shading order only).  At most 128
@@ -1014,6 +1072,28 @@ template <int kLobes, bool kLight = true>
 __global__ void __maxnreg__(128) k_shade_hero(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                     int depth, int parity) {
   shadeLevel<kShadeSortGlobal, kLobes, true, kLight>(sc, fc, wb, depth, parity);
+}
+
+// Completes the weights of the children a light-sampling level deferred
+// (WaveBuffers::defer): the light-pdf sum along the child's direction from its
+// parent hit (emission.wesl:120-149) joins the rest of the balance-heuristic
+// denominator, fmaxf(lobes + light, 1e-6) as balancePdfDenominator
+// (sample.wesl:505-554) forms it, and the weight becomes W * (dist / denom)
+// as the shading kernel forms it for the other children (W: the stored parent
+// weight, dist: the stored lobe value).  One ray per thread, a grid-strided
+// loop over the level's queue.
+__global__ void __launch_bounds__(256) k_light_pdf(SceneView sc, WaveBuffers wb, int out) {
+  const uint32_t n = min(wb.counts[out], wb.capacity);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float4 dp = wb.defer[i];
+    if (dp.w == -1.0f) continue;  // not deferred (the lobes' sum is >= 0 or NaN)
+    const float4 d4 = wb.ray_d[out][i];
+    const float pl = lightPdf(sc, V3{dp.x, dp.y, dp.z}, V3{d4.x, d4.y, d4.z}, wb.status);
+    const float denom = fmaxf(__fadd_rn(dp.w, pl), 1e-6f);  // balanceDenom's sum, light count 1
+    float* wp = reinterpret_cast<float*>(wb.ray_o[out] + i) + 3;
+    *wp = *wp * (wb.defer_dist[i] / denom);
+  }
 }
 
 // ---- resolve: spp loop sum + running mean + sRGB (compute.wesl:41-61) -----------
@@ -1198,6 +1278,15 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
   if (ls.shade_sort == kShadeSortGlobal) {  // keys and counts came with the closest hits
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
     // one launch per lobe group, each over its keys' range of the permutation
+    // the light-pdf terms in a separate pass (not where roulette needs the
+    // final weights)
+    if (light && wb.defer && wb.defer_dist && !(fc.roulette != 0u && static_cast<uint32_t>(depth) >= fc.roulette)) {
+      k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade<kShadeSortGlobal, kOpaque, true, true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade<kShadeSortGlobal, kLobesAll, true, true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_light_pdf<<<gridFor(8u), 256, 0, s>>>(sc, wb, parity ^ 1);
+      return 5;
+    }
     if (light) {
       k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
       k_shade<kShadeSortGlobal, kOpaque><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);

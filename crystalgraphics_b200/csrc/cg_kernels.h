@@ -71,6 +71,16 @@ struct WaveBuffers {
   float4* sh_w;
   float4* s_L4;
   uint32_t hero;
+  // per queued ray of a level that draws light samples: the hit position of
+  // its parent (xyz) and its balance-heuristic denominator without the light
+  // term (w; -1: the ray's weight is final), and the lobe value the weight is
+  // still to be multiplied by (defer_dist; ray_o.w holds the parent's weight
+  // meanwhile).  k_light_pdf adds the light-pdf term and completes the weight
+  // after the shading launches.  Null (and in hero-wavelength mode, with a
+  // per-block or no shading order, or where roulette is active): shading
+  // completes the weights itself.
+  float4* defer;
+  float* defer_dist;
 };
 
 struct FrameConst {
@@ -115,7 +125,8 @@ void launchGen(const FrameConst& fc, const WaveBuffers& wb, const ChunkDesc& ch,
 void launchExtend(const SceneView& sc, const WaveBuffers& wb, int parity, bool counting,
                   const LaunchShape& ls, bool cut, cudaStream_t s);
 // Returns the number of kernels launched (one, or with the global sort the
-// scatter and one shading launch per lobe group: four).
+// scatter and one shading launch per lobe group: four, and k_light_pdf after
+// them on a light-sampling level with wb.defer set: five).
 // `light`: the level can draw light samples (false leaves the light-sample code
 // out of the level's global-order shading launches).
 int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb, int depth,

@@ -43,7 +43,9 @@ constexpr size_t kOffSLambda = kOffSL + Q * 4;
 constexpr size_t kOffSProb = kOffSLambda + Q * 4;
 constexpr size_t kOffKey = kOffSProb + Q * 4;      // shading keys (1 B per ray)
 constexpr size_t kOffPerm = kOffKey + Q;           // shading order
-constexpr size_t kOffCounts = kOffPerm + Q * 4;    // 256 B: queue counts
+constexpr size_t kOffDefer = kOffPerm + Q * 4;     // light-pdf deferral (16 B per ray)
+constexpr size_t kOffDeferDist = kOffDefer + Q * 16;  // its lobe values (4 B per ray)
+constexpr size_t kOffCounts = kOffDeferDist + Q * 4;  // 256 B: queue counts
 constexpr size_t kOffStats = kOffCounts + 256;     // 256 B: ray statistics
 constexpr size_t kOffStatus = kOffStats + 256;     // 256 B: kernel status word
 constexpr size_t kOffView = kOffStatus + 256;      // 256 B: the ViewDev table
@@ -53,7 +55,7 @@ constexpr size_t kScratchBytes = kOffWlConst + 256;
 static_assert(sizeof(ViewDev) <= 256, "the view table slot holds one ViewDev");
 static_assert(kOffCounts % 256 == 0 && kOffWlTree % 256 == 0, "256-byte aligned parts");
 
-// ~19.3 MB per device; file scope so that only this file's host code asks for
+// ~21.9 MB per device; file scope so that only this file's host code asks for
 // its address.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -158,6 +160,8 @@ WaveBuffers scratchBuffers(unsigned char* b) {
   w.s_prob = reinterpret_cast<float*>(b + kOffSProb);
   w.shade_key = b + kOffKey;
   w.shade_perm = reinterpret_cast<uint32_t*>(b + kOffPerm);
+  w.defer = reinterpret_cast<float4*>(b + kOffDefer);
+  w.defer_dist = reinterpret_cast<float*>(b + kOffDeferDist);
   w.counts = reinterpret_cast<uint32_t*>(b + kOffCounts);
   w.stats = reinterpret_cast<unsigned long long*>(b + kOffStats);
   w.status = reinterpret_cast<uint32_t*>(b + kOffStatus);

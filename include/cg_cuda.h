@@ -545,7 +545,7 @@ CG_API int cg_server_get_stats(cg_server_t server, cg_server_stats* out);
  * per pixel, `film_rgba8` (may be NULL) uchar4 sRGB — on `stream` (NULL = the
  * default stream) of the current device, and returns when it is done.
  * It calls no cudaMalloc or cudaFree: the ray queues and tables live in a
- * library-owned device array of about 19.3 MB (131072 queued rays) that every
+ * library-owned device array of about 21.9 MB (131072 queued rays) that every
  * GPU loading the library holds until the process exits.  A view whose spp
  * cannot fit that array in one chunk is rejected with CG_E_INVALID.  The call
  * runs on the caller's current device, which must be the device and CUDA

@@ -139,6 +139,32 @@ def test_chunk_pipelines_render_the_same_films(cornell, use_graph):
     B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
 
 
+def test_deferred_light_pdf_matches_inline(cornell):
+    """With the level-wide shading order, the children of a light-sampling
+    level leave the light-pdf term of their denominators to a separate pass
+    (k_light_pdf); with the per-block order the shading kernel adds it itself.
+    Both walk the light BVH with the same explicitly rounded arithmetic, so a
+    512x512, 4 spp frame (one chunk, and several chunks with a 2^20-ray queue)
+    has the same keyed samples either way."""
+    s, g = cornell
+    conf = B.PathTraceConf(render_width=512, render_height=512, sample_count=4, trace_depth=3)
+    out = {}
+    for sort, queue in (("global", 0), ("block", 1 << 20), ("global", 1 << 20)):
+        B.EnvInit(conf)
+        B.SetTuning(queue_capacity=queue, shade_sort=sort)
+        B.View(g, B.Camera.from_c(s.camera))
+        st = B.LastStats()
+        out[(sort, queue)] = (B.ReadFilm(), st.chunks, st.extend_rays, st.shadow_rays)
+    ref = out[("global", 0)]
+    assert ref[1] == 1 and float(np.abs(ref[0]).mean()) > 0.0
+    for key in (("block", 1 << 20), ("global", 1 << 20)):
+        o = out[key]
+        assert o[1] > 1, key
+        assert (o[2], o[3]) == (ref[2], ref[3]), key
+        assert _close(o[0], ref[0]) < RTOL, key
+    B.EnvInit(B.PathTraceConf(render_width=64, render_height=64, sample_count=1, trace_depth=3))
+
+
 def test_view_graph_replay_matches_direct_launches(cornell):
     """View() replays its captured launch sequence; accumulated frames, a
     camera change and a switch to another scene (a new capture) give the films
