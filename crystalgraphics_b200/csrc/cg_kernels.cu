@@ -365,8 +365,13 @@ __device__ __forceinline__ void persistentTraverse(const SceneView& sc, WaveBuff
 // counts[3] (extend) and counts[4] (shadow) are the work counters; each is
 // zeroed by the kernel before its user in stream order (k_gen for depth 0,
 // k_shade for the next extend, k_extend for the shadow launch after it).
+#ifdef CG_TRAV_MAXNREG  // a measurement switch: another register cap for the closest-hit walk
+#define CG_EXTEND_BOUNDS __maxnreg__(CG_TRAV_MAXNREG)
+#else
+#define CG_EXTEND_BOUNDS __launch_bounds__(256, 4)
+#endif
 template <bool kCount, int kNodes, bool kSpec = false>
-__global__ void __launch_bounds__(256, 4) k_extend_persistent(SceneView sc, WaveBuffers wb,
+__global__ void CG_EXTEND_BOUNDS k_extend_persistent(SceneView sc, WaveBuffers wb,
                                                               int parity, int keys) {
   const uint32_t n = min(wb.counts[parity], wb.capacity);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
