@@ -1064,9 +1064,18 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
 
 // At most 96 registers: five blocks of 128 threads per SM (the lobe groups
 // need 90-93 without spills; uncapped they took 98, which left room for four).
+// The launches of levels without light samples fit 64 without spills: eight
+// blocks instead of seven at their natural 72 registers, shading 84.7 -> 73.7
+// ms per 10 icosphere frames and 378 -> 340 ms per 3 instanced frames (a cap of
+// 72 for the deferring launches spilled 32 B and gained nothing).
+// CG_SHADE_NL_REGS overrides the light-free cap for measurements.
+#ifndef CG_SHADE_NL_REGS
+#define CG_SHADE_NL_REGS 64
+#endif
 template <int kSort, int kLobes = kLobesAll, bool kLight = true, bool kDefer = false>
-__global__ void __maxnreg__(96) k_shade(SceneView sc, FrameConst fc, WaveBuffers wb, int depth,
-                                        int parity) {
+__global__ void __maxnreg__(kLight ? 96 : CG_SHADE_NL_REGS) k_shade(SceneView sc, FrameConst fc,
+                                                                    WaveBuffers wb, int depth,
+                                                                    int parity) {
   shadeLevel<kSort, kLobes, false, kLight, kDefer>(sc, fc, wb, depth, parity);
 }
 
