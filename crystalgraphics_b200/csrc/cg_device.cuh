@@ -313,8 +313,8 @@ __device__ __forceinline__ Mat decodeValues(const DevMaterial& m, V3 base, float
     float inv_abbe = m.dispersion / 20.0f;
     real_ior = fmaxf(m.ior + (m.ior - 1.0f) * inv_abbe * (523655.0f / (w * w) - 1.5168f), 1.0f);
   }
-  float im = sqrtf(wclamp((4.0f * real_ior) / (1.0f - reflectance) - powf(real_ior + 1.0f, 2.0f),
-                          0.0f, 10.0f));
+  const float ip1 = real_ior + 1.0f;  // pow(real_ior + 1, 2) as a product
+  float im = sqrtf(wclamp((4.0f * real_ior) / (1.0f - reflectance) - ip1 * ip1, 0.0f, 10.0f));
   Mat e;
   e.diffuse_reflectance = (1.0f - metallic) * (1.0f - transmission) * reflectance;
   e.microfacet_roughness = roughness * roughness;
@@ -431,18 +431,27 @@ constexpr float VNDF_EPS = 1e-6f;
 __device__ __forceinline__ float ggxD(V3 micro, V3 macro, float alpha) {
   float nc = wclamp(dot(micro, macro), 0.0f, 1.0f);
   float nts = fmaxf(0.0f, 1.0f - nc * nc) / fmaxf(nc * nc, VNDF_EPS);
-  float denom = PI * powf(nc, 4.0f) * powf(alpha + nts, 2.0f);
+  // pow(nc, 4) and pow(alpha + nts, 2) as products (the same values up to
+  // rounding; powf's log / exp sequence costs some forty instructions)
+  const float nc2 = nc * nc, an = alpha + nts;
+  float denom = PI * (nc2 * nc2) * (an * an);
   return alpha / fmaxf(denom, VNDF_EPS);
 }
-__device__ __forceinline__ float ggxLambdaTerm(float angle, float alpha) {
-  float t = tanf(angle);
+// The masking terms take the cosine c of the angle whose tangent they need:
+// the reference forms tan(acos(c)), here sqrt(1 - c^2) / c, the same value
+// without the two transcendental calls.  Like acos, it is NaN for c > 1 (a
+// dot product of unit vectors a rounding step above 1), which keeps the
+// reference's unclamped-acos NaN samples; c >= 1e-6 at every call.
+__device__ __forceinline__ float tanOfAcos(float c) { return sqrtf(fmaf(-c, c, 1.0f)) / c; }
+__device__ __forceinline__ float ggxLambdaTerm(float cos_angle, float alpha) {
+  float t = tanOfAcos(cos_angle);
   return (sqrtf(1.0f + alpha * t * t) - 1.0f) / 2.0f;
 }
-__device__ __forceinline__ float ggxG1(float angle, float alpha) {
-  return 1.0f / (1.0f + ggxLambdaTerm(angle, alpha));
+__device__ __forceinline__ float ggxG1(float cos_angle, float alpha) {
+  return 1.0f / (1.0f + ggxLambdaTerm(cos_angle, alpha));
 }
-__device__ __forceinline__ float ggxG2(float a1, float a2, float alpha) {
-  return 1.0f / (1.0f + ggxLambdaTerm(a1, alpha) + ggxLambdaTerm(a2, alpha));
+__device__ __forceinline__ float ggxG2(float c1, float c2, float alpha) {
+  return 1.0f / (1.0f + ggxLambdaTerm(c1, alpha) + ggxLambdaTerm(c2, alpha));
 }
 __device__ __forceinline__ V3 sampleNorm(V3 curr, const Surf& s, float alpha, Rng& rng) {
   V3 macro = orientedNormal(curr, s.sn);
@@ -467,7 +476,7 @@ __device__ __forceinline__ V3 sampleNorm(V3 curr, const Surf& s, float alpha, Rn
 __device__ __forceinline__ float reflectPdf(V3 curr, V3 micro, V3 macro, float alpha) {
   float cmp = fmaxf(dot(-curr, macro), VNDF_EPS);
   float cmi = fmaxf(dot(-curr, micro), VNDF_EPS);
-  float vnp = ggxD(micro, macro, alpha) * ggxG1(acosf(cmp), alpha) * cmi / cmp;
+  float vnp = ggxD(micro, macro, alpha) * ggxG1(cmp, alpha) * cmi / cmp;
   return vnp / (4.0f * cmi);
 }
 __device__ __forceinline__ float relIorT(IOR i) { return fmaxf(i.re, VNDF_EPS); }
@@ -475,7 +484,7 @@ __device__ __forceinline__ float transmitPdf(V3 curr, V3 micro, V3 macro, V3 nex
                                              float alpha) {
   float cmp = fmaxf(dot(-curr, macro), VNDF_EPS);
   float cmi = fmaxf(dot(-curr, micro), VNDF_EPS);
-  float vnp = ggxD(micro, macro, alpha) * ggxG1(acosf(cmp), alpha) * cmi / cmp;
+  float vnp = ggxD(micro, macro, alpha) * ggxG1(cmp, alpha) * cmi / cmp;
   float nmi = dot(next, micro);
   float denom = nmi + cmi / tior;
   return vnp * cmi / fmaxf(denom * denom, VNDF_EPS);
@@ -548,7 +557,7 @@ __device__ __forceinline__ float roughReflectDist(V3 curr, V3 next, const Surf& 
   float alpha = m.microfacet_roughness;
   float cmp = fmaxf(dot(-curr, macro), VNDF_EPS);
   float nmp = fmaxf(dot(next, macro), VNDF_EPS);
-  float rd = ggxD(micro, macro, alpha) * ggxG2(acosf(cmp), acosf(nmp), alpha) / (4.0f * cmp * nmp);
+  float rd = ggxD(micro, macro, alpha) * ggxG2(cmp, nmp, alpha) / (4.0f * cmp * nmp);
   return fresnel(curr, micro, rel) * rd * np;
 }
 __device__ __forceinline__ float specularTransmitDist(V3 curr, V3 next, const Surf& s, const Mat& m) {
@@ -575,7 +584,7 @@ __device__ __forceinline__ float roughTransmitDist(V3 curr, V3 next, const Surf&
   float cmi = fmaxf(dot(-curr, micro), VNDF_EPS);
   float nmi = dot(next, micro);
   float denom = nmi + cmi / tior;
-  float td = m.transmission * ggxD(micro, macro, alpha) * ggxG2(acosf(cmp), acosf(nmp), alpha) *
+  float td = m.transmission * ggxD(micro, macro, alpha) * ggxG2(cmp, nmp, alpha) *
              fabsf(cmi * nmi) / fmaxf(cmp * nmp * denom * denom, VNDF_EPS);
   return (1.0f - fresnel(curr, micro, rel)) * td * np;
 }

@@ -1072,8 +1072,11 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
 #ifndef CG_SHADE_NL_REGS
 #define CG_SHADE_NL_REGS 64
 #endif
+#ifndef CG_SHADE_DEFER_REGS
+#define CG_SHADE_DEFER_REGS 96
+#endif
 template <int kSort, int kLobes = kLobesAll, bool kLight = true, bool kDefer = false>
-__global__ void __maxnreg__(kLight ? 96 : CG_SHADE_NL_REGS) k_shade(SceneView sc, FrameConst fc,
+__global__ void __maxnreg__(kDefer ? CG_SHADE_DEFER_REGS : kLight ? 96 : CG_SHADE_NL_REGS) k_shade(SceneView sc, FrameConst fc,
                                                                     WaveBuffers wb, int depth,
                                                                     int parity) {
   shadeLevel<kSort, kLobes, false, kLight, kDefer>(sc, fc, wb, depth, parity);
