@@ -60,7 +60,12 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(make, depth, spp):
         torch.cuda.synchronize()
         out = film.cpu().numpy()
         assert np.all(np.isfinite(out)), call
-        assert float(np.abs(out[..., :3] - ref).max()) / scale < RTOL, call
+        # per value, against its own size plus the film's mean: the sample
+        # trees' terms reach a sample slot in another order here, and on the
+        # depth-8 icosphere a bright pixel's 1e-6 relative reordering error is
+        # above 1e-4 of the film's mean
+        err = np.abs(out[..., :3] - ref) / (np.abs(ref) + scale)
+        assert float(err.max()) < RTOL, call
         assert int(rgba.cpu().numpy()[..., 3].min()) == 255
     g.close()
     B.EnvTerm()
