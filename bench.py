@@ -688,9 +688,10 @@ def run_ours(args):
     B.SetProfiling(False)
 
     # ---- the options beyond the reference on the same frame: Russian roulette
-    # after the third bounce (as configs[1] states it) and hero-wavelength
-    # sampling (four wavelengths per sample, as configs[0] states it); device
-    # time of the same number of frames, L2 flushed between them ----
+    # after the third bounce (as the icosphere workload's specification states
+    # it) and hero-wavelength sampling (four wavelengths per sample, as the
+    # Cornell workload's states it); device time of the same number of frames,
+    # L2 flushed between them ----
     variants = None
     if (rank == 0 and args.spectral == "reference" and not args.roulette and
             WORKLOAD_NAME == "icosphere" and args.case == "full"):
