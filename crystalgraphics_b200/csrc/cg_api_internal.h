@@ -125,7 +125,7 @@ struct Renderer {
   static constexpr size_t kStatsHostStride = 128;
   unsigned char* stats_host = nullptr;
   bool counting = false;
-  // 64M rays per level queue (~9.7 GB of path state): large chunks keep every
+  // 64M rays per level queue (~11.1 GB of path state): large chunks keep every
   // level's launch full
   cg_tuning tuning{64u << 20, 128u, 128u, 1u, 4u, 1u, 1u, 32u, 2u, 1024u};
   DeviceArena wave_arena;

@@ -441,7 +441,7 @@ CG_API int cg_batch_render(cg_scene_t scene, const cg_view_desc* views,
  * several views) and keeps the best. */
 typedef struct cg_tuning {
   uint32_t queue_capacity;  /* rays per level queue, in [4096, 2^28] (default
-                               64M: ~9.7 GB of path state per pipeline) */
+                               64M: ~11.1 GB of path state per pipeline) */
   uint32_t extend_block;  /* threads per block of the traversal launches: a
                              multiple of 32 in [32, 256] (default 128; 0 = keep) */
   uint32_t shade_block;   /* the same for the shading launch (larger values
