@@ -366,20 +366,21 @@ int allocWave(DeviceArena& arena, WaveBuffers& w, uint32_t capacity) {
 int attachHero(DeviceArena& arena, WaveBuffers& w) {
   const size_t Q = w.capacity, S = w.sample_capacity;
   const size_t q16 = align256(Q * 16);
-  int rc = arena.alloc(3 * q16 + align256(S * 16));
+  int rc = arena.alloc(4 * q16 + align256(S * 16));
   if (rc != CG_OK) return rc;
   char* p = static_cast<char*>(arena.base);
   w.ray_w[0] = reinterpret_cast<float4*>(p);
   w.ray_w[1] = reinterpret_cast<float4*>(p + q16);
   w.sh_w = reinterpret_cast<float4*>(p + 2 * q16);
-  w.s_L4 = reinterpret_cast<float4*>(p + 3 * q16);
+  w.defer_w = reinterpret_cast<float4*>(p + 3 * q16);
+  w.s_L4 = reinterpret_cast<float4*>(p + 4 * q16);
   w.hero = 1u;
   return CG_OK;
 }
 
 void detachHero(DeviceArena& arena, WaveBuffers& w) {
   arena.release();
-  w.ray_w[0] = w.ray_w[1] = w.sh_w = w.s_L4 = nullptr;
+  w.ray_w[0] = w.ray_w[1] = w.sh_w = w.s_L4 = w.defer_w = nullptr;
   w.hero = 0u;
 }
 

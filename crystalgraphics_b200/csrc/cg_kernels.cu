@@ -582,6 +582,11 @@ struct Child {
   uint32_t key;
 };
 
+// Hero mode, a deferred child (k_light_pdf completes it): bit 1 of its ray_w
+// flags says its weight takes the factor kHeroCount (the wavelengths sample
+// differently at its parent and the hero goes alone below).
+constexpr uint32_t kDeferredKw = 2u;
+
 // Russian roulette (an option beyond the reference, which has none): a child
 // spawned at a hit of depth >= FrameConst::roulette survives with
 // q = min(1, its path weight t) and then carries t / q.  Returns the factor
@@ -692,8 +697,8 @@ __global__ void __launch_bounds__(kScatterBlock) k_shade_scatter(WaveBuffers wb,
 // Emission is exact per wavelength.
 // kLight: the level can draw light samples (false: no ray of the level has a
 // light-sample count, so the light sample and the light pdf's code are left out).
-// kDefer (with kLight, not in hero mode): children leave the light-pdf term of
-// their denominators to k_light_pdf (WaveBuffers::defer).
+// kDefer (with kLight): children leave the light-pdf term of their
+// denominators to k_light_pdf (WaveBuffers::defer, and defer_w in hero mode).
 template <int kSort, int kLobes, bool kHero, bool kLight = true, bool kDefer = false>
 __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst& fc,
                                            const WaveBuffers& wb, int depth, int parity) {
@@ -748,8 +753,10 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
     // the hero alone below)
     float4 chw[kHero ? 4 : 1];
     // kDefer: per child its denominator without the light-pdf term (x; -1:
-    // the weight is final) and its lobe value (y)
+    // the weight is final) and its lobe value (y); in hero mode also the
+    // other wavelengths' lobe values
     float2 cha[kDefer ? 4 : 1];
+    float3 chd[kDefer && kHero ? 4 : 1];
     uint32_t nch = 0;
     bool shadow = false;
     float4 sh_o = make_float4(0, 0, 0, 0), sh_d = make_float4(0, 0, 0, 0);
@@ -879,10 +886,13 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
           if constexpr (kHero) {
             float cw = W * coeff * kw;
             float c1 = 0.0f, c2 = 0.0f, c3 = 0.0f;
+            float3 dx = make_float3(0.0f, 0.0f, 0.0f);  // the other wavelengths' lobe values
             if (uniform) {
-              c1 = Wx.x * (lobeDist(model, curr, next, s, mx[0]) / denom);
-              c2 = Wx.y * (lobeDist(model, curr, next, s, mx[1]) / denom);
-              c3 = Wx.z * (lobeDist(model, curr, next, s, mx[2]) / denom);
+              dx = make_float3(lobeDist(model, curr, next, s, mx[0]), lobeDist(model, curr, next, s, mx[1]),
+                               lobeDist(model, curr, next, s, mx[2]));
+              c1 = Wx.x * (dx.x / denom);
+              c2 = Wx.y * (dx.y / denom);
+              c3 = Wx.z * (dx.z / denom);
             }
             if (roulette) {
               const float tmax = fmaxf(fmaxf(cw, 0.0f), fmaxf(fmaxf(c1, c2), c3));
@@ -895,7 +905,19 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
               c3 = c3 * rr;
             }
             if (cw != 0.0f || c1 != 0.0f || c2 != 0.0f || c3 != 0.0f) {
-              chw[nch] = make_float4(c1, c2, c3, __uint_as_float(uniform ? 0u : 1u));
+              uint32_t flags = uniform ? 0u : 1u;
+              if constexpr (kDefer) {
+                cha[nch] = make_float2(a, dist);
+                if (a != -1.0f) {  // completed by k_light_pdf: the parent's weights stay
+                  cw = W;
+                  c1 = Wx.x;
+                  c2 = Wx.y;
+                  c3 = Wx.z;
+                  chd[nch] = dx;
+                  if (kw != 1.0f) flags |= kDeferredKw;
+                }
+              }
+              chw[nch] = make_float4(c1, c2, c3, __uint_as_float(flags));
               ch[nch++] = Child{spawnOrigin(s, next), next, cw, ck};
             }
           } else {
@@ -1040,6 +1062,7 @@ __device__ __forceinline__ void shadeLevel(const SceneView& sc, const FrameConst
           if constexpr (kDefer) {
             wb.defer[pos] = make_float4(dpos.x, dpos.y, dpos.z, cha[k].x);
             wb.defer_dist[pos] = cha[k].y;
+            if constexpr (kHero) wb.defer_w[pos] = make_float4(chd[k].x, chd[k].y, chd[k].z, 0.0f);
           }
         }
       }
@@ -1085,10 +1108,10 @@ __global__ void __maxnreg__(kDefer ? CG_SHADE_DEFER_REGS : kLight ? 96 : CG_SHAD
 // Hero-wavelength mode (level-wide shading order only).  At most 128
 // registers: the group with transmission needs 109 without spills (ptxas
 // chose 96 with spills when left free).
-template <int kLobes, bool kLight = true>
+template <int kLobes, bool kLight = true, bool kDefer = false>
 __global__ void __maxnreg__(128) k_shade_hero(SceneView sc, FrameConst fc, WaveBuffers wb,
                                                     int depth, int parity) {
-  shadeLevel<kShadeSortGlobal, kLobes, true, kLight>(sc, fc, wb, depth, parity);
+  shadeLevel<kShadeSortGlobal, kLobes, true, kLight, kDefer>(sc, fc, wb, depth, parity);
 }
 
 // Completes the weights of the children a light-sampling level deferred
@@ -1109,7 +1132,18 @@ __global__ void __launch_bounds__(256) k_light_pdf(SceneView sc, WaveBuffers wb,
     const float pl = lightPdf(sc, V3{dp.x, dp.y, dp.z}, V3{d4.x, d4.y, d4.z}, wb.status);
     const float denom = fmaxf(__fadd_rn(dp.w, pl), 1e-6f);  // balanceDenom's sum, light count 1
     float* wp = reinterpret_cast<float*>(wb.ray_o[out] + i) + 3;
-    *wp = *wp * (wb.defer_dist[i] / denom);
+    float w = *wp * (wb.defer_dist[i] / denom);
+    if (wb.hero) {  // the other wavelengths' weights, and the factor kHeroCount
+      float4 x = wb.ray_w[out][i];
+      const float4 dx = wb.defer_w[i];
+      uint32_t flags = __float_as_uint(x.w);
+      if (flags & kDeferredKw) w = w * static_cast<float>(kHeroCount);
+      flags &= ~kDeferredKw;
+      x = make_float4(x.x * (dx.x / denom), x.y * (dx.y / denom), x.z * (dx.z / denom),
+                      __uint_as_float(flags));
+      wb.ray_w[out][i] = x;
+    }
+    *wp = w;
   }
 }
 
@@ -1279,8 +1313,16 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
   const uint32_t block = ls.shade_block > 256u ? 256u : ls.shade_block;
   const uint32_t grid = ls.grid_shade ? ls.grid_shade : gridFor(1024u / block);
   constexpr int kOpaque = kLobeHit | kLobeDiffuse | kLobeReflect;
+  const bool rr = fc.roulette != 0u && static_cast<uint32_t>(depth) >= fc.roulette;
   if (wb.hero) {  // hero-wavelength mode: level-wide order, one launch per lobe group
     k_shade_scatter<<<gridFor(4u), kScatterBlock, 0, s>>>(wb, parity);
+    if (light && wb.defer && wb.defer_dist && wb.defer_w && !rr) {  // light-pdf terms in a pass
+      k_shade_hero<0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade_hero<kOpaque, true, true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_shade_hero<kLobesAll, true, true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
+      k_light_pdf<<<gridFor(8u), 256, 0, s>>>(sc, wb, parity ^ 1);
+      return 5;
+    }
     if (light) {
       k_shade_hero<0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
       k_shade_hero<kOpaque><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
@@ -1297,7 +1339,7 @@ int launchShade(const SceneView& sc, const FrameConst& fc, const WaveBuffers& wb
     // one launch per lobe group, each over its keys' range of the permutation
     // the light-pdf terms in a separate pass (not where roulette needs the
     // final weights)
-    if (light && wb.defer && wb.defer_dist && !(fc.roulette != 0u && static_cast<uint32_t>(depth) >= fc.roulette)) {
+    if (light && wb.defer && wb.defer_dist && !rr) {
       k_shade<kShadeSortGlobal, 0><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
       k_shade<kShadeSortGlobal, kOpaque, true, true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);
       k_shade<kShadeSortGlobal, kLobesAll, true, true><<<grid, block, 0, s>>>(sc, fc, wb, depth, parity);

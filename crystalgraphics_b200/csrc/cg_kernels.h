@@ -76,11 +76,13 @@ struct WaveBuffers {
   // term (w; -1: the ray's weight is final), and the lobe value the weight is
   // still to be multiplied by (defer_dist; ray_o.w holds the parent's weight
   // meanwhile).  k_light_pdf adds the light-pdf term and completes the weight
-  // after the shading launches.  Null (and in hero-wavelength mode, with a
-  // per-block or no shading order, or where roulette is active): shading
-  // completes the weights itself.
+  // after the shading launches.  Null (and with a per-block or no shading
+  // order, or where roulette is active): shading completes the weights itself.
   float4* defer;
   float* defer_dist;
+  // hero-wavelength mode: per deferred ray the other three wavelengths' lobe
+  // values (xyz; ray_w.xyz holds the parent's weights meanwhile)
+  float4* defer_w;
 };
 
 struct FrameConst {
